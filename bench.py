@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Gradient evaluations per second of the clinical field (forward dose + plan loss + adjoint).
+
+Workload: water, 128^3 voxels of 2 mm, 41x41 spots at 2.5 mm x 40 layers (67,240 pencil
+beams), ranges 60-160 mm, SOBP-like float32 weights (seed 1); loss L = sum m (D - P)^2
+with a 60 mm target cube at 110 mm depth and a 20 mm shell; gradients wrt all weights
+and the 40 per-layer range shifts.  One step = one gradient evaluation.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank evaluates its own copy of the field
+(independent gradient evaluations, e.g. robust scenarios): weak scaling, no collective
+on the data path; the job time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "fwd+adjoint dose-gradient evals/s, 67,240 spots/128^3 voxels"
+UNIT = "grad_evals/s"
+CREDITED_NOTE = ("credited FLOPs = 2*sum over (layer,slice) pairs with IDD != 0 of "
+                 "(nsx*nsy*ny + nx*nsx*ny), forward and W-adjoint each")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=None)
+    ap.add_argument("--cpu-budget-s", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_arrays():
+    pb = importlib.import_module("gpu-proton-dose-engine_b200")
+    wl = pb.workloads.build_workload(2)
+    return pb, wl
+
+
+def credited_flops(wl, active_pairs):
+    nsx, nsy = wl["n_sx"], wl["n_sy"]
+    g = wl["grid"]
+    per_pair = 2 * (nsx * nsy * g["ny"] + g["nx"] * nsx * g["ny"])
+    return per_pair * active_pairs
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples (every 200 ms) during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_traffic(kernel):
+    """Per-launch DRAM bytes of ``kernel`` from the committed ncu summary, if present."""
+    path = os.path.join(REPO, "profiles", "traffic_per_launch.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# --------------------------------------------------------------------------- CPU port
+def cpu_port_grad_eval(wl, tables, torch):
+    """One gradient evaluation with the oracle's torch CPU port of the reference engine
+    (engines.py:256-274) in float64, autograd for dL/dW and dL/d(idd, sigma), chained
+    with the range-derivative tables for dL/dR."""
+    from oracle import engine_ref as er
+    g = wl["grid"]
+    xv = g["ox"] + np.arange(g["nx"]) * g["dx"]
+    yv = g["oy"] + np.arange(g["ny"]) * g["dy"]
+    xs = (np.arange(wl["n_sx"]) - (wl["n_sx"] - 1) / 2.0) * wl["spot_pitch"]
+    ys = (np.arange(wl["n_sy"]) - (wl["n_sy"] - 1) / 2.0) * wl["spot_pitch"]
+    w = torch.tensor(wl["weights"], dtype=torch.float64, requires_grad=True)
+    idd = torch.tensor(tables["idd"], requires_grad=True)
+    sig = torch.tensor(tables["sigma"], requires_grad=True)
+    d = er.separable_torch(xv, yv, xs, ys, w, idd, sig)
+    loss = er.masked_quadratic_loss(d, tables["mask"], tables["presc"])
+    loss.backward()
+    gr = (idd.grad * tables["didd"]).sum(1) + (sig.grad * tables["dsig"]).sum(1)
+    return {"loss": float(loss), "dose": d.detach(), "grad_w": w.grad, "grad_range": gr}
+
+
+def cpu_tables(wl):
+    from oracle import physics_ref as pr
+    import torch
+    g = wl["grid"]
+    z = g["oz"] + np.arange(g["nz"]) * g["dz"]
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    idd, sig = pr.layer_luts(z, en)
+    h = 0.005
+    ip, sp = pr.layer_luts(z, en, range_shift=np.full(len(en), h))
+    im, sm = pr.layer_luts(z, en, range_shift=np.full(len(en), -h))
+    return {"idd": idd, "sigma": sig, "didd": torch.tensor((ip - im) / (2 * h)),
+            "dsig": torch.tensor((sp - sm) / (2 * h)),
+            "mask": torch.tensor(wl["mask"], dtype=torch.float64),
+            "presc": torch.tensor(wl["presc"], dtype=torch.float64)}
+
+
+def run_cpu_port(wl, budget_s, max_evals=None, warmup=1):
+    import torch
+    tables = cpu_tables(wl)
+    for _ in range(warmup):
+        cpu_port_grad_eval(wl, tables, torch)
+    n, t0, last = 0, time.perf_counter(), None
+    while True:
+        last = cpu_port_grad_eval(wl, tables, torch)
+        n += 1
+        el = time.perf_counter() - t0
+        if (max_evals is not None and n >= max_evals) or (max_evals is None and el >= budget_s):
+            break
+    return n / el, n, el, torch.get_num_threads(), last
+
+
+# --------------------------------------------------------------------------- reference arm
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    pb, wl = workload_arrays()
+    steps = max(1, args.steps)
+    rate, n, el, cores, _ = run_cpu_port(wl, budget_s=0.0, max_evals=steps,
+                                         warmup=min(args.warmup, 2))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * el / n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "grid": [128, 128, 128], "spots": 67240,
+                       "layers": 40, "engine": "torch CPU port of engines.torch_separable "
+                       "(per_layer=True) + autograd, float64"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{n} full gradient evaluations"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    pb, wl = workload_arrays()
+    lib = pb._lib
+    prec = args.precision or pb.engines.DEFAULT_PRECISION
+    prob = pb.model.problem_from_workload(wl)
+    plan = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
+    active = plan.active_pairs()
+    flops_eval = 2 * credited_flops(wl, active)
+    m = torch.as_tensor(wl["mask"], device=dev)
+    p = torch.as_tensor(wl["presc"], device=dev)
+    out = plan.alloc_outputs()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    for _ in range(max(args.warmup, 3)):
+        plan.loss_grad(m, p, outputs=out)
+    torch.cuda.synchronize(dev)
+
+    # ---- device-resident timed region ----
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    n0 = lib.launch_count()
+    lib.profile_begin()
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record()
+        plan.loss_grad(m, p, outputs=out)
+        ev[k][1].record()
+    torch.cuda.synchronize(dev)
+    prof = lib.profile_end()
+    launches = lib.launch_count() - n0
+    barrier()
+    clk = clocks.stop()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        t = torch.tensor([t_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    value = world * K / (t_ms * 1e-3)
+
+    # ---- end to end through the public API, host buffers ----
+    w_host = torch.tensor(wl["weights"], dtype=torch.float32).pin_memory()
+    gw_host = torch.empty_like(w_host).pin_memory()
+    gr_host = torch.empty(wl["n_layers"], dtype=torch.float32).pin_memory()
+    loss_host = torch.empty((), dtype=torch.float64).pin_memory()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(K)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(K):
+        flush.zero_()
+        ev2[k][0].record()
+        o = plan.loss_grad(m, p, w=w_host, outputs=out)
+        gw_host.copy_(o["grad_w"], non_blocking=True)
+        gr_host.copy_(o["grad_range"], non_blocking=True)
+        loss_host.copy_(o["loss"], non_blocking=True)
+        ev2[k][1].record()
+    torch.cuda.synchronize(dev)
+    barrier()
+    t2 = sum(a.elapsed_time(b) for a, b in ev2)
+    if world > 1:
+        t = torch.tensor([t2], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t2 = float(t.item())
+    e2e = world * K / (t2 * 1e-3)
+    h2d = w_host.numel() * 4
+    d2h = gw_host.numel() * 4 + gr_host.numel() * 4 + 8
+
+    # ---- roofline of the dominant kernel ----
+    pk, pk_src = peaks()
+    dom = "adjoint" if prof["adj_ms"] >= prof["fwd_ms"] else "forward"
+    dom_ms = (prof["adj_ms"] / max(prof["n_adj"], 1)) if dom == "adjoint" else \
+        (prof["fwd_ms"] / max(prof["n_fwd"], 1))
+    per_launch_flop = flops_eval / 2.0
+    achieved = per_launch_flop / (dom_ms * 1e-3) / 1e12
+    peak = float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops")))
+    kname = "adj_simt_kernel" if dom == "adjoint" else "fwd_simt_kernel"
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": read_traffic(kname), "kernel": kname,
+            "kernel_ms_per_launch": dom_ms, "flop_per_launch": per_launch_flop,
+            "peak_source": f"{pk_src} bf16 sustained (MEASURED_PEAKS.json)" if pk_src == "measured"
+            else "fallback bf16 sustained", "note": CREDITED_NOTE,
+            "fwd_ms_per_launch": prof["fwd_ms"] / max(prof["n_fwd"], 1),
+            "adj_ms_per_launch": prof["adj_ms"] / max(prof["n_adj"], 1)}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": max(args.warmup, 3), "ms_per_step": t_ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32" if prec == "fp32" else prec,
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "grid": [128, 128, 128], "spots": 67240,
+                       "layers": 40, "active_pairs": active, "precision": prec,
+                       "credited_flop_per_eval": flops_eval,
+                       "l2": "flushed between steps (256 MiB write, outside the events)",
+                       "parallelism": f"{world} independent evaluations (one per rank)"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "roofline": roof, "clocks": clk}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, n, el, cores, ref = run_cpu_port(wl, args.cpu_budget_s)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{n} full gradient evaluations in {el:.1f} s "
+                                          "(torch CPU float64 port + autograd)"}
+        torch.cuda.synchronize(dev)
+        o = plan.loss_grad(m, p, outputs=out)
+        torch.cuda.synchronize(dev)
+        dref = ref["dose"].numpy()
+        gwr = ref["grad_w"].numpy()
+        grr = ref["grad_range"].numpy()
+        line["accuracy_vs_fp64"] = {
+            "dose_max_rel": float(np.max(np.abs(o["dose"].cpu().numpy() - dref)) / np.max(np.abs(dref))),
+            "grad_w_max_rel": float(np.max(np.abs(o["grad_w"].cpu().numpy() - gwr)) / np.max(np.abs(gwr))),
+            "grad_range_max_rel": float(np.max(np.abs(o["grad_range"].cpu().numpy() - grr))
+                                        / np.max(np.abs(grr)))}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

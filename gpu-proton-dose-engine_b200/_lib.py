@@ -1,0 +1,169 @@
+"""ctypes binding of libpbdose_b200.so (the C ABI declared in include/pbdose_b200.h).
+
+The library is loaded lazily on first use so that the host-only parts of the package
+(model types, workloads) import on machines without a GPU.  Every call that reaches
+the device goes through ``call`` which raises ``PbdError`` with the library's own
+message for a non-zero return code.  There is no fallback: a missing library or a
+missing CUDA device is an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from ctypes import POINTER, c_char_p, c_double, c_int, c_size_t, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpbdose_b200.so")
+
+PBD_OK = 0
+PREC = {"fp32": 0, "tf32x3": 1, "tf32": 2, "bf16x3": 3, "bf16": 4}
+MAX_JOBS = 128
+
+
+class PbdError(RuntimeError):
+    def __init__(self, fn, code, msg):
+        super().__init__(f"{fn} failed: {msg} (code {code})")
+        self.code = code
+
+
+class Field(ctypes.Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("nz", c_int),
+                ("dx", c_double), ("dy", c_double), ("dz", c_double),
+                ("ox", c_double), ("oy", c_double), ("oz", c_double),
+                ("n_sx", c_int), ("n_sy", c_int), ("n_layers", c_int),
+                ("dx_spot", c_double), ("dy_spot", c_double),
+                ("x0", c_double), ("y0", c_double)]
+
+
+class LutSpec(ctypes.Structure):
+    _fields_ = [("nz", c_int), ("z0", c_double), ("dz", c_double), ("depth_scale", c_double),
+                ("anchor_surface", c_int),
+                ("sigma_x0", c_double), ("sigma_theta0", c_double), ("rho0", c_double),
+                ("fe_n_sub", c_int), ("fe_max_step", c_double),
+                ("straggling_model", c_int), ("strag_coef", c_double), ("strag_exp", c_double),
+                ("energy_spread", c_double), ("atten_len", c_double), ("idd_n_fine", c_int),
+                ("fd_step", c_double)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("field", Field), ("w", c_void_p), ("idd", c_void_p), ("sigma", c_void_p),
+                ("dose", c_void_p)]
+
+
+_SIGS = {
+    "pbd_strerror": (c_char_p, [c_int]),
+    "pbd_version": (c_int, []),
+    "pbd_field_validate": (c_int, [POINTER(Field)]),
+    "pbd_set_schedule": (c_int, [c_int, c_int]),
+    "pbd_profile_begin": (c_int, []),
+    "pbd_profile_end": (c_int, [POINTER(c_double), POINTER(c_int), POINTER(c_double),
+                                POINTER(c_int)]),
+    "pbd_launch_count": (c_int, [POINTER(ctypes.c_longlong)]),
+    "pbd_lut_workspace": (c_int, [POINTER(LutSpec), c_int, POINTER(c_size_t)]),
+    "pbd_build_luts": (c_int, [POINTER(LutSpec), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "pbd_csda_range": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "pbd_energy_from_range": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "pbd_forward_workspace": (c_int, [POINTER(Field), c_int, POINTER(c_size_t)]),
+    "pbd_forward": (c_int, [POINTER(Field), c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                            c_void_p, c_size_t, c_void_p]),
+    "pbd_adjoint_workspace": (c_int, [POINTER(Field), c_int, POINTER(c_size_t)]),
+    "pbd_adjoint": (c_int, [POINTER(Field), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                            c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
+    "pbd_loss_grad_workspace": (c_int, [POINTER(Field), c_int, POINTER(c_size_t)]),
+    "pbd_loss_grad": (c_int, [POINTER(Field), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
+    "pbd_forward_batch_workspace": (c_int, [POINTER(Job), c_int, c_int, POINTER(c_size_t)]),
+    "pbd_forward_batch": (c_int, [POINTER(Job), c_int, c_int, c_void_p, c_size_t, c_void_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def exported_symbols():
+    """Names the C ABI header declares (used by the symbol test)."""
+    return sorted(_SIGS)
+
+
+def load():
+    """Load the shared library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                    "(there is no CPU fallback)")
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def strerror(code: int) -> str:
+    return load().pbd_strerror(code).decode()
+
+
+def call(name: str, *args) -> None:
+    rc = getattr(load(), name)(*args)
+    if rc != PBD_OK:
+        raise PbdError(name, rc, strerror(rc))
+
+
+def query(name: str, *args) -> int:
+    out = c_size_t(0)
+    call(name, *args, ctypes.byref(out))
+    return int(out.value)
+
+
+def launch_count() -> int:
+    n = ctypes.c_longlong(0)
+    call("pbd_launch_count", ctypes.byref(n))
+    return int(n.value)
+
+
+def profile_begin() -> None:
+    call("pbd_profile_begin")
+
+
+def profile_end() -> dict:
+    fm, am = c_double(0), c_double(0)
+    fn, an = c_int(0), c_int(0)
+    call("pbd_profile_end", ctypes.byref(fm), ctypes.byref(fn), ctypes.byref(am), ctypes.byref(an))
+    return {"fwd_ms": fm.value, "n_fwd": fn.value, "adj_ms": am.value, "n_adj": an.value}
+
+
+def ptr(t) -> int | None:
+    """Device address of a torch tensor (None for None)."""
+    if t is None:
+        return None
+    return int(t.data_ptr())
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device is required: this engine has no CPU path")
+    return torch
+
+
+def stream_handle(device=None) -> int:
+    torch = require_cuda()
+    return int(torch.cuda.current_stream(device).cuda_stream)
+
+
+def precision_code(p) -> int:
+    if isinstance(p, int):
+        return p
+    try:
+        return PREC[str(p).lower()]
+    except KeyError:
+        raise ValueError(f"unknown precision {p!r}; expected one of {sorted(PREC)}") from None

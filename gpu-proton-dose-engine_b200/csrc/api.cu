@@ -1,0 +1,509 @@
+// api.cu -- extern "C" entry points of libpbdose_b200.so (declared in include/pbdose_b200.h).
+//
+// Rules of the boundary (the reference ABI's, pencil_beam.cu:647-730): validate first,
+// return PBD_OK or a negative code, never exit, never throw across the boundary.  Work
+// goes onto the caller's stream; no host<->device copies and no allocation happen here:
+// per-call device state (job descriptors, schedules, partial sums) lives in the
+// caller's workspace and is written by kernels from launch parameters, so every call
+// can be captured into a CUDA graph.
+#include <math.h>
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "pbd_internal.cuh"
+
+namespace pbd {
+
+namespace {
+thread_local int g_fwd_chunk = 0;   // 0 = default
+thread_local int g_adj_chunk = 0;
+
+struct JobPair {
+    JobDev j[2];
+    int n;
+};
+
+__global__ void install_jobs_kernel(JobPair p, JobDev* dst) {
+    if ((int)threadIdx.x < p.n) dst[threadIdx.x] = p.j[threadIdx.x];
+}
+
+struct JobLite {
+    int nx, ny, nz, nsx, nsy, nl;
+    int item_base, max_items, max_chunks, pad_;
+    double ox, oy, dx, dy, sx0, sy0, dsx, dsy;
+    const float* w;
+    const double* idd;
+    const double* sigma;
+    float* dose;
+    size_t partial_off, nchunk_off;
+};
+
+struct JobTable {
+    int n;
+    JobLite j[PBD_MAX_JOBS];
+};
+static_assert(sizeof(JobTable) < 32000, "kernel parameter limit");
+
+__global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_base, int* nchunk_base) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= t.n) return;
+    const JobLite& a = t.j[k];
+    JobDev J;
+    memset(&J, 0, sizeof(J));
+    J.nx = a.nx; J.ny = a.ny; J.nz = a.nz; J.nsx = a.nsx; J.nsy = a.nsy; J.nl = a.nl;
+    J.ntx = (a.nx + kTile - 1) / kTile;
+    J.nty = (a.ny + kTile - 1) / kTile;
+    J.max_chunks = a.max_chunks; J.item_base = a.item_base; J.max_items = a.max_items;
+    J.ox = a.ox; J.oy = a.oy; J.dx = a.dx; J.dy = a.dy;
+    J.sx0 = a.sx0; J.sy0 = a.sy0; J.dsx = a.dsx; J.dsy = a.dsy;
+    J.w = a.w; J.idd = a.idd; J.sigma = a.sigma; J.dose = a.dose;
+    J.partial = partial_base + a.partial_off;
+    J.nchunks = nchunk_base + a.nchunk_off;
+    dst[k] = J;
+}
+
+int g_sms[64] = {0};
+std::mutex g_sms_mu;
+
+struct ProfState {
+    bool on = false;
+    std::vector<cudaEvent_t> ev[2];   // alternating begin/end per kernel kind
+    size_t used[2] = {0, 0};
+    long long launches = 0;
+};
+thread_local ProfState g_prof;
+
+int choose_fwd_chunk(const pbd_field* f) {
+    int c = g_fwd_chunk > 0 ? g_fwd_chunk : fwd_chunk_layers(f);
+    return c < 1 ? 1 : (c > kMaxChunkCost ? kMaxChunkCost : c);
+}
+int choose_adj_chunk(const pbd_field* f) {
+    int c = g_adj_chunk > 0 ? g_adj_chunk : adj_chunk_depths(f);
+    return c < 1 ? 1 : (c > kMaxChunkCost ? kMaxChunkCost : c);
+}
+
+bool finite_pos(double v) { return isfinite(v) && v > 0.0; }
+
+int check_precision(int p) {
+    if (p == PBD_PREC_FP32) return PBD_OK;
+    if (p >= PBD_PREC_TF32X3 && p <= PBD_PREC_BF16) return PBD_ERR_UNSUPPORTED;
+    return PBD_ERR_BAD_VALUE;
+}
+
+int adjoint_supported(const pbd_field* f) {
+    if (f->n_sx > kAdjMaxSpots || f->n_sy > kAdjMaxSpots) return PBD_ERR_UNSUPPORTED;
+    return PBD_OK;
+}
+
+// Workspace of the single-job paths.
+struct Ws {
+    JobDev* jobs;        // [0] forward view, [1] adjoint view
+    int* counters;       // [0] forward, [1] adjoint
+    FwdItem* fitems;
+    int* fnch;
+    float* fpart;
+    double* loss_part;
+    AdjItem* aitems;
+    int* anch;
+    float* apart;
+    float* dc;
+    float* dsg;
+    int f_items, a_items, f_chunk, a_chunk;
+};
+
+int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, void* base, Ws& w, size_t* used) {
+    Carve c(base);
+    w.jobs = c.take<JobDev>(2);
+    w.counters = c.take<int>(2);
+    w.f_chunk = choose_fwd_chunk(f);
+    w.a_chunk = choose_adj_chunk(f);
+    w.fitems = nullptr; w.fnch = nullptr; w.fpart = nullptr; w.loss_part = nullptr;
+    w.aitems = nullptr; w.anch = nullptr; w.apart = nullptr; w.dc = nullptr; w.dsg = nullptr;
+    w.f_items = w.a_items = 0;
+    if (fwd) {
+        size_t pe = 0;
+        PBD_TRY(fwd_plan_sizes(f, w.f_chunk, &pe, &w.f_items));
+        w.fitems = c.take<FwdItem>(w.f_items);
+        w.fnch = c.take<int>(f->nz);
+        w.fpart = c.take<float>(pe);
+    }
+    if (loss) w.loss_part = c.take<double>(kLossBlocks);
+    if (adj) {
+        size_t pe = 0;
+        PBD_TRY(adj_plan_sizes(f, w.a_chunk, &pe, &w.a_items));
+        w.aitems = c.take<AdjItem>(w.a_items);
+        w.anch = c.take<int>(f->n_layers);
+        w.apart = c.take<float>(pe);
+        w.dc = c.take<float>((size_t)f->n_layers * f->nz);
+        w.dsg = c.take<float>((size_t)f->n_layers * f->nz);
+    }
+    *used = c.used + 256;
+    return PBD_OK;
+}
+
+}  // namespace
+
+int num_sms() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> g(g_sms_mu);
+    if (g_sms[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        g_sms[dev] = v;
+    }
+    return g_sms[dev];
+}
+
+void prof_mark(int which, int end, cudaStream_t s) {
+    if (!g_prof.on) return;
+    std::vector<cudaEvent_t>& v = g_prof.ev[which];
+    size_t& u = g_prof.used[which];
+    if ((end == 0) != (u % 2 == 0)) return;   // keep begin/end paired
+    if (u == v.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        v.push_back(e);
+    }
+    cudaEventRecord(v[u], s);
+    ++u;
+}
+
+void count_launch(int n) { g_prof.launches += n; }
+
+int host_validate_field(const pbd_field* f) {
+    if (!f) return PBD_ERR_NULL_ARG;
+    if (f->nx <= 0 || f->ny <= 0 || f->nz <= 0 || f->n_sx <= 0 || f->n_sy <= 0 || f->n_layers <= 0)
+        return PBD_ERR_BAD_DIM;
+    if (f->n_sx > 4096 || f->n_sy > 4096 || f->n_layers > 4096) return PBD_ERR_UNSUPPORTED;
+    if ((double)f->nx * f->ny * f->nz > 2147483647.0) return PBD_ERR_UNSUPPORTED;
+    if (!finite_pos(f->dx) || !finite_pos(f->dy) || !finite_pos(f->dz) ||
+        !finite_pos(f->dx_spot) || !finite_pos(f->dy_spot))
+        return PBD_ERR_BAD_VALUE;
+    if (!isfinite(f->ox) || !isfinite(f->oy) || !isfinite(f->oz) || !isfinite(f->x0) ||
+        !isfinite(f->y0))
+        return PBD_ERR_BAD_VALUE;
+    return PBD_OK;
+}
+
+int fill_job(const pbd_field* f, JobDev* J) {
+    memset(J, 0, sizeof(*J));
+    J->nx = f->nx; J->ny = f->ny; J->nz = f->nz;
+    J->nsx = f->n_sx; J->nsy = f->n_sy; J->nl = f->n_layers;
+    J->ntx = (f->nx + kTile - 1) / kTile;
+    J->nty = (f->ny + kTile - 1) / kTile;
+    J->ox = f->ox; J->oy = f->oy; J->dx = f->dx; J->dy = f->dy;
+    J->sx0 = f->x0; J->sy0 = f->y0; J->dsx = f->dx_spot; J->dsy = f->dy_spot;
+    return PBD_OK;
+}
+
+}  // namespace pbd
+
+using namespace pbd;
+
+extern "C" {
+
+const char* pbd_strerror(int code) {
+    switch (code) {
+        case PBD_OK: return "ok";
+        case PBD_ERR_NULL_ARG: return "null argument";
+        case PBD_ERR_BAD_DIM: return "invalid dimension";
+        case PBD_ERR_BAD_VALUE: return "invalid value (non-finite or non-positive spacing, step or sigma)";
+        case PBD_ERR_CUDA: return "CUDA runtime error";
+        case PBD_ERR_UNSUPPORTED: return "unsupported configuration";
+        case PBD_ERR_NO_SMEM: return "insufficient shared memory per block";
+        case PBD_ERR_WORKSPACE: return "workspace missing or too small";
+        case PBD_ERR_TIMEOUT: return "bounded device wait ran out";
+        case PBD_ERR_TOO_MANY: return "too many jobs for one launch";
+        default: return "unknown error";
+    }
+}
+
+int pbd_version(void) { return 100; }
+
+int pbd_field_validate(const pbd_field* f) { return host_validate_field(f); }
+
+int pbd_set_schedule(int fwd_layers_per_item, int adj_depths_per_item) {
+    if (fwd_layers_per_item < 0 || fwd_layers_per_item > kMaxChunkCost ||
+        adj_depths_per_item < 0 || adj_depths_per_item > kMaxChunkCost)
+        return PBD_ERR_BAD_VALUE;
+    g_fwd_chunk = fwd_layers_per_item;
+    g_adj_chunk = adj_depths_per_item;
+    return PBD_OK;
+}
+
+int pbd_profile_begin(void) {
+    g_prof.on = true;
+    g_prof.used[0] = g_prof.used[1] = 0;
+    return PBD_OK;
+}
+
+int pbd_profile_end(double* fwd_ms, int* n_fwd, double* adj_ms, int* n_adj) {
+    double* ms[2] = {fwd_ms, adj_ms};
+    int* cnt[2] = {n_fwd, n_adj};
+    int rc = PBD_OK;
+    for (int k = 0; k < 2; ++k) {
+        double tot = 0.0;
+        int n = 0;
+        for (size_t i = 0; i + 1 < g_prof.used[k]; i += 2) {
+            float t = 0.f;
+            if (cudaEventSynchronize(g_prof.ev[k][i + 1]) != cudaSuccess ||
+                cudaEventElapsedTime(&t, g_prof.ev[k][i], g_prof.ev[k][i + 1]) != cudaSuccess) {
+                rc = PBD_ERR_CUDA;
+                break;
+            }
+            tot += t;
+            ++n;
+        }
+        if (ms[k]) *ms[k] = tot;
+        if (cnt[k]) *cnt[k] = n;
+    }
+    g_prof.on = false;
+    g_prof.used[0] = g_prof.used[1] = 0;
+    return rc;
+}
+
+int pbd_launch_count(long long* n) {
+    if (!n) return PBD_ERR_NULL_ARG;
+    *n = g_prof.launches;
+    return PBD_OK;
+}
+
+int pbd_lut_workspace(const pbd_lut_spec* spec, int n_layers, size_t* bytes) {
+    return lut_workspace_bytes(spec, n_layers, bytes);
+}
+
+int pbd_build_luts(const pbd_lut_spec* spec, int n_layers, const double* energies,
+                   const double* range_shift, double* idd, double* sigma, double* didd_dr,
+                   double* dsigma_dr, void* workspace, size_t workspace_bytes, void* stream) {
+    return lut_build(spec, n_layers, energies, range_shift, idd, sigma, didd_dr, dsigma_dr,
+                     workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int pbd_csda_range(const double* energy, double* range_cm, int n, void* stream) {
+    return lut_csda(energy, range_cm, n, 0, (cudaStream_t)stream);
+}
+
+int pbd_energy_from_range(const double* range_cm, double* energy, int n, void* stream) {
+    return lut_csda(range_cm, energy, n, 1, (cudaStream_t)stream);
+}
+
+int pbd_forward_workspace(const pbd_field* f, int precision, size_t* bytes) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_precision(precision));
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    Ws w;
+    return carve_ws(f, true, false, false, nullptr, w, bytes);
+}
+
+int pbd_forward(const pbd_field* f, const float* w, const double* idd, const double* sigma,
+                float* dose, int precision, void* workspace, size_t workspace_bytes, void* stream) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_precision(precision));
+    if (!w || !idd || !sigma || !dose) return PBD_ERR_NULL_ARG;
+    size_t need = 0;
+    Ws ws;
+    PBD_TRY(carve_ws(f, true, false, false, nullptr, ws, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_ws(f, true, false, false, workspace, ws, &need));
+    cudaStream_t s = (cudaStream_t)stream;
+    JobPair p;
+    memset(&p, 0, sizeof(p));
+    p.n = 1;
+    JobDev& J = p.j[0];
+    fill_job(f, &J);
+    J.w = w; J.idd = idd; J.sigma = sigma; J.dose = dose;
+    J.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
+    J.item_base = 0; J.max_items = ws.f_items;
+    J.partial = ws.fpart; J.nchunks = ws.fnch;
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 0, s);
+}
+
+int pbd_adjoint_workspace(const pbd_field* f, int precision, size_t* bytes) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_precision(precision));
+    PBD_TRY(adjoint_supported(f));
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    Ws w;
+    return carve_ws(f, false, true, false, nullptr, w, bytes);
+}
+
+static void fill_adj_view(const pbd_field* f, const Ws& ws, JobDev& A) {
+    A.max_chunks = (f->nz + ws.a_chunk - 1) / ws.a_chunk;
+    A.item_base = 0;
+    A.max_items = ws.a_items;
+    A.partial = ws.apart;
+    A.nchunks = ws.anch;
+    A.dc = ws.dc;
+    A.dsg = ws.dsg;
+}
+
+int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const double* sigma,
+                const double* didd_dr, const double* dsigma_dr, const float* grad_dose,
+                float* grad_w, float* grad_range, int precision, void* workspace,
+                size_t workspace_bytes, void* stream) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_precision(precision));
+    PBD_TRY(adjoint_supported(f));
+    if (!w || !idd || !sigma || !grad_dose || !grad_w) return PBD_ERR_NULL_ARG;
+    const int with_range = grad_range != nullptr;
+    if (with_range && (!didd_dr || !dsigma_dr)) return PBD_ERR_NULL_ARG;
+    size_t need = 0;
+    Ws ws;
+    PBD_TRY(carve_ws(f, false, true, false, nullptr, ws, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_ws(f, false, true, false, workspace, ws, &need));
+    cudaStream_t s = (cudaStream_t)stream;
+    JobPair p;
+    memset(&p, 0, sizeof(p));
+    p.n = 2;
+    JobDev& A = p.j[1];
+    fill_job(f, &A);
+    A.w = w; A.idd = idd; A.sigma = sigma; A.didd_dr = didd_dr; A.dsig_dr = dsigma_dr;
+    A.grad_dose = const_cast<float*>(grad_dose);
+    A.grad_w = grad_w; A.grad_range = grad_range;
+    fill_adj_view(f, ws, A);
+    p.j[0] = A;
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 1, ws.a_chunk,
+                          with_range, 0, s);
+}
+
+int pbd_loss_grad_workspace(const pbd_field* f, int precision, size_t* bytes) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_precision(precision));
+    PBD_TRY(adjoint_supported(f));
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    Ws w;
+    return carve_ws(f, true, true, true, nullptr, w, bytes);
+}
+
+int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const double* sigma,
+                  const double* didd_dr, const double* dsigma_dr, const float* mask,
+                  const float* presc, float* dose, float* grad_dose, double* loss, float* grad_w,
+                  float* grad_range, int precision, void* workspace, size_t workspace_bytes,
+                  void* stream) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_precision(precision));
+    PBD_TRY(adjoint_supported(f));
+    if (!w || !idd || !sigma || !mask || !presc || !dose || !grad_dose || !loss || !grad_w)
+        return PBD_ERR_NULL_ARG;
+    const int with_range = grad_range != nullptr;
+    if (with_range && (!didd_dr || !dsigma_dr)) return PBD_ERR_NULL_ARG;
+    size_t need = 0;
+    Ws ws;
+    PBD_TRY(carve_ws(f, true, true, true, nullptr, ws, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_ws(f, true, true, true, workspace, ws, &need));
+    cudaStream_t s = (cudaStream_t)stream;
+    JobPair p;
+    memset(&p, 0, sizeof(p));
+    p.n = 2;
+    JobDev& F = p.j[0];
+    fill_job(f, &F);
+    F.w = w; F.idd = idd; F.sigma = sigma; F.didd_dr = didd_dr; F.dsig_dr = dsigma_dr;
+    F.dose = dose; F.mask = mask; F.presc = presc; F.grad_dose = grad_dose;
+    F.loss_part = ws.loss_part; F.loss = loss; F.grad_w = grad_w; F.grad_range = grad_range;
+    JobDev A = F;
+    F.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
+    F.item_base = 0; F.max_items = ws.f_items;
+    F.partial = ws.fpart; F.nchunks = ws.fnch;
+    fill_adj_view(f, ws, A);
+    p.j[1] = A;
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 1, s));
+    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 1, ws.a_chunk,
+                          with_range, 1, s);
+}
+
+int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, size_t* bytes) {
+    if (!jobs || !bytes) return PBD_ERR_NULL_ARG;
+    if (n_jobs <= 0) return PBD_ERR_BAD_DIM;
+    if (n_jobs > PBD_MAX_JOBS) return PBD_ERR_TOO_MANY;
+    PBD_TRY(check_precision(precision));
+    Carve c(nullptr);
+    c.take<JobDev>(n_jobs);
+    c.take<int>(1);
+    size_t items = 0, nch = 0, part = 0;
+    for (int k = 0; k < n_jobs; ++k) {
+        PBD_TRY(host_validate_field(&jobs[k].field));
+        const int ch = choose_fwd_chunk(&jobs[k].field);
+        size_t pe = 0;
+        int it = 0;
+        PBD_TRY(fwd_plan_sizes(&jobs[k].field, ch, &pe, &it));
+        items += it;
+        nch += jobs[k].field.nz;
+        part += pe;
+    }
+    if (items > (size_t)1 << 30) return PBD_ERR_UNSUPPORTED;
+    c.take<FwdItem>(items);
+    c.take<int>(nch);
+    c.take<float>(part);
+    *bytes = c.used + 256;
+    return PBD_OK;
+}
+
+int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+    size_t need = 0;
+    PBD_TRY(pbd_forward_batch_workspace(jobs, n_jobs, precision, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    for (int k = 0; k < n_jobs; ++k)
+        if (!jobs[k].w || !jobs[k].idd || !jobs[k].sigma || !jobs[k].dose) return PBD_ERR_NULL_ARG;
+    static JobTable t;                 // large; filled under the lock below
+    static std::mutex mu;
+    std::lock_guard<std::mutex> g(mu);
+    memset(&t, 0, sizeof(t));
+    t.n = n_jobs;
+    int item_base = 0;
+    size_t nch_off = 0, part_off = 0;
+    int chunk = kMaxChunkCost;
+    JobDev host_view[PBD_MAX_JOBS];
+    for (int k = 0; k < n_jobs; ++k) {
+        const pbd_field* f = &jobs[k].field;
+        const int ch = choose_fwd_chunk(f);
+        chunk = ch < chunk ? ch : chunk;
+    }
+    for (int k = 0; k < n_jobs; ++k) {
+        const pbd_field* f = &jobs[k].field;
+        size_t pe = 0;
+        int it = 0;
+        PBD_TRY(fwd_plan_sizes(f, chunk, &pe, &it));
+        JobLite& a = t.j[k];
+        a.nx = f->nx; a.ny = f->ny; a.nz = f->nz; a.nsx = f->n_sx; a.nsy = f->n_sy;
+        a.nl = f->n_layers;
+        a.item_base = item_base; a.max_items = it;
+        a.max_chunks = (f->n_layers + chunk - 1) / chunk;
+        a.ox = f->ox; a.oy = f->oy; a.dx = f->dx; a.dy = f->dy;
+        a.sx0 = f->x0; a.sy0 = f->y0; a.dsx = f->dx_spot; a.dsy = f->dy_spot;
+        a.w = jobs[k].w; a.idd = jobs[k].idd; a.sigma = jobs[k].sigma; a.dose = jobs[k].dose;
+        a.partial_off = part_off; a.nchunk_off = nch_off;
+        fill_job(f, &host_view[k]);
+        item_base += it;
+        nch_off += f->nz;
+        part_off += pe;
+    }
+    Carve c(workspace);
+    JobDev* jd = c.take<JobDev>(n_jobs);
+    int* counter = c.take<int>(1);
+    FwdItem* items = c.take<FwdItem>(item_base);
+    int* nchb = c.take<int>(nch_off);
+    float* partb = c.take<float>(part_off);
+    cudaStream_t s = (cudaStream_t)stream;
+    install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, chunk, 0, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,493 @@
+// lut.cu -- FP64 depth-LUT builder on the device.
+//
+// Builds, for every energy layer, the integral depth dose IDD_l(z) (physics.py:328-387,
+// normalize=False) and the lateral width sigma_l(z) (physics.py:221-286) at the dose
+// grid's depths, plus their central differences in CSDA range for the range-shift
+// gradient.  This file is compiled with -fmad=false: products and sums are rounded one
+// at a time, in the order the reference's NumPy expressions evaluate them, so the
+// tables agree with the reference to the last few ulps of the transcendental functions.
+//
+// Two steps are restated in a different but equivalent form:
+//  * CSDA range table cumulative sum: one thread, sequential, as numpy.cumsum.
+//  * Range-straggling convolution.  The reference multiplies the zero-padded rfft of
+//    the binned dose (nfft = 16384 >= 2 n_fine) by exp(-2 (pi f sigma_R)^2).  By the
+//    Poisson summation formula, irfft of that Gaussian spectrum is h * phi_sigma(k h)
+//    summed over periods of nfft*h; all other periods and all frequencies past Nyquist
+//    are below 1e-300 for any sigma_R >= 2 h, and the zero padding makes the circular
+//    convolution linear.  The device therefore computes the linear convolution
+//    smooth[n] = sum_m binned[m] * h * phi(|n-m| h) directly in FP64, truncated at
+//    16 sigma_R (kernel weight < 1e-55).  The two agree to FFT round-off (~1e-16 of
+//    the peak).
+#include <math.h>
+#include <stdio.h>
+
+#include "pbd_internal.cuh"
+
+namespace pbd {
+namespace {
+
+// physics.py:42-66
+constexpr double kMp = 938.27208816;
+constexpr double kMe = 0.51099895000;
+constexpr double kKbb = 0.307075;
+constexpr double kZA = 10.0 / 18.01528;
+constexpr double kI = 75.0 * 1e-6;
+constexpr double kRho = 1.0;
+constexpr double kX0 = 36.08;
+constexpr double kPowerP = 1.77;
+constexpr double kHighland = 13.6;
+constexpr double kElo = 0.5;
+constexpr double kEhi = 400.0;
+constexpr double kBohr = kKbb * kZA * kRho * kMe;   // physics.py:151
+constexpr int kTableN = 3797;                        // 800 + 899 + 899 + 1199 points
+constexpr int kBohrN = 4000;                         // physics.py:154
+
+__device__ double g_etab[kTableN];
+__device__ double g_rtab[kTableN];
+
+// numpy.linspace(a, b, n)[k]: k*step + a, the last point set to b exactly.
+__device__ __forceinline__ double lin(double a, double b, int n, int k) {
+    if (k == n - 1) return b;
+    double step = (b - a) / (double)(n - 1);
+    return (double)k * step + a;
+}
+
+// Energy grid of the range table (physics.py:118-123): four linspace pieces with the
+// shared end points 2, 20 and 60 MeV kept once.
+__device__ double table_energy(int k) {
+    if (k < 800) return lin(kElo, 2.0, 800, k);
+    if (k < 1699) return lin(2.0, 20.0, 900, k - 799);
+    if (k < 2598) return lin(20.0, 60.0, 900, k - 1698);
+    return lin(60.0, kEhi, 1200, k - 2597);
+}
+
+// beta_gamma, physics.py:72-77
+__device__ __forceinline__ void kinematics(double e, double& beta, double& gam, double& b2) {
+    gam = 1.0 + e / kMp;
+    b2 = 1.0 - 1.0 / (gam * gam);
+    b2 = fmin(fmax(b2, 1e-14), 1.0);
+    beta = sqrt(b2);
+}
+
+// bethe_bloch_water, physics.py:80-100
+__device__ double stopping_power(double e) {
+    double beta, gam, b2;
+    kinematics(e, beta, gam, b2);
+    const double me_mp = kMe / kMp;
+    double g2 = gam * gam;
+    double tmax = 2.0 * kMe * b2 * g2 / (1.0 + 2.0 * gam * me_mp + me_mp * me_mp);
+    double arg = 2.0 * kMe * b2 * g2 * tmax / (kI * kI);
+    arg = fmax(arg, 1.0 + 1e-12);
+    return kKbb * kZA * kRho / b2 * (0.5 * log(arg) - b2);
+}
+
+// scattering_power(model="highland_local") at L = 1, physics.py:202-217
+__device__ double highland_local(double e) {
+    double beta, gam, b2;
+    kinematics(e, beta, gam, b2);
+    double pc = sqrt(fmax(gam * gam - 1.0, 0.0)) * kMp;
+    double bpc = fmax(beta * pc, 1e-9);
+    double q = kHighland / bpc;
+    double base = q * q / kX0;
+    const double lnl = 0.0;   // log(1)
+    return base * (1.0 + 0.038 * lnl) * (1.076 + 0.038 * lnl);
+}
+
+// numpy.interp on a strictly increasing table.
+__device__ double interp(double x, const double* xp, const double* fp, int n, double left,
+                         double right) {
+    if (x < xp[0]) return left;
+    if (x > xp[n - 1]) return right;
+    if (x == xp[n - 1]) return fp[n - 1];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (xp[mid] <= x) lo = mid; else hi = mid;
+    }
+    if (xp[lo] == x) return fp[lo];
+    double slope = (fp[lo + 1] - fp[lo]) / (xp[lo + 1] - xp[lo]);
+    return slope * (x - xp[lo]) + fp[lo];
+}
+
+// numpy.interp where xp = linspace(a, b, n) is generated on the fly.
+__device__ double interp_lin(double x, double a, double b, int n, const double* fp, double left,
+                             double right) {
+    if (x < a) return left;
+    if (x > b) return right;
+    if (x == b) return fp[n - 1];
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (lin(a, b, n, mid) <= x) lo = mid; else hi = mid;
+    }
+    double x0 = lin(a, b, n, lo);
+    if (x0 == x) return fp[lo];
+    double x1 = lin(a, b, n, lo + 1);
+    double slope = (fp[lo + 1] - fp[lo]) / (x1 - x0);
+    return slope * (x - x0) + fp[lo];
+}
+
+__device__ __forceinline__ double csda(double e) {
+    return interp(e, g_etab, g_rtab, kTableN, g_rtab[0], g_rtab[kTableN - 1]);
+}
+__device__ __forceinline__ double energy_at_range(double r) {
+    double rc = fmin(fmax(r, 0.0), g_rtab[kTableN - 1]);
+    return interp(rc, g_rtab, g_etab, kTableN, g_etab[0], g_etab[kTableN - 1]);
+}
+
+// _range_table, physics.py:111-127.  Trapezoid steps in parallel, cumulative sum in
+// one thread in the order numpy.cumsum adds.
+__global__ void range_table_kernel() {
+    __shared__ double inv_s[kTableN];
+    for (int k = threadIdx.x; k < kTableN; k += blockDim.x) {
+        double e = table_energy(k);
+        g_etab[k] = e;
+        inv_s[k] = 1.0 / stopping_power(e);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        g_rtab[0] = 0.0;
+        double e_prev = g_etab[0];
+        for (int k = 1; k < kTableN; ++k) {
+            double e = g_etab[k];
+            r = r + 0.5 * (inv_s[k] + inv_s[k - 1]) * (e - e_prev);
+            g_rtab[k] = r;
+            e_prev = e;
+        }
+    }
+}
+
+__global__ void csda_kernel(const double* in, double* out, int n, int inverse) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = inverse ? energy_at_range(in[i]) : csda(in[i]);
+}
+
+// Per (layer, variant) scalars.  Variant 0 is the nominal build, 1 and 2 are built at
+// CSDA range +fd_step and -fd_step.
+struct LayerScal {
+    double e0, r0, sig_r, zmax, h;
+    int conv_k;
+    int pad_;
+};
+
+struct LutDims {
+    int n_layers, nvar, nz, n_idd, n_fe;
+    double fe_lo, fe_hi;      // Fermi-Eyges fine grid end points
+    double fd_step;
+};
+
+// Setup of one (layer, variant): energy, range, sigma_R (physics.py:154-174, 310-322),
+// the binned CSDA dose (physics.py:362-370), the Gaussian kernel table and the local
+// scattering power on the Fermi-Eyges fine grid (physics.py:259-264).
+__global__ void layer_setup_kernel(pbd_lut_spec spec, LutDims dm, const double* energies,
+                                   const double* shift, LayerScal* scal, double* binned,
+                                   double* ker, double* t_fe) {
+    __shared__ double f_bohr[kBohrN];
+    __shared__ double red[256];
+    const int lv = blockIdx.x;
+    const int l = lv / dm.nvar, v = lv % dm.nvar;
+    const double off = v == 0 ? 0.0 : (v == 1 ? dm.fd_step : -dm.fd_step);
+    const double s = (shift ? shift[l] : 0.0) + off;
+    const double e_in = energies[l];
+    const double e0 = (s == 0.0) ? e_in : energy_at_range(csda(e_in) + s);
+    const double r0 = csda(e0);
+
+    // range straggling
+    double strag = 0.0;
+    if (spec.straggling_model == 0) {
+        double acc = 0.0;
+        if (e0 > kElo) {
+            for (int k = threadIdx.x; k < kBohrN; k += blockDim.x) {
+                double e = lin(kElo, e0, kBohrN, k);
+                double sp = stopping_power(e);
+                double beta, gam, b2;
+                kinematics(e, beta, gam, b2);
+                f_bohr[k] = kBohr / (fmax(b2, 1e-12) * (sp * sp * sp));
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < kBohrN - 1; k += blockDim.x) {
+                double de = lin(kElo, e0, kBohrN, k + 1) - lin(kElo, e0, kBohrN, k);
+                acc += de * (f_bohr[k + 1] + f_bohr[k]) / 2.0;
+            }
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        strag = sqrt(red[0]);
+    } else if (spec.straggling_model == 1) {
+        strag = spec.strag_coef * pow(r0, spec.strag_exp);
+    }
+    const double espr = kPowerP * spec.energy_spread * r0;
+    const double sig_r = hypot(strag, espr);
+    const int n = dm.n_idd;
+    const double zmax = r0 + 8.0 * sig_r + 0.2;
+    const double h = lin(0.0, zmax, n, 1) - 0.0;
+    int kk = 0;
+    if (sig_r > 0.0) {
+        double kf = ceil(16.0 * sig_r / h);
+        kk = kf > (double)(n - 1) ? n - 1 : (int)kf;
+    }
+    if (threadIdx.x == 0) {
+        LayerScal sc;
+        sc.e0 = e0; sc.r0 = r0; sc.sig_r = sig_r; sc.zmax = zmax; sc.h = h; sc.conv_k = kk;
+        sc.pad_ = 0;
+        scal[lv] = sc;
+    }
+    double* bin = binned + (size_t)lv * n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double zf = lin(0.0, zmax, n, k);
+        double ea = lin(0.0, zmax, n + 1, k);
+        double eb = lin(0.0, zmax, n + 1, k + 1);
+        double ena = ea < r0 ? energy_at_range(fmax(r0 - ea, 0.0)) : 0.0;
+        double enb = eb < r0 ? energy_at_range(fmax(r0 - eb, 0.0)) : 0.0;
+        double fl = exp(-zf / spec.atten_len);
+        bin[k] = fl * (ena - enb) / h;
+    }
+    if (sig_r > 0.0) {
+        double* kr = ker + (size_t)lv * n;
+        const double c = kInvSqrt2Pi / sig_r;
+        for (int k = threadIdx.x; k <= kk; k += blockDim.x) {
+            double t = (double)k * h;
+            kr[k] = h * (c * exp(-(t * t) / (2.0 * sig_r * sig_r)));
+        }
+    }
+    double* tf = t_fe + (size_t)lv * dm.n_fe;
+    for (int i = threadIdx.x; i < dm.n_fe; i += blockDim.x) {
+        double zf = lin(dm.fe_lo, dm.fe_hi, dm.n_fe, i);
+        double t = 0.0;
+        if (zf < r0) {
+            double el = energy_at_range(fmax(r0 - zf, 0.0));
+            t = highland_local(fmax(el, 1e-3));
+        }
+        tf[i] = t;
+    }
+}
+
+// Range-straggling convolution (see the file comment).
+__global__ void conv_kernel(LutDims dm, const LayerScal* scal, const double* binned,
+                            const double* ker, double* smooth) {
+    const int lv = blockIdx.x;
+    const int n = dm.n_idd;
+    const int i = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double* bin = binned + (size_t)lv * n;
+    const LayerScal sc = scal[lv];
+    if (sc.sig_r <= 0.0) {
+        smooth[(size_t)lv * n + i] = bin[i];
+        return;
+    }
+    const double* kr = ker + (size_t)lv * n;
+    const int lo = max(0, i - sc.conv_k), hi = min(n - 1, i + sc.conv_k);
+    double acc = 0.0;
+    for (int m = lo; m <= hi; ++m) acc += bin[m] * kr[abs(i - m)];
+    smooth[(size_t)lv * n + i] = acc;
+}
+
+// Fermi-Eyges direct scattering integral B(zf_i) = sum_{j<i} (zf_i - zf_j)^2 T_j h_j,
+// physics.py:266-270, with h = numpy.gradient(zf).
+__device__ __forceinline__ double fe_h(const LutDims& dm, int j) {
+    const int n = dm.n_fe;
+    if (j == 0) return lin(dm.fe_lo, dm.fe_hi, n, 1) - lin(dm.fe_lo, dm.fe_hi, n, 0);
+    if (j == n - 1) return lin(dm.fe_lo, dm.fe_hi, n, n - 1) - lin(dm.fe_lo, dm.fe_hi, n, n - 2);
+    return (lin(dm.fe_lo, dm.fe_hi, n, j + 1) - lin(dm.fe_lo, dm.fe_hi, n, j - 1)) / 2.0;
+}
+
+__global__ void fe_grid_kernel(LutDims dm, double* zf, double* hf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < dm.n_fe; i += gridDim.x * blockDim.x) {
+        zf[i] = lin(dm.fe_lo, dm.fe_hi, dm.n_fe, i);
+        hf[i] = fe_h(dm, i);
+    }
+}
+
+__global__ void fe_b_kernel(LutDims dm, const double* zf, const double* hf, const double* t_fe,
+                            double* b_fe) {
+    const int lv = blockIdx.x;
+    const int i = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= dm.n_fe) return;
+    const double* tf = t_fe + (size_t)lv * dm.n_fe;
+    const double zi = zf[i];
+    double acc = 0.0;
+    for (int j = 0; j < i; ++j) {
+        double d = zi - zf[j];
+        acc += d * d * tf[j] * hf[j];
+    }
+    b_fe[(size_t)lv * dm.n_fe + i] = acc;
+}
+
+// Tables at the requested depths, all variants of one layer per block; the variants
+// combine into the range derivatives.
+__global__ void lut_output_kernel(pbd_lut_spec spec, LutDims dm, const LayerScal* scal,
+                                  const double* smooth, const double* zf_fe, const double* b_fe,
+                                  double single_depth, double* idd, double* sigma,
+                                  double* didd, double* dsig) {
+    const int l = blockIdx.x;
+    for (int k = threadIdx.x; k < dm.nz; k += blockDim.x) {
+        double d = spec.depth_scale * (spec.z0 + (double)k * spec.dz);
+        double dz_eval = (dm.nz == 1 && !spec.anchor_surface) ? single_depth : d;
+        double out_i[3], out_s[3];
+        for (int v = 0; v < dm.nvar; ++v) {
+            const int lv = l * dm.nvar + v;
+            const LayerScal sc = scal[lv];
+            out_i[v] = interp_lin(d, 0.0, sc.zmax, dm.n_idd, smooth + (size_t)lv * dm.n_idd, 0.0,
+                                  0.0);
+            double b = 0.0;
+            if (!(spec.anchor_surface && d <= 0.0))
+                b = interp(dz_eval, zf_fe, b_fe + (size_t)lv * dm.n_fe, dm.n_fe,
+                           b_fe[(size_t)lv * dm.n_fe], b_fe[(size_t)lv * dm.n_fe + dm.n_fe - 1]);
+            double zp = dz_eval / spec.depth_scale;
+            double var = spec.sigma_x0 * spec.sigma_x0
+                       + 2.0 * spec.rho0 * spec.sigma_x0 * spec.sigma_theta0 * zp
+                       + spec.sigma_theta0 * spec.sigma_theta0 * (zp * zp)
+                       + b / (spec.depth_scale * spec.depth_scale);
+            out_s[v] = sqrt(fmax(var, 0.0));
+        }
+        const size_t o = (size_t)l * dm.nz + k;
+        idd[o] = out_i[0];
+        sigma[o] = out_s[0];
+        if (dm.nvar == 3) {
+            if (didd) didd[o] = (out_i[1] - out_i[2]) / (2.0 * dm.fd_step);
+            if (dsig) dsig[o] = (out_s[1] - out_s[2]) / (2.0 * dm.fd_step);
+        }
+    }
+}
+
+// Depth list of the Fermi-Eyges integral (host): its first and last points and size.
+struct FeList {
+    int n_list;
+    double lo, hi, single_depth;
+    int n_fine;
+};
+
+FeList fe_list(const pbd_lut_spec* s) {
+    FeList fl{};
+    const int nz = s->nz;
+    auto depth = [&](int k) { return s->depth_scale * (s->z0 + (double)k * s->dz); };
+    fl.single_depth = 0.0;
+    if (!s->anchor_surface) {
+        if (nz == 1) {  // physics.py:249-253
+            double z1 = depth(0);
+            fl.single_depth = z1 > 0 ? z1 : 1e-6;
+            fl.lo = 0.0; fl.hi = fl.single_depth; fl.n_list = 2;
+        } else {
+            fl.lo = depth(0); fl.hi = depth(nz - 1); fl.n_list = nz;
+        }
+    } else {
+        int pos = 0;
+        for (int k = 0; k < nz; ++k) pos += depth(k) > 0.0;
+        fl.lo = 0.0;
+        fl.hi = pos > 0 ? depth(nz - 1) : 1e-6;
+        fl.n_list = pos + 1;
+    }
+    double span = fl.hi - fl.lo;   // physics.py:256-258
+    int need = span > 0 ? (int)ceil(span / fmax(s->fe_max_step, 1e-6)) + 1 : 2;
+    int a = (fl.n_list - 1) * s->fe_n_sub + 1;
+    int nf = a > need ? a : need;
+    fl.n_fine = nf > 2 ? nf : 2;
+    return fl;
+}
+
+int validate_spec(const pbd_lut_spec* s, int n_layers) {
+    if (!s) return PBD_ERR_NULL_ARG;
+    if (n_layers <= 0 || s->nz <= 0 || s->idd_n_fine < 3 || s->fe_n_sub < 1) return PBD_ERR_BAD_DIM;
+    if (!(s->dz > 0.0) || !(s->depth_scale > 0.0) || !(s->atten_len > 0.0) ||
+        !(s->fe_max_step > 0.0) || !(s->fd_step >= 0.0) || !(s->sigma_x0 >= 0.0) ||
+        !(s->energy_spread >= 0.0))
+        return PBD_ERR_BAD_VALUE;
+    if (s->straggling_model < 0 || s->straggling_model > 2) return PBD_ERR_BAD_VALUE;
+    if (s->idd_n_fine > (1 << 20)) return PBD_ERR_UNSUPPORTED;
+    FeList fl = fe_list(s);
+    if (fl.n_fine > (1 << 16)) return PBD_ERR_UNSUPPORTED;
+    return PBD_OK;
+}
+
+struct LutWs {
+    LayerScal* scal;
+    double *binned, *ker, *smooth, *t_fe, *b_fe, *zf_fe, *hf_fe;
+};
+
+size_t carve_lut(Carve& c, LutWs& w, int n_layers, int nvar, int n_idd, int n_fe) {
+    const size_t lv = (size_t)n_layers * nvar;
+    w.scal = c.take<LayerScal>(lv);
+    w.binned = c.take<double>(lv * n_idd);
+    w.ker = c.take<double>(lv * n_idd);
+    w.smooth = c.take<double>(lv * n_idd);
+    w.t_fe = c.take<double>(lv * n_fe);
+    w.b_fe = c.take<double>(lv * n_fe);
+    w.zf_fe = c.take<double>(n_fe);
+    w.hf_fe = c.take<double>(n_fe);
+    return c.used;
+}
+
+}  // namespace
+
+int lut_workspace_bytes(const pbd_lut_spec* s, int n_layers, size_t* bytes) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    FeList fl = fe_list(s);
+    Carve c(nullptr);
+    LutWs w;
+    *bytes = carve_lut(c, w, n_layers, s->fd_step > 0 ? 3 : 1, s->idd_n_fine, fl.n_fine) + 256;
+    return PBD_OK;
+}
+
+int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const double* shift,
+              double* idd, double* sigma, double* didd, double* dsig, void* ws, size_t ws_bytes,
+              cudaStream_t st) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!energies || !idd || !sigma) return PBD_ERR_NULL_ARG;
+    if (s->fd_step > 0 && (!didd || !dsig)) return PBD_ERR_NULL_ARG;
+    size_t need = 0;
+    PBD_TRY(lut_workspace_bytes(s, n_layers, &need));
+    if (!ws || ws_bytes < need) return PBD_ERR_WORKSPACE;
+    FeList fl = fe_list(s);
+    LutDims dm;
+    dm.n_layers = n_layers;
+    dm.nvar = s->fd_step > 0 ? 3 : 1;
+    dm.nz = s->nz;
+    dm.n_idd = s->idd_n_fine;
+    dm.n_fe = fl.n_fine;
+    dm.fe_lo = fl.lo;
+    dm.fe_hi = fl.hi;
+    dm.fd_step = s->fd_step;
+    Carve c(ws);
+    LutWs w;
+    carve_lut(c, w, n_layers, dm.nvar, dm.n_idd, dm.n_fe);
+    const int lvn = n_layers * dm.nvar;
+
+    range_table_kernel<<<1, 1024, 0, st>>>();
+    PBD_LAUNCH_CHECK();
+    fe_grid_kernel<<<(dm.n_fe + 255) / 256, 256, 0, st>>>(dm, w.zf_fe, w.hf_fe);
+    PBD_LAUNCH_CHECK();
+    layer_setup_kernel<<<lvn, 256, 0, st>>>(*s, dm, energies, shift, w.scal, w.binned, w.ker,
+                                            w.t_fe);
+    PBD_LAUNCH_CHECK();
+    conv_kernel<<<dim3(lvn, (dm.n_idd + 127) / 128), 128, 0, st>>>(dm, w.scal, w.binned, w.ker,
+                                                                   w.smooth);
+    PBD_LAUNCH_CHECK();
+    fe_b_kernel<<<dim3(lvn, (dm.n_fe + 127) / 128), 128, 0, st>>>(dm, w.zf_fe, w.hf_fe, w.t_fe,
+                                                                  w.b_fe);
+    PBD_LAUNCH_CHECK();
+    lut_output_kernel<<<n_layers, 128, 0, st>>>(*s, dm, w.scal, w.smooth, w.zf_fe, w.b_fe,
+                                                 fl.single_depth, idd, sigma, didd, dsig);
+    PBD_LAUNCH_CHECK();
+    count_launch(6);
+    return PBD_OK;
+}
+
+int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st) {
+    if (!e || !r) return PBD_ERR_NULL_ARG;
+    if (n < 0) return PBD_ERR_BAD_DIM;
+    range_table_kernel<<<1, 1024, 0, st>>>();
+    PBD_LAUNCH_CHECK();
+    if (n == 0) return PBD_OK;
+    csda_kernel<<<(n + 255) / 256, 256, 0, st>>>(e, r, n, inverse);
+    PBD_LAUNCH_CHECK();
+    count_launch(2);
+    return PBD_OK;
+}
+
+}  // namespace pbd

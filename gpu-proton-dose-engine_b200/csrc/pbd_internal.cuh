@@ -1,0 +1,127 @@
+// Internal declarations shared by the CUDA translation units of libpbdose_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/pbdose_b200.h"
+
+namespace pbd {
+
+constexpr double kInvSqrt2Pi = 0.39894228040143267794;   // 1/sqrt(2 pi)
+constexpr double kInv2Pi = 0.15915494309189533577;       // 1/(2 pi)
+constexpr double kLog2e = 1.44269504088896340736;
+
+// ---------------------------------------------------------------------------
+// Device-side view of one job (field x scenario).  Written into the workspace by
+// the scheduling kernels from the launch parameters, read by the compute kernels.
+// ---------------------------------------------------------------------------
+struct JobDev {
+    int nx, ny, nz, nsx, nsy, nl;
+    int ntx, nty;                 // lateral tiles of 128 x 128 voxels
+    int max_chunks;               // forward: layer chunks per depth slice; adjoint: z chunks per layer
+    int item_base, max_items;     // slice of the flat item array owned by this job
+    int pad_;
+    double ox, oy, dx, dy;        // voxel centres x = ox + k dx
+    double sx0, sy0, dsx, dsy;    // spot centres xs = sx0 + (i - (nsx-1)/2) dsx
+    const float* w;               // (nl, nsy, nsx)
+    const double* idd;            // (nl, nz)
+    const double* sigma;          // (nl, nz)
+    const double* didd_dr;        // (nl, nz) or null
+    const double* dsig_dr;        // (nl, nz) or null
+    float* dose;                  // (nz, ny, nx)
+    float* partial;               // forward: (max_chunks, nz, ny, nx); adjoint: (nl, max_chunks, nsy, nsx)
+    int* nchunks;                 // forward: (nz); adjoint: (nl)
+    const float* mask;            // loss
+    const float* presc;
+    float* grad_dose;             // (nz, ny, nx): written by the loss, read by the adjoint
+    double* loss_part;            // per-block partial sums of the loss
+    double* loss;                 // device scalar
+    float* grad_w;                // (nl, nsy, nsx)
+    float* grad_range;            // (nl)
+    float* dc;                    // (nl, nz) dL/dIDD
+    float* dsg;                   // (nl, nz) dL/dsigma
+};
+
+struct FwdItem { int job, z, ty, tx, lb, le, chunk, cost; };
+struct AdjItem { int job, l, zb, ze, chunk, cost, pad0, pad1; };
+
+constexpr int kTile = 128;          // lateral tile edge (voxels)
+constexpr int kSpotChunk = 64;      // spots per lattice chunk in the FP32 forward
+constexpr int kAdjMaxSpots = 64;    // adjoint lattice limit per axis
+constexpr int kMaxChunkCost = 64;   // largest layers-per-item / z-per-item
+constexpr int kLossBlocks = 296;    // fixed grid of the loss reduction (deterministic order)
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? PBD_OK : PBD_ERR_CUDA; }
+
+#define PBD_TRY(expr)                         \
+    do {                                      \
+        int pbd_rc_ = (expr);                 \
+        if (pbd_rc_ != PBD_OK) return pbd_rc_; \
+    } while (0)
+
+#define PBD_LAUNCH_CHECK()                                       \
+    do {                                                         \
+        cudaError_t pbd_e_ = cudaGetLastError();                 \
+        if (pbd_e_ != cudaSuccess) return PBD_ERR_CUDA;          \
+    } while (0)
+
+// Bump allocator over the caller's workspace.  With base == nullptr it only sizes.
+struct Carve {
+    char* base;
+    size_t used;
+    explicit Carve(void* b) : base(static_cast<char*>(b)), used(0) {}
+    template <class T>
+    T* take(size_t count) {
+        used = align_up(used, 256);
+        T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+        used += count * sizeof(T);
+        return p;
+    }
+};
+
+// Host-side planning of one job (shared by the forward and adjoint paths).
+struct JobPlan {
+    JobDev dev;
+    size_t partial_elems;
+    size_t nchunk_elems;
+    int items;
+};
+
+int fill_job(const pbd_field* f, JobDev* j);
+
+// Profiling hooks (api.cu): event pairs around the dominant kernels while enabled on
+// the calling thread, and a per-thread count of kernels this library launched.
+enum ProfKernel { kProfFwd = 0, kProfAdj = 1 };
+void prof_mark(int which, int end, cudaStream_t s);
+void count_launch(int n = 1);
+int host_validate_field(const pbd_field* f);
+int num_sms();
+
+// forward (FP32 SIMT) -- fwd_simt.cu
+int fwd_chunk_layers(const pbd_field* f);
+int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items);
+int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
+                   int total_items, int* counter, int chunk, int with_loss, cudaStream_t s);
+
+// adjoint (FP32 SIMT) -- adj_simt.cu
+int adj_chunk_depths(const pbd_field* f);
+int adj_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items);
+int launch_adjoint(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, AdjItem* items,
+                   int total_items, int* counter, int chunk, int with_range, int finalize_loss,
+                   cudaStream_t s);
+
+// LUT builder -- lut.cu
+int lut_workspace_bytes(const pbd_lut_spec* s, int n_layers, size_t* bytes);
+int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const double* shift,
+              double* idd, double* sigma, double* didd, double* dsig, void* ws, size_t ws_bytes,
+              cudaStream_t st);
+int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st);
+
+}  // namespace pbd

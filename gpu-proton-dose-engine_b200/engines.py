@@ -1,0 +1,304 @@
+"""Dose engines: the drop-in ``torch_separable`` and its differentiable, plan-based form.
+
+``torch_separable`` keeps the reference's signature and return convention
+(engines.py:208-283) and computes the per-layer exact separable dose with the CUDA
+library.  ``DosePlan`` holds one field's geometry, weights and depth tables on the
+device for repeated forward / adjoint / loss-gradient calls; ``SeparableDose`` is the
+``torch.autograd.Function`` over it, differentiable in the spot weights and the
+per-layer range shifts.  There is no CPU path: every function here that computes a
+dose needs the built library and a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from . import physics as ph
+from .model import PBProblem
+
+INV_SQRT_2PI = 1.0 / np.sqrt(2.0 * np.pi)
+DEFAULT_PRECISION = "fp32"
+DEFAULT_FD_STEP = 0.005   # cm: central-difference step of the range-derivative tables
+
+
+def lateral_kernel(vox_axis, spot_axis, sigma, normalized: bool = True) -> np.ndarray:
+    """Host utility with the reference's semantics (engines.py:49-61); not used by the engine,
+    whose kernels generate these factors on the fly."""
+    d = (np.asarray(vox_axis)[:, None] - np.asarray(spot_axis)[None, :]) ** 2
+    s = np.clip(np.asarray(sigma, dtype=np.float64), 1e-9, None)
+    out = np.exp(-d / (2.0 * s[..., None, None] ** 2))
+    if normalized:
+        out = out * (INV_SQRT_2PI / s)[..., None, None]
+    return out
+
+
+def relative_error(a, b, mask=None) -> dict:
+    """Error of ``a`` against reference ``b`` (engines.py:364-378): max |a-b| / max |b| etc."""
+    a = np.asarray(a.detach().cpu() if hasattr(a, "detach") else a, dtype=np.float64)
+    b = np.asarray(b.detach().cpu() if hasattr(b, "detach") else b, dtype=np.float64)
+    if mask is None:
+        mask = np.ones_like(b, dtype=bool)
+    d = (a - b)[mask]
+    ref_max = float(np.max(np.abs(b))) or 1.0
+    return {
+        "max_abs_err": float(np.abs(d).max()) if d.size else 0.0,
+        "max_rel_err_global": float(np.abs(d).max() / ref_max) if d.size else 0.0,
+        "rms_err": float(np.sqrt((d**2).mean())) if d.size else 0.0,
+        "rms_rel_global": float(np.sqrt((d**2).mean()) / ref_max) if d.size else 0.0,
+        "n_vox": int(mask.sum()),
+    }
+
+
+def normalize_dose(d, mode: str = "max", roi=None):
+    """Dose normalisation (engines.py:381-388)."""
+    d = np.asarray(d, dtype=np.float64)
+    ref = float(d[roi].max()) if (mode == "roi_max" and roi is not None) else float(d.max())
+    return d / (ref if ref > 0 else 1.0), ref
+
+
+def operation_counts(problem: PBProblem, active_pairs: Optional[int] = None) -> dict:
+    """Multiply-add counts of the separable contraction, with the layer factor included
+    (the reference's engines.py:83-96 counts one layer).  ``active_pairs`` = number of
+    (layer, slice) pairs with non-zero IDD; default: all."""
+    g, L = problem.grid, problem.lattice
+    per_pair = L.n_sx * L.n_sy * g.ny + g.nx * L.n_sx * g.ny
+    pairs = L.n_layers * g.nz if active_pairs is None else int(active_pairs)
+    return {"naive": L.n_spots * g.n_vox, "separable_exact": per_pair * pairs, "pairs": pairs,
+            "M": L.n_spots, "N_vox": g.n_vox, "L": L.n_layers}
+
+
+class _Workspace:
+    """Device scratch buffers cached by (name, size)."""
+
+    def __init__(self, device):
+        self.device = device
+        self._bufs = {}
+
+    def get(self, name, nbytes):
+        torch = _lib.require_cuda()
+        buf = self._bufs.get(name)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=self.device)
+            self._bufs[name] = buf
+        return buf
+
+
+class DosePlan:
+    """One field resident on the device: geometry, weights, depth tables, scratch.
+
+    ``tables`` may be ("problem") the problem's own host tables (the drop-in's
+    semantics), or ("device") tables rebuilt by the device LUT builder from the lattice
+    energies, which also provides the range-derivative tables needed for
+    dL/d(range shift)."""
+
+    def __init__(self, problem: PBProblem, *, precision: str = DEFAULT_PRECISION,
+                 tables: str = "device", fd_step: float = DEFAULT_FD_STEP, device=None,
+                 range_shift=None):
+        torch = _lib.require_cuda()
+        self.torch = torch
+        self.device = torch.device(device or "cuda")
+        self.problem = problem
+        self.field = problem.field_descriptor()
+        _lib.call("pbd_field_validate", ctypes.byref(self.field))
+        self.precision = _lib.precision_code(precision)
+        self.fd_step = float(fd_step)
+        g, L = problem.grid, problem.lattice
+        self.shape = (g.nz, g.ny, g.nx)
+        self.w = torch.as_tensor(np.ascontiguousarray(L.ensure_weights(), dtype=np.float32),
+                                 device=self.device)
+        self.energies = None if L.energies is None else np.asarray(L.energies, dtype=np.float64)
+        self.ws = _Workspace(self.device)
+        self.tables_mode = tables
+        self.range_shift = None
+        if tables == "problem":
+            self.idd = torch.as_tensor(np.ascontiguousarray(problem.idd, dtype=np.float64),
+                                       device=self.device)
+            self.sigma = torch.as_tensor(np.ascontiguousarray(problem.sigma, dtype=np.float64),
+                                         device=self.device)
+            self.didd = self.dsig = None
+        elif tables == "device":
+            if self.energies is None:
+                raise ValueError("device tables need lattice.energies")
+            self.set_range_shift(range_shift)
+        else:
+            raise ValueError("tables must be 'problem' or 'device'")
+
+    # -- tables ------------------------------------------------------------------
+    def set_range_shift(self, range_shift=None):
+        """(Re)build the depth tables on the device at CSDA ranges R0_l + range_shift_l."""
+        torch = self.torch
+        g = self.problem.grid
+        if range_shift is not None:
+            rs = torch.as_tensor(range_shift, dtype=torch.float64, device=self.device).reshape(-1)
+            if self.range_shift is not None and torch.equal(rs, self.range_shift):
+                return
+        elif self.range_shift is None and getattr(self, "idd", None) is not None:
+            return
+        t = ph.build_tables(g.nz, g.oz, g.dz, self.energies, range_shift=range_shift,
+                            fd_step=self.fd_step, device=self.device)
+        self.idd, self.sigma, self.didd, self.dsig = t.idd, t.sigma, t.didd_dr, t.dsigma_dr
+        self.range_shift = None if range_shift is None else rs.clone()
+
+    def active_pairs(self) -> int:
+        return int((self.idd != 0).sum().item())
+
+    # -- weights -----------------------------------------------------------------
+    def _weights(self, w):
+        torch = self.torch
+        if w is None:
+            return self.w
+        if not torch.is_tensor(w):
+            w = torch.as_tensor(np.asarray(w, dtype=np.float32))
+        if w.device != self.device:
+            w = w.to(self.device, non_blocking=True)
+        return w.to(torch.float32).contiguous()
+
+    # -- forward -------------------------------------------------------------------
+    def forward(self, w=None, out=None, idd=None, sigma=None):
+        torch = self.torch
+        w = self._weights(w)
+        idd = self.idd if idd is None else idd
+        sigma = self.sigma if sigma is None else sigma
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        nbytes = _lib.query("pbd_forward_workspace", ctypes.byref(self.field), self.precision)
+        ws = self.ws.get("fwd", nbytes)
+        _lib.call("pbd_forward", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(idd),
+                  _lib.ptr(sigma), _lib.ptr(out), self.precision, _lib.ptr(ws), ws.numel(),
+                  _lib.stream_handle(self.device))
+        return out
+
+    # -- adjoint -------------------------------------------------------------------
+    def adjoint(self, grad_dose, w=None, idd=None, sigma=None, didd=None, dsig=None,
+                with_range: bool = True):
+        torch = self.torch
+        w = self._weights(w)
+        idd = self.idd if idd is None else idd
+        sigma = self.sigma if sigma is None else sigma
+        didd = self.didd if didd is None else didd
+        dsig = self.dsig if dsig is None else dsig
+        with_range = with_range and didd is not None and dsig is not None
+        g = grad_dose.to(self.device, torch.float32).contiguous()
+        gw = torch.empty_like(w)
+        gr = torch.zeros(w.shape[0], dtype=torch.float32, device=self.device) if with_range else None
+        nbytes = _lib.query("pbd_adjoint_workspace", ctypes.byref(self.field), self.precision)
+        ws = self.ws.get("adj", nbytes)
+        _lib.call("pbd_adjoint", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(idd),
+                  _lib.ptr(sigma), _lib.ptr(didd if with_range else None),
+                  _lib.ptr(dsig if with_range else None), _lib.ptr(g), _lib.ptr(gw),
+                  _lib.ptr(gr), self.precision, _lib.ptr(ws), ws.numel(),
+                  _lib.stream_handle(self.device))
+        return gw, gr
+
+    # -- fused loss gradient -------------------------------------------------------
+    def loss_grad(self, mask, presc, w=None, outputs=None):
+        """L = sum m (D - P)^2 and its gradients in one library call.
+
+        Returns a dict of device tensors: loss (float64 scalar), dose, grad_dose,
+        grad_w, grad_range (None when the plan has no range-derivative tables)."""
+        torch = self.torch
+        w = self._weights(w)
+        o = outputs or self.alloc_outputs()
+        with_range = self.didd is not None
+        nbytes = _lib.query("pbd_loss_grad_workspace", ctypes.byref(self.field), self.precision)
+        ws = self.ws.get("lossgrad", nbytes)
+        _lib.call("pbd_loss_grad", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(self.idd),
+                  _lib.ptr(self.sigma), _lib.ptr(self.didd if with_range else None),
+                  _lib.ptr(self.dsig if with_range else None), _lib.ptr(mask), _lib.ptr(presc),
+                  _lib.ptr(o["dose"]), _lib.ptr(o["grad_dose"]), _lib.ptr(o["loss"]),
+                  _lib.ptr(o["grad_w"]), _lib.ptr(o["grad_range"] if with_range else None),
+                  self.precision, _lib.ptr(ws), ws.numel(), _lib.stream_handle(self.device))
+        if not with_range:
+            o = dict(o, grad_range=None)
+        return o
+
+    def alloc_outputs(self):
+        torch = self.torch
+        nl = self.w.shape[0]
+        return {"dose": torch.empty(self.shape, dtype=torch.float32, device=self.device),
+                "grad_dose": torch.empty(self.shape, dtype=torch.float32, device=self.device),
+                "loss": torch.zeros((), dtype=torch.float64, device=self.device),
+                "grad_w": torch.empty_like(self.w),
+                "grad_range": torch.zeros(nl, dtype=torch.float32, device=self.device)}
+
+
+def _autograd_function():
+    torch = _lib.require_cuda()
+
+    class SeparableDose(torch.autograd.Function):
+        """D(w, range_shift) with a hand-written backward (the adjoint kernel)."""
+
+        @staticmethod
+        def forward(ctx, w, range_shift, plan):
+            if range_shift is not None:
+                plan.set_range_shift(range_shift.detach())
+            dose = plan.forward(w)
+            ctx.plan = plan
+            ctx.tables = (plan.idd, plan.sigma, plan.didd, plan.dsig)
+            ctx.has_shift = range_shift is not None
+            ctx.shift_dtype = None if range_shift is None else range_shift.dtype
+            ctx.save_for_backward(w)
+            return dose
+
+        @staticmethod
+        def backward(ctx, grad_dose):
+            (w,) = ctx.saved_tensors
+            idd, sig, didd, dsig = ctx.tables
+            need_r = ctx.has_shift and ctx.needs_input_grad[1]
+            gw, gr = ctx.plan.adjoint(grad_dose, w, idd, sig, didd, dsig, with_range=need_r)
+            gr = gr.to(ctx.shift_dtype) if (need_r and gr is not None) else None
+            return gw, gr, None
+
+    return SeparableDose
+
+
+_SEPARABLE_DOSE = None
+
+
+def separable_dose(w, range_shift, plan: DosePlan):
+    """Differentiable dose D(w, range_shift); gradients through the CUDA adjoint."""
+    global _SEPARABLE_DOSE
+    if _SEPARABLE_DOSE is None:
+        _SEPARABLE_DOSE = _autograd_function()
+    return _SEPARABLE_DOSE.apply(w, range_shift, plan)
+
+
+def torch_separable(problem: PBProblem, device: str = "cuda", dtype=None, allow_tf32: bool = False,
+                    per_layer: bool = True, layer_chunk: Optional[int] = None,
+                    return_timing: bool = False, return_intermediates: bool = False,
+                    precision: Optional[str] = None):
+    """Drop-in for the reference's per-layer batched-matmul engine (engines.py:208-283).
+
+    Same arguments and return value: a float32 CUDA tensor D of shape (nz, ny, nx), or
+    (D, seconds) with ``return_timing``.  Like the reference it uploads the problem's
+    arrays on every call and synchronises before returning.  Differences, all loud:
+    ``device`` must be CUDA (no CPU path), ``dtype`` must be float32 (the contraction
+    is FP32 or a split tensor-core form, within 1e-6 of FP64), and ``per_layer=False``
+    (the single-sigma approximation) is not provided.  ``allow_tf32=True`` selects
+    plain TF32 tensor cores; ``precision`` picks any mode explicitly; ``layer_chunk``
+    sets the layers per work item."""
+    torch = _lib.require_cuda()
+    if not str(device).startswith("cuda"):
+        raise RuntimeError("torch_separable: this engine runs on CUDA only (no CPU path)")
+    if dtype not in (None, torch.float32):
+        raise NotImplementedError("torch_separable: the device contraction returns float32")
+    if not per_layer:
+        raise NotImplementedError("torch_separable: the single-sigma approximation "
+                                  "(per_layer=False) is not provided; use per_layer=True")
+    prec = precision or ("tf32" if allow_tf32 else DEFAULT_PRECISION)
+    t0 = time.perf_counter()
+    if layer_chunk:
+        _lib.call("pbd_set_schedule", int(layer_chunk), 0)
+    try:
+        plan = DosePlan(problem, precision=prec, tables="problem", device=device)
+        dose = plan.forward()
+        torch.cuda.synchronize(plan.device)
+    finally:
+        if layer_chunk:
+            _lib.call("pbd_set_schedule", 0, 0)
+    t1 = time.perf_counter()
+    return (dose, t1 - t0) if return_timing else dose

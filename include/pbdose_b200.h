@@ -1,0 +1,177 @@
+/*
+ * pbdose_b200.h -- C ABI of the B200 (sm_100a) separable proton pencil-beam dose engine.
+ *
+ * Dose model (per-energy-layer exact separable pencil beam, water):
+ *
+ *   D[z,y,x] = sum_l IDD_l(z) * sum_{j,i} Gy_l(z)[y,j] * W_l[j,i] * Gx_l(z)[x,i]
+ *   Gx_l(z)[x,i] = exp(-(x_v - xs_i)^2 / (2 s^2)) / (sqrt(2 pi) s),  s = sigma_l(z)
+ *
+ * Conventions (the same as the reference's Python engine, engines.py:208-283):
+ *   - dose is (nz, ny, nx), x innermost; voxel centres x_v = ox + k*dx (model.py:7-9, 48-52);
+ *   - weights are (L, nsy, nsx) float32; spot centres xs_i = x0 + (i - (nsx-1)/2)*dx_spot
+ *     (model.py:106-113);
+ *   - depth tables idd, sigma are (L, nz) float64, row l = energy layer, column k = voxel
+ *     slice k (model.py:137-151).
+ *
+ * Every entry point validates its arguments first, returns 0 (PBD_OK) or a negative
+ * PBD_ERR_* code readable with pbd_strerror(), never exits the process and never throws
+ * across the ABI (the reference's ABI rules, pencil_beam.cu:647-730).  All array pointers
+ * are DEVICE pointers unless stated otherwise.  Work is enqueued on `stream` (a
+ * cudaStream_t passed as void*; NULL = legacy default stream) and is asynchronous: the
+ * caller synchronises.  The caller owns all memory; scratch comes from the caller's
+ * `workspace`, sized by the matching *_workspace() query.
+ */
+#ifndef PBDOSE_B200_H
+#define PBDOSE_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define PBD_API __attribute__((visibility("default")))
+#else
+#define PBD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes; pencil_beam.cu:647-653 (same values for the shared meanings). */
+#define PBD_OK                0
+#define PBD_ERR_NULL_ARG     -1
+#define PBD_ERR_BAD_DIM      -2
+#define PBD_ERR_BAD_VALUE    -3   /* NaN / non-positive sigma, spacing or step */
+#define PBD_ERR_CUDA         -4
+#define PBD_ERR_UNSUPPORTED  -5
+#define PBD_ERR_NO_SMEM      -6
+#define PBD_ERR_WORKSPACE    -7   /* workspace missing or smaller than the query result */
+#define PBD_ERR_TIMEOUT      -8   /* a bounded device-side wait ran out; results invalid */
+#define PBD_ERR_TOO_MANY     -9   /* more jobs than PBD_MAX_JOBS in one launch */
+
+/* Arithmetic used for the two Gaussian contractions.  All accumulate in FP32. */
+#define PBD_PREC_FP32    0   /* FP32 FMA on the CUDA cores */
+#define PBD_PREC_TF32X3  1   /* tcgen05 TF32, hi/lo split, three products */
+#define PBD_PREC_TF32    2   /* tcgen05 TF32, one product */
+#define PBD_PREC_BF16X3  3   /* tcgen05 BF16, hi/lo split, three products */
+#define PBD_PREC_BF16    4   /* tcgen05 BF16, one product */
+
+#define PBD_MAX_JOBS 128     /* jobs (fields x scenarios) per batched launch */
+
+/* One field: dose grid (DoseGrid, model.py:27-38) + spot lattice (SpotLattice,
+ * model.py:85-100).  Host memory, read during the call only. */
+typedef struct pbd_field {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double ox, oy, oz;
+    int n_sx, n_sy, n_layers;
+    double dx_spot, dy_spot;
+    double x0, y0;
+} pbd_field;
+
+/* Parameters of the depth-LUT builder (physics.py:221-387 with the defaults of
+ * IDDModel, physics.py:292-308, and fermi_eyges_moments).  The tables are built at the
+ * water-equivalent depths d_k = depth_scale * (z0 + k*dz), k < nz.  depth_scale = 1 and
+ * z0 = the grid's oz give exactly the reference's tables; other values model a
+ * depth shift (z0 = oz - shift) or a stopping-power scaling (depth_scale = s, in which
+ * case B is divided by s^2 to return to physical lateral units). */
+typedef struct pbd_lut_spec {
+    int nz;
+    double z0, dz, depth_scale;
+    int anchor_surface;                    /* 0: scattering integral starts at the first depth
+                                              (reference semantics); 1: starts at depth 0 and
+                                              depths <= 0 get sigma_x0 and IDD 0 */
+    double sigma_x0, sigma_theta0, rho0;   /* initial beam phase space, cm / rad */
+    int fe_n_sub;                          /* fine-grid subdivision (4) */
+    double fe_max_step;                    /* fine-grid max step, cm (0.02) */
+    int straggling_model;                  /* 0 bohr, 1 icru49, 2 none */
+    double strag_coef, strag_exp;          /* icru49: coef * R0^exp */
+    double energy_spread;                  /* relative 1-sigma (0.0033) */
+    double atten_len;                      /* nuclear attenuation length, cm (150) */
+    int idd_n_fine;                        /* CSDA binning points (6000) */
+    double fd_step;                        /* range step of the derivative tables, cm; 0 = none */
+} pbd_lut_spec;
+
+/* One job of a batched launch: a field, its device arrays and its outputs. */
+typedef struct pbd_job {
+    pbd_field field;
+    const float *w;          /* (L, nsy, nsx) */
+    const double *idd;       /* (L, nz) */
+    const double *sigma;     /* (L, nz) */
+    float *dose;             /* (nz, ny, nx) out */
+} pbd_job;
+
+/* ---- utilities --------------------------------------------------------------- */
+/* Replaces pb_strerror, pencil_beam.cu:687-699. Never NULL. */
+PBD_API const char *pbd_strerror(int code);
+/* ABI version, major*10000 + minor*100 + patch. */
+PBD_API int pbd_version(void);
+/* Validates a field descriptor; replaces pb_problem_validate, pencil_beam.cu:717-730. */
+PBD_API int pbd_field_validate(const pbd_field *f);
+/* Work-item granularity of the calling host thread's subsequent calls (0 = built-in
+ * default): energy layers per forward item, depth slices per adjoint item.  The
+ * workspace queries use the same setting, so set it before sizing.  No counterpart in
+ * the reference (it plays the role of engines.torch_separable's layer_chunk knob). */
+PBD_API int pbd_set_schedule(int fwd_layers_per_item, int adj_depths_per_item);
+/* Measurement utilities (no counterpart in the reference).  Between begin and end, the
+ * calling thread's forward and adjoint calls record CUDA events around their main dose
+ * kernel; end() waits for them and returns the summed kernel time (ms) and the number
+ * of launches of each.  Not for use inside stream capture. */
+PBD_API int pbd_profile_begin(void);
+PBD_API int pbd_profile_end(double *fwd_ms, int *n_fwd, double *adj_ms, int *n_adj);
+/* Number of kernels this library has launched from the calling thread so far. */
+PBD_API int pbd_launch_count(long long *n);
+
+/* ---- depth-LUT builder (FP64, on the device) -------------------------------------
+ * Replaces the per-layer host loop of model.py:225-233 (physics.idd_pristine with
+ * normalize=False and physics.fermi_eyges_moments(...)["sigma_x"]).
+ * energies: (L) MeV; range_shift: (L) cm or NULL (layer l is built at the CSDA range
+ * R0_l + range_shift_l); outputs idd, sigma (L, nz); didd_dr, dsigma_dr (L, nz) central
+ * differences in range with step spec->fd_step (may be NULL when fd_step == 0). */
+PBD_API int pbd_lut_workspace(const pbd_lut_spec *spec, int n_layers, size_t *bytes);
+PBD_API int pbd_build_luts(const pbd_lut_spec *spec, int n_layers, const double *energies,
+                   const double *range_shift, double *idd, double *sigma,
+                   double *didd_dr, double *dsigma_dr,
+                   void *workspace, size_t workspace_bytes, void *stream);
+/* CSDA range table lookups (physics.py:130-139), elementwise on device arrays. */
+PBD_API int pbd_csda_range(const double *energy, double *range_cm, int n, void *stream);
+PBD_API int pbd_energy_from_range(const double *range_cm, double *energy, int n, void *stream);
+
+/* ---- forward dose -----------------------------------------------------------------
+ * Replaces engines.torch_separable(per_layer=True), engines.py:208-283, and the
+ * reference ABI's pb_dose_forward_separable, pencil_beam.cu:799-851. */
+PBD_API int pbd_forward_workspace(const pbd_field *f, int precision, size_t *bytes);
+PBD_API int pbd_forward(const pbd_field *f, const float *w, const double *idd, const double *sigma,
+                float *dose, int precision, void *workspace, size_t workspace_bytes,
+                void *stream);
+
+/* ---- adjoint (no counterpart in the reference, which has no gradient) --------------
+ * Given grad_dose = dL/dD (nz, ny, nx), writes grad_w = dL/dW (L, nsy, nsx) and
+ * grad_range = dL/d(range shift) (L), the latter through didd_dr and dsigma_dr
+ * (either may be NULL together with grad_range == NULL to skip it). */
+PBD_API int pbd_adjoint_workspace(const pbd_field *f, int precision, size_t *bytes);
+PBD_API int pbd_adjoint(const pbd_field *f, const float *w, const double *idd, const double *sigma,
+                const double *didd_dr, const double *dsigma_dr, const float *grad_dose,
+                float *grad_w, float *grad_range, int precision,
+                void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- fused plan-loss gradient evaluation --------------------------------------------
+ * L = sum_v mask_v (D_v - presc_v)^2.  Writes dose, grad_dose = 2 mask (D - presc),
+ * loss (device float64 scalar), grad_w and grad_range, in one call. */
+PBD_API int pbd_loss_grad_workspace(const pbd_field *f, int precision, size_t *bytes);
+PBD_API int pbd_loss_grad(const pbd_field *f, const float *w, const double *idd, const double *sigma,
+                  const double *didd_dr, const double *dsigma_dr,
+                  const float *mask, const float *presc,
+                  float *dose, float *grad_dose, double *loss, float *grad_w, float *grad_range,
+                  int precision, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- batched forward: several fields / scenarios in one persistent launch ----------
+ * jobs: HOST array of n_jobs <= PBD_MAX_JOBS descriptors (copied into the launch's
+ * parameters; may be freed on return). */
+PBD_API int pbd_forward_batch_workspace(const pbd_job *jobs, int n_jobs, int precision, size_t *bytes);
+PBD_API int pbd_forward_batch(const pbd_job *jobs, int n_jobs, int precision,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBDOSE_B200_H */

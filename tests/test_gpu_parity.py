@@ -1,0 +1,327 @@
+"""GPU parity of the CUDA path against the oracle (tests/golden + oracle/).
+
+Tolerances (written here, not tuned per run):
+  * depth tables (FP64 device builder) vs the reference's NumPy: 1e-9 of the table max;
+  * dose, FP32 path: max |dD| / max D <= 1e-6 against the float64 oracle;
+  * gradients: dL/dW within 1e-4 (relative to max |g|) of float64 autograd through the
+    oracle's separable engine; dL/dR within 1e-4 of float64 central differences.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import golden, has_gpu, load_pkg
+from oracle import engine_ref as er
+from oracle import physics_ref as pr
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")]
+
+DOSE_TOL = 1e-6
+GRAD_TOL = 1e-4
+LUT_TOL = 1e-9
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def pb():
+    return load_pkg()
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+def axes(prob):
+    return prob.grid.x, prob.grid.y, prob.lattice.spot_x, prob.lattice.spot_y
+
+
+# ----------------------------------------------------------------------- LUT builder
+@pytest.mark.parametrize("cfg", [0, 1, 4])
+def test_device_luts_match_reference(pb, cfg):
+    g = golden(f"luts_cfg{cfg}.npz")
+    t = pb.physics.build_tables(len(g["z"]), g["z"][0], g["z"][1] - g["z"][0], g["energies"])
+    assert rel(t.idd.cpu().numpy(), g["idd"]) < LUT_TOL
+    assert rel(t.sigma.cpu().numpy(), g["sigma"]) < LUT_TOL
+
+
+def test_device_range_lookups(pb):
+    g = golden("physics.npz")
+    assert rel(pb.physics.csda_range(g["e_q"]), g["csda_q"]) < 1e-13
+    assert rel(pb.physics.energy_from_range(g["r_q"]), g["efr_q"]) < 1e-13
+
+
+def test_device_idd_fine_axis(pb):
+    """IDD on the reference's 0.02 cm axis at 100 and 200 MeV (convolution vs FFT)."""
+    g = golden("physics.npz")
+    z = g["idd_z"]
+    t = pb.physics.build_tables(len(z), z[0], 0.02, g["idd_e"])
+    assert rel(t.idd.cpu().numpy(), g["idd"]) < LUT_TOL
+
+
+def test_range_derivative_tables(pb):
+    g = golden("luts_cfg0.npz")
+    h = 0.005
+    z = g["z"]
+    t = pb.physics.build_tables(len(z), z[0], z[1] - z[0], g["energies"], fd_step=h)
+    ip, sp = pr.layer_luts(z, g["energies"], range_shift=np.full(len(g["energies"]), h))
+    im, sm = pr.layer_luts(z, g["energies"], range_shift=np.full(len(g["energies"]), -h))
+    assert rel(t.didd_dr.cpu().numpy(), (ip - im) / (2 * h)) < 1e-6
+    assert rel(t.dsigma_dr.cpu().numpy(), (sp - sm) / (2 * h)) < 1e-6
+
+
+def test_scenario_luts(pb):
+    z0, dz, nz = 0.0 - 0.3, 0.2, 64
+    en = pr.layer_energies(8, 4.0, 9.0)
+    for s in (0.965, 1.0, 1.035):
+        t = pb.physics.build_tables(nz, z0, dz, en, depth_scale=s, anchor_surface=True)
+        ri, rs = pr.scenario_luts(z0, dz, nz, en, depth_scale=s)
+        assert rel(t.idd.cpu().numpy(), ri) < LUT_TOL
+        assert rel(t.sigma.cpu().numpy(), rs) < LUT_TOL
+
+
+# ----------------------------------------------------------------------- forward
+def test_forward_cfg0_vs_reference_dose(pb):
+    wl = pb.workloads.build_workload(0)
+    lut = golden("luts_cfg0.npz")
+    prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
+    d = pb.engines.torch_separable(prob, "cuda")
+    assert d.shape == (64, 32, 32) and str(d.dtype) == "torch.float32"
+    assert rel(d.cpu().numpy(), golden("dose_cfg0.npz")["dose"]) < DOSE_TOL
+
+
+def test_forward_engine_check_case(pb):
+    g = golden("engine_check.npz")
+    M = pb.model
+    grid = M.DoseGrid(24, 24, 32, 0.25, 0.25, 0.25, -3.0, -3.0, 0.0)
+    lat = M.SpotLattice(3, 3, 3, 0.5, 0.5, energies=g["energies"], weights=g["w"])
+    prob = M.PBProblem(grid, lat, g["idd"], g["sigma"])
+    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    assert rel(d, g["dose_naive"]) < DOSE_TOL
+    assert rel(d, g["dose_sep"]) < DOSE_TOL
+
+
+@pytest.mark.slow
+def test_forward_cfg1_clinical(pb):
+    wl = pb.workloads.build_workload(1)
+    lut = golden("luts_cfg1.npz")
+    prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
+    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    ref = golden("dose_cfg1_slices.npz")
+    assert rel(d[ref["k"]], ref["slices"]) <= DOSE_TOL * ref["dmax"] / np.max(np.abs(ref["slices"]))
+    full = er.separable_torch(*axes(prob), wl["weights"], lut["idd"], lut["sigma"]).numpy()
+    assert rel(d, full) < DOSE_TOL
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1, 1, 1, 1), (150, 70, 33, 70, 13, 5),
+                                   (37, 129, 9, 5, 66, 3), (200, 200, 3, 61, 61, 2)])
+def test_forward_ragged_and_chunked(pb, shape):
+    """Odd grids (not multiples of the 128 tile), lattices over the 64-spot chunk, 1x1x1."""
+    nx, ny, nz, nsx, nsy, nl = shape
+    rng = np.random.default_rng(sum(shape))
+    M = pb.model
+    grid = M.DoseGrid(nx, ny, nz, 0.15, 0.2, 0.3, -(nx - 1) * 0.075, -(ny - 1) * 0.1, 0.0)
+    w = rng.uniform(0.1, 1.0, (nl, nsy, nsx))
+    lat = M.SpotLattice(nsx, nsy, nl, 0.25, 0.3, x0=0.07, y0=-0.11, weights=w)
+    idd = rng.uniform(0.0, 5.0, (nl, nz))
+    idd[rng.random((nl, nz)) < 0.3] = 0.0     # inactive (layer, slice) pairs
+    sig = rng.uniform(0.2, 0.8, (nl, nz))
+    prob = M.PBProblem(grid, lat, idd, sig)
+    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    ref = er.separable_f64(grid.x, grid.y, lat.spot_x, lat.spot_y, w, idd, sig)
+    if np.max(np.abs(ref)) == 0:
+        assert np.all(d == 0)
+    else:
+        assert rel(d, ref) < DOSE_TOL
+
+
+def test_forward_all_layers_inactive(pb):
+    M = pb.model
+    grid = M.DoseGrid(20, 20, 10, 0.2, 0.2, 0.2, -1.9, -1.9, 0.0)
+    lat = M.SpotLattice(5, 5, 2, 0.5, 0.5, weights=np.ones((2, 5, 5)))
+    prob = M.PBProblem(grid, lat, np.zeros((2, 10)), np.full((2, 10), 0.4))
+    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    assert np.all(d == 0.0)
+
+
+def test_device_tables_end_to_end_cfg0(pb):
+    """Device LUT builder + kernel against the reference's own float64 dose."""
+    wl = pb.workloads.build_workload(0)
+    prob = pb.model.problem_from_workload(wl)
+    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    assert rel(d, golden("dose_cfg0.npz")["dose"]) < DOSE_TOL
+
+
+def test_layer_chunk_and_schedule_invariance(pb):
+    wl = pb.workloads.build_workload(0)
+    lut = golden("luts_cfg0.npz")
+    prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
+    base = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    for c in (1, 3, 8):
+        d = pb.engines.torch_separable(prob, "cuda", layer_chunk=c).cpu().numpy()
+        assert rel(d, base) < 1e-6
+
+
+def test_api_errors(pb, torch):
+    wl = pb.workloads.build_workload(0)
+    lut = golden("luts_cfg0.npz")
+    prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
+    with pytest.raises(RuntimeError):
+        pb.engines.torch_separable(prob, "cpu")
+    with pytest.raises(NotImplementedError):
+        pb.engines.torch_separable(prob, "cuda", per_layer=False)
+    with pytest.raises(NotImplementedError):
+        pb.engines.torch_separable(prob, "cuda", dtype=torch.float64)
+    d, t = pb.engines.torch_separable(prob, "cuda", return_timing=True)
+    assert t > 0 and d.is_cuda
+
+
+# ----------------------------------------------------------------------- adjoint
+def _loss_oracle(prob, w, idd, sig, mask, presc):
+    import torch
+    wt = torch.tensor(np.asarray(w, np.float64), requires_grad=True)
+    d = er.separable_torch(*axes(prob), wt, idd, sig)
+    loss = er.masked_quadratic_loss(d, torch.as_tensor(mask, dtype=torch.float64),
+                                    torch.as_tensor(presc, dtype=torch.float64))
+    loss.backward()
+    return float(loss), d.detach().numpy(), wt.grad.numpy()
+
+
+def test_loss_grad_cfg0_vs_autograd(pb, torch):
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    plan = pb.engines.DosePlan(prob, tables="device")
+    mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
+    presc = presc * 100.0
+    out = plan.loss_grad(torch.as_tensor(mask, device="cuda"), torch.as_tensor(presc, device="cuda"))
+    idd, sig = plan.idd.cpu().numpy(), plan.sigma.cpu().numpy()
+    loss, d, gw = _loss_oracle(prob, wl["weights"], idd, sig, mask, presc)
+    assert rel(out["dose"].cpu().numpy(), d) < DOSE_TOL
+    assert abs(out["loss"].item() - loss) / abs(loss) < 1e-5
+    assert rel(out["grad_w"].cpu().numpy(), gw) < GRAD_TOL
+    # the stand-alone adjoint on the same dL/dD agrees with the fused path
+    gw2, gr2 = plan.adjoint(out["grad_dose"])
+    assert rel(gw2.cpu().numpy(), out["grad_w"].cpu().numpy()) < 1e-6
+    assert rel(gr2.cpu().numpy(), out["grad_range"].cpu().numpy()) < 1e-6
+
+
+def test_range_gradient_vs_fd_cfg0(pb, torch):
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    plan = pb.engines.DosePlan(prob, tables="device")
+    mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
+    presc = presc * 100.0
+    out = plan.loss_grad(torch.as_tensor(mask, device="cuda"), torch.as_tensor(presc, device="cuda"))
+    gr = out["grad_range"].cpu().numpy().astype(np.float64)
+    h = 0.005
+    fd = np.zeros(len(en))
+    for l in range(len(en)):
+        vals = []
+        for sgn in (1.0, -1.0):
+            shift = np.zeros(len(en))
+            shift[l] = sgn * h
+            idd, sig = pr.layer_luts(prob.grid.z, en, range_shift=shift)
+            d = er.separable_torch(*axes(prob), wl["weights"], idd, sig).numpy()
+            vals.append(float(er.masked_quadratic_loss(d, mask, presc)))
+        fd[l] = (vals[0] - vals[1]) / (2 * h)
+    assert np.max(np.abs(gr - fd)) / np.max(np.abs(fd)) < GRAD_TOL
+
+
+def test_autograd_function(pb, torch):
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    plan = pb.engines.DosePlan(prob, tables="device")
+    w = torch.tensor(wl["weights"], device="cuda", requires_grad=True)
+    dr = torch.zeros(len(en), dtype=torch.float64, device="cuda", requires_grad=True)
+    d = pb.engines.separable_dose(w, dr, plan)
+    mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
+    m = torch.as_tensor(mask, device="cuda")
+    p = torch.as_tensor(presc, device="cuda") * 100
+    loss = (m * (d - p) ** 2).sum()
+    loss.backward()
+    out = plan.loss_grad(m, p)
+    assert rel(w.grad.cpu().numpy(), out["grad_w"].cpu().numpy()) < 1e-5
+    assert rel(dr.grad.cpu().numpy(), out["grad_range"].cpu().numpy()) < 1e-5
+
+
+@pytest.mark.slow
+def test_clinical_fd_checks_cfg2(pb, torch):
+    """Config 2: gradients wrt 64 sampled spot weights (step 1e-3) and 8 layer range
+    shifts (step 0.05 mm), central differences in float64 through the oracle."""
+    wl = pb.workloads.build_workload(2)
+    lut = golden("luts_cfg1.npz")
+    en = lut["energies"]
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    plan = pb.engines.DosePlan(prob, tables="device")
+    m = torch.as_tensor(wl["mask"], device="cuda")
+    p = torch.as_tensor(wl["presc"], device="cuda")
+    out = plan.loss_grad(m, p)
+    gw = out["grad_w"].cpu().numpy().astype(np.float64)
+    gr = out["grad_range"].cpu().numpy().astype(np.float64)
+    idd, sig = plan.idd.cpu().numpy(), plan.sigma.cpu().numpy()
+    assert rel(idd, lut["idd"]) < LUT_TOL
+    spots, layers = pb.workloads.fd_sample(wl)
+    w0 = wl["weights"].astype(np.float64)
+    ax = axes(prob)
+    mask, presc = wl["mask"].astype(np.float64), wl["presc"].astype(np.float64)
+
+    def loss_w(wv, i_, s_):
+        d = er.separable_torch(*ax, wv, i_, s_).numpy()
+        return float(er.masked_quadratic_loss(d, mask, presc))
+
+    # weights: the loss is quadratic in w, so the central difference is exact up to
+    # rounding; the tolerance is relative to the largest sampled gradient
+    fdw = []
+    for (l, j, i) in spots:
+        wp, wm = w0.copy(), w0.copy()
+        wp[l, j, i] += 1e-3
+        wm[l, j, i] -= 1e-3
+        fdw.append((loss_w(wp, idd, sig) - loss_w(wm, idd, sig)) / 2e-3)
+    fdw = np.array(fdw)
+    gsel = gw[spots[:, 0], spots[:, 1], spots[:, 2]]
+    assert np.max(np.abs(gsel - fdw)) / np.max(np.abs(fdw)) < GRAD_TOL
+    h = 0.005
+    fdr = []
+    for l in layers:
+        vals = []
+        for sgn in (1.0, -1.0):
+            shift = np.zeros(len(en))
+            shift[l] = sgn * h
+            i_, s_ = pr.layer_luts(prob.grid.z, en, range_shift=shift)
+            vals.append(loss_w(w0, i_, s_))
+        fdr.append((vals[0] - vals[1]) / (2 * h))
+    fdr = np.array(fdr)
+    assert np.max(np.abs(gr[layers] - fdr)) / np.max(np.abs(fdr)) < GRAD_TOL
+
+
+# ----------------------------------------------------------------------- batch
+def test_scenario_batch_matches_single(pb, torch):
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    scen = [(0, 0, 0, 1.0), (0.3, -0.3, 0.3, 1.035), (-0.3, 0.0, -0.3, 0.965)]
+    b = pb.robust.ScenarioBatch([prob], scen)
+    b.run()
+    torch.cuda.synchronize()
+    doses = [d.clone() for d in b.doses]
+    g = prob.grid
+    for k, (sx, sy, sz, s) in enumerate(scen):
+        idd, sig = pr.scenario_luts(g.oz - sz, g.dz, g.nz, en, depth_scale=s)
+        xs = prob.lattice.spot_x + sx
+        ys = prob.lattice.spot_y + sy
+        ref = er.separable_f64(g.x, g.y, xs, ys, wl["weights"], idd, sig)
+        assert rel(doses[k].cpu().numpy(), ref) < DOSE_TOL
+    replay = [d.clone() for d in b.replay()]
+    torch.cuda.synchronize()
+    for d0, d1 in zip(doses, replay):
+        assert torch.equal(d0, d1)

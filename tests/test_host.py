@@ -1,0 +1,161 @@
+"""Host-side tests (no GPU): the C ABI library loads and exports every declared symbol,
+argument validation returns the documented codes before any device work, and the
+workload / model host logic matches the reference's conventions."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO, has_gpu, load_pkg
+
+HEADER = os.path.join(REPO, "include", "pbdose_b200.h")
+
+
+@pytest.fixture(scope="module")
+def pb():
+    return load_pkg()
+
+
+@pytest.fixture(scope="module")
+def lib(pb):
+    if not os.path.exists(pb._lib.LIB_PATH):
+        pytest.skip("library not built")
+    return pb._lib.load()
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"PBD_API\s+[\w\s\*]*?\b(pbd_\w+)\s*\(", txt)))
+
+
+def test_every_declared_symbol_is_exported_and_bound(pb, lib):
+    decl = declared_symbols()
+    assert len(decl) >= 15
+    for name in decl:
+        assert hasattr(lib, name), name
+    assert sorted(pb._lib.exported_symbols()) == decl
+
+
+def field(pb, **kw):
+    f = dict(nx=32, ny=32, nz=64, dx=0.2, dy=0.2, dz=0.2, ox=-3.1, oy=-3.1, oz=0.0, n_sx=11,
+             n_sy=11, n_layers=8, dx_spot=0.5, dy_spot=0.5, x0=0.0, y0=0.0)
+    f.update(kw)
+    return pb._lib.Field(**f)
+
+
+def test_field_validation_codes(pb, lib):
+    assert lib.pbd_field_validate(ctypes.byref(field(pb))) == 0
+    assert lib.pbd_field_validate(None) == -1
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, nx=0))) == -2
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, n_layers=-1))) == -2
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, dx=float("nan")))) == -3
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, dx_spot=0.0))) == -3
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, n_sx=5000))) == -5
+    for code in range(-12, 1):
+        assert lib.pbd_strerror(code)
+
+
+def test_entry_points_validate_before_device_work(pb, lib):
+    f = field(pb)
+    sz = ctypes.c_size_t(0)
+    assert lib.pbd_forward_workspace(ctypes.byref(f), 0, ctypes.byref(sz)) == 0 and sz.value > 0
+    assert lib.pbd_forward_workspace(ctypes.byref(f), 99, ctypes.byref(sz)) == -3
+    fake = 0x1000
+    # null arrays, missing / short workspace -> errors, and nothing launched
+    assert lib.pbd_forward(ctypes.byref(f), None, fake, fake, fake, 0, fake, 1 << 30, None) == -1
+    assert lib.pbd_forward(ctypes.byref(f), fake, fake, fake, fake, 0, None, 0, None) == -7
+    assert lib.pbd_forward(ctypes.byref(f), fake, fake, fake, fake, 0, fake, 16, None) == -7
+    assert lib.pbd_adjoint(ctypes.byref(f), fake, fake, fake, fake, fake, fake, fake, fake, 0,
+                           None, 0, None) == -7
+    big = field(pb, n_sx=65)
+    assert lib.pbd_adjoint_workspace(ctypes.byref(big), 0, ctypes.byref(sz)) == -5
+    assert lib.pbd_loss_grad(ctypes.byref(f), fake, fake, fake, None, None, fake, fake, fake, fake,
+                             fake, fake, fake, 0, None, 0, None) == -1
+    assert lib.pbd_set_schedule(65, 0) == -3
+    assert lib.pbd_set_schedule(0, 0) == 0
+
+
+def test_batch_limits(pb, lib):
+    jobs = (pb._lib.Job * 129)()
+    for k in range(129):
+        jobs[k].field = field(pb)
+    sz = ctypes.c_size_t(0)
+    assert lib.pbd_forward_batch_workspace(jobs, 129, 0, ctypes.byref(sz)) == -9
+    assert lib.pbd_forward_batch_workspace(jobs, 0, 0, ctypes.byref(sz)) == -2
+    assert lib.pbd_forward_batch_workspace(jobs, 4, 0, ctypes.byref(sz)) == 0
+    assert lib.pbd_forward_batch(jobs, 4, 0, ctypes.c_void_p(0x1000), sz.value, None) == -1
+
+
+def test_lut_spec_validation(pb, lib):
+    s = pb.physics.lut_spec(64, 0.0, 0.2)
+    sz = ctypes.c_size_t(0)
+    assert lib.pbd_lut_workspace(ctypes.byref(s), 8, ctypes.byref(sz)) == 0 and sz.value > 0
+    bad = pb.physics.lut_spec(64, 0.0, -0.2)
+    assert lib.pbd_lut_workspace(ctypes.byref(bad), 8, ctypes.byref(sz)) == -3
+    assert lib.pbd_lut_workspace(ctypes.byref(s), 0, ctypes.byref(sz)) == -2
+    with pytest.raises(ValueError):
+        pb.physics.lut_spec(64, 0.0, 0.2, idd_model=pb.physics.IDDModel(straggling_model="x"))
+
+
+# ----------------------------------------------------------------------- host logic
+def test_workloads(pb):
+    W = pb.workloads
+    w0 = W.build_workload(0)
+    assert w0["weights"].shape == (8, 11, 11) and w0["weights"].dtype == np.float32
+    assert 0.5 <= w0["weights"].min() and w0["weights"].max() <= 1.5
+    w1 = W.build_workload(1)
+    assert w1["weights"].shape == (40, 41, 41)
+    lw = w1["weights"].mean(axis=(1, 2))
+    assert lw[0] < 0.33 and lw[-1] > 0.95 and np.all(np.diff(lw) > 0)
+    np.testing.assert_array_equal(W.build_workload(1)["weights"], w1["weights"])
+    w2 = W.build_workload(2)
+    m, p = w2["mask"], w2["presc"]
+    assert m.shape == (128, 128, 128)
+    assert set(np.unique(m).tolist()) == {0.0, float(np.float32(0.2)), 1.0}
+    assert np.all(p[m == 1.0] == 2.0) and np.all(p[m != 1.0] == 0.0)
+    assert (m == 1.0).sum() == 31 * 30 * 30  # z centres 8.0..14.0 cm, x/y within +-3 cm
+    w4 = W.build_workload(4)
+    assert w4["weights"].shape == (60, 61, 61) and w4["grid"]["nz"] == 256
+    fields = W.robust_fields()
+    assert [f["weights"].shape for f in fields] == [(16, 21, 21), (28, 33, 33), (40, 41, 41),
+                                                   (48, 41, 51)]
+    sc = W.robust_scenarios()
+    assert len(sc) == 25 and len(set(sc)) == 25 and (0.0, 0.0, 0.0, 1.0) in sc
+    spots, layers = W.fd_sample(w2)
+    assert spots.shape == (64, 3) and len(layers) == 8
+
+
+def test_model_api_host_parts(pb):
+    M = pb.model
+    g = M.DoseGrid.centered(128, 0.2)
+    assert g.shape == (128, 128, 128) and g.n_vox == 128**3
+    assert g.ox == -(127 * 0.2 / 2.0)
+    np.testing.assert_array_equal(g.x, g.ox + np.arange(128) * 0.2)
+    assert g.z[0] == 0.0
+    lat = M.SpotLattice(41, 41, 40, 0.25, 0.25)
+    np.testing.assert_array_equal(lat.spot_x, 0.0 + (np.arange(41) - 20.0) * 0.25)
+    assert lat.n_spots == 67240
+    x, y, l, w = lat.flat_spot_table()
+    assert x.shape == (67240,)
+    fw = M.flat_field_weights(41, 41, 3)
+    assert fw.shape == (3, 41, 41) and fw.min() >= 0.0
+    prob = M.PBProblem(g, lat, np.zeros((40, 128)), np.ones((40, 128)))
+    f = prob.field_descriptor()
+    assert (f.nx, f.n_layers, f.dx_spot) == (128, 40, 0.25)
+    c = pb.engines.operation_counts(prob, active_pairs=2727)
+    assert abs(2 * c["separable_exact"] - 4.837e9) / 4.837e9 < 1e-3
+
+
+def test_no_cpu_path(pb):
+    if has_gpu():
+        pytest.skip("checks the CPU-only behaviour")
+    M = pb.model
+    g = M.DoseGrid(8, 8, 8, 0.2, 0.2, 0.2)
+    lat = M.SpotLattice(3, 3, 1, 0.5, 0.5, weights=np.ones((1, 3, 3)))
+    prob = M.PBProblem(g, lat, np.ones((1, 8)), np.ones((1, 8)))
+    with pytest.raises(RuntimeError):
+        pb.engines.torch_separable(prob, "cuda")
+    with pytest.raises(RuntimeError):
+        pb.physics.csda_range(100.0)
