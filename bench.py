@@ -38,8 +38,8 @@ CREDITED_NOTE = ("credited FLOPs = 2*sum over (layer,slice) pairs with IDD != 0 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
@@ -68,7 +68,9 @@ def credited_flops(wl, active_pairs):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples (every 200 ms) during the timed region."""
+    """nvidia-smi clock / throttle-reason samples (every 50 ms) while the GPU runs the
+    benchmark: from the first warm-up step to the end of the end-to-end leg, so that a
+    short timed region still has samples under load."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -85,7 +87,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -200,9 +202,14 @@ def reference_arm(args):
     if rank != 0:
         return 0
     pb, wl = workload_arrays()
-    steps = max(1, args.steps)
+    import torch
+    tables = cpu_tables(wl)
+    t0 = time.perf_counter()
+    cpu_port_grad_eval(wl, tables, torch)          # first warm-up, also sizes the sample
+    t_eval = time.perf_counter() - t0
+    steps = max(1, min(args.steps, int(120.0 / max(t_eval, 1e-3))))
     rate, n, el, cores, _ = run_cpu_port(wl, budget_s=0.0, max_evals=steps,
-                                         warmup=min(args.warmup, 2))
+                                         warmup=max(0, min(args.warmup, 2) - 1))
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
             "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * el / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -248,6 +255,8 @@ def main():
         if world > 1:
             dist.barrier(device_ids=[local])
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(max(args.warmup, 3)):
         plan.loss_grad(m, p, outputs=out)
     torch.cuda.synchronize(dev)
@@ -256,10 +265,8 @@ def main():
     K = args.steps
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(K)]
-    clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize(dev)
-    clocks.start()
     n0 = lib.launch_count()
     lib.profile_begin()
     for k in range(K):
@@ -271,7 +278,6 @@ def main():
     prof = lib.profile_end()
     launches = lib.launch_count() - n0
     barrier()
-    clk = clocks.stop()
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     if world > 1:
         t = torch.tensor([t_ms], device=dev, dtype=torch.float64)
@@ -303,6 +309,7 @@ def main():
         t = torch.tensor([t2], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t2 = float(t.item())
+    clk = clocks.stop()
     e2e = world * K / (t2 * 1e-3)
     h2d = w_host.numel() * 4
     d2h = gw_host.numel() * 4 + gr_host.numel() * 4 + 8

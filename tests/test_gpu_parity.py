@@ -290,7 +290,24 @@ def test_clinical_fd_checks_cfg2(pb, torch):
     fdw = np.array(fdw)
     gsel = gw[spots[:, 0], spots[:, 1], spots[:, 2]]
     assert np.max(np.abs(gsel - fdw)) / np.max(np.abs(fdw)) < GRAD_TOL
+    # range shifts: (1) float64 autograd through the oracle engine chained with the
+    # float64 central-difference tables (same step) -- the same mathematics, tol 1e-4
     h = 0.005
+    tabs = {}
+    for sgn in (1.0, -1.0):
+        tabs[sgn] = pr.layer_luts(prob.grid.z, en, range_shift=np.full(len(en), sgn * h))
+    didd = (tabs[1.0][0] - tabs[-1.0][0]) / (2 * h)
+    dsig = (tabs[1.0][1] - tabs[-1.0][1]) / (2 * h)
+    it = torch.tensor(idd, requires_grad=True)
+    st = torch.tensor(sig, requires_grad=True)
+    d = er.separable_torch(*ax, w0, it, st)
+    er.masked_quadratic_loss(d, torch.tensor(mask), torch.tensor(presc)).backward()
+    chain = ((it.grad.numpy() * didd).sum(1) + (st.grad.numpy() * dsig).sum(1))
+    assert np.max(np.abs(gr - chain)) / np.max(np.abs(chain)) < GRAD_TOL
+    # (2) central differences of the loss itself at 0.05 mm.  The reference's tables are
+    # not smooth in range on this scale (CSDA binning at 1/6000 of the range, the T = 0
+    # cut at R0 on the 0.2 mm Fermi-Eyges grid), so the loss secant and the chain rule
+    # through secant tables differ at second order: measured <= 9e-4 of max |g|.
     fdr = []
     for l in layers:
         vals = []
@@ -301,7 +318,7 @@ def test_clinical_fd_checks_cfg2(pb, torch):
             vals.append(loss_w(w0, i_, s_))
         fdr.append((vals[0] - vals[1]) / (2 * h))
     fdr = np.array(fdr)
-    assert np.max(np.abs(gr[layers] - fdr)) / np.max(np.abs(fdr)) < GRAD_TOL
+    assert np.max(np.abs(gr[layers] - fdr)) / np.max(np.abs(fdr)) < 2e-3
 
 
 # ----------------------------------------------------------------------- batch
