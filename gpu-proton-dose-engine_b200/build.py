@@ -27,6 +27,7 @@ SOURCES = {
     "lut.cu": ["-fmad=false"],
     "fwd_simt.cu": [],
     "adj_simt.cu": [],
+    "tc_fwd.cu": [],
 }
 
 

@@ -87,9 +87,15 @@ int choose_adj_chunk(const pbd_field* f) {
 bool finite_pos(double v) { return isfinite(v) && v > 0.0; }
 
 int check_precision(int p) {
-    if (p == PBD_PREC_FP32) return PBD_OK;
-    if (p >= PBD_PREC_TF32X3 && p <= PBD_PREC_BF16) return PBD_ERR_UNSUPPORTED;
+    if (p >= PBD_PREC_FP32 && p <= PBD_PREC_BF16) return PBD_OK;
     return PBD_ERR_BAD_VALUE;
+}
+
+int check_field_precision(const pbd_field* f, int p) {
+    PBD_TRY(check_precision(p));
+    if (p == PBD_PREC_FP32) return PBD_OK;
+    int k1 = 0, n1 = 0;
+    return tc_operand_dims(p, f->n_sx, f->n_sy, &k1, &n1);
 }
 
 int adjoint_supported(const pbd_field* f) {
@@ -100,7 +106,7 @@ int adjoint_supported(const pbd_field* f) {
 // Workspace of the single-job paths.
 struct Ws {
     JobDev* jobs;        // [0] forward view, [1] adjoint view
-    int* counters;       // [0] forward, [1] adjoint
+    int* counters;       // [0] forward items, [1] forward error word, [2] adjoint items
     FwdItem* fitems;
     int* fnch;
     float* fpart;
@@ -116,7 +122,7 @@ struct Ws {
 int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, void* base, Ws& w, size_t* used) {
     Carve c(base);
     w.jobs = c.take<JobDev>(2);
-    w.counters = c.take<int>(2);
+    w.counters = c.take<int>(4);
     w.f_chunk = choose_fwd_chunk(f);
     w.a_chunk = choose_adj_chunk(f);
     w.fitems = nullptr; w.fnch = nullptr; w.fpart = nullptr; w.loss_part = nullptr;
@@ -293,7 +299,7 @@ int pbd_energy_from_range(const double* range_cm, double* energy, int n, void* s
 
 int pbd_forward_workspace(const pbd_field* f, int precision, size_t* bytes) {
     PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_precision(precision));
+    PBD_TRY(check_field_precision(f, precision));
     if (!bytes) return PBD_ERR_NULL_ARG;
     Ws w;
     return carve_ws(f, true, false, false, nullptr, w, bytes);
@@ -302,7 +308,7 @@ int pbd_forward_workspace(const pbd_field* f, int precision, size_t* bytes) {
 int pbd_forward(const pbd_field* f, const float* w, const double* idd, const double* sigma,
                 float* dose, int precision, void* workspace, size_t workspace_bytes, void* stream) {
     PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_precision(precision));
+    PBD_TRY(check_field_precision(f, precision));
     if (!w || !idd || !sigma || !dose) return PBD_ERR_NULL_ARG;
     size_t need = 0;
     Ws ws;
@@ -322,12 +328,13 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 0, s);
+    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 0,
+                          precision, s);
 }
 
 int pbd_adjoint_workspace(const pbd_field* f, int precision, size_t* bytes) {
     PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_precision(precision));
+    PBD_TRY(check_field_precision(f, precision));
     PBD_TRY(adjoint_supported(f));
     if (!bytes) return PBD_ERR_NULL_ARG;
     Ws w;
@@ -349,7 +356,7 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
                 float* grad_w, float* grad_range, int precision, void* workspace,
                 size_t workspace_bytes, void* stream) {
     PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_precision(precision));
+    PBD_TRY(check_field_precision(f, precision));
     PBD_TRY(adjoint_supported(f));
     if (!w || !idd || !sigma || !grad_dose || !grad_w) return PBD_ERR_NULL_ARG;
     const int with_range = grad_range != nullptr;
@@ -373,13 +380,13 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 1, ws.a_chunk,
+    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 2, ws.a_chunk,
                           with_range, 0, s);
 }
 
 int pbd_loss_grad_workspace(const pbd_field* f, int precision, size_t* bytes) {
     PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_precision(precision));
+    PBD_TRY(check_field_precision(f, precision));
     PBD_TRY(adjoint_supported(f));
     if (!bytes) return PBD_ERR_NULL_ARG;
     Ws w;
@@ -392,7 +399,7 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
                   float* grad_range, int precision, void* workspace, size_t workspace_bytes,
                   void* stream) {
     PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_precision(precision));
+    PBD_TRY(check_field_precision(f, precision));
     PBD_TRY(adjoint_supported(f));
     if (!w || !idd || !sigma || !mask || !presc || !dose || !grad_dose || !loss || !grad_w)
         return PBD_ERR_NULL_ARG;
@@ -421,8 +428,9 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 1, s));
-    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 1, ws.a_chunk,
+    PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 1,
+                           precision, s));
+    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 2, ws.a_chunk,
                           with_range, 1, s);
 }
 
@@ -433,10 +441,11 @@ int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, 
     PBD_TRY(check_precision(precision));
     Carve c(nullptr);
     c.take<JobDev>(n_jobs);
-    c.take<int>(1);
+    c.take<int>(2);
     size_t items = 0, nch = 0, part = 0;
     for (int k = 0; k < n_jobs; ++k) {
         PBD_TRY(host_validate_field(&jobs[k].field));
+        PBD_TRY(check_field_precision(&jobs[k].field, precision));
         const int ch = choose_fwd_chunk(&jobs[k].field);
         size_t pe = 0;
         int it = 0;
@@ -495,7 +504,7 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     }
     Carve c(workspace);
     JobDev* jd = c.take<JobDev>(n_jobs);
-    int* counter = c.take<int>(1);
+    int* counter = c.take<int>(2);
     FwdItem* items = c.take<FwdItem>(item_base);
     int* nchb = c.take<int>(nch_off);
     float* partb = c.take<float>(part_off);
@@ -503,7 +512,7 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, chunk, 0, s);
+    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, chunk, 0, precision, s);
 }
 
 }  // extern "C"

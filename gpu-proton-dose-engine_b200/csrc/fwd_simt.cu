@@ -210,16 +210,18 @@ fwd_simt_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ ite
 }
 
 // Sum of the chunk partials (chunk order), dose out, optional loss + dL/dD.
-__global__ void fwd_finalize_kernel(const JobDev* __restrict__ jobs, int with_loss) {
+__global__ void fwd_finalize_kernel(const JobDev* __restrict__ jobs, int with_loss,
+                                    const int* __restrict__ err) {
     const JobDev& J = jobs[blockIdx.y];
     const size_t plane = (size_t)J.nx * J.ny;
     const size_t n = plane * J.nz;
+    const bool bad = *err != 0;   // a main-kernel wait timed out: make the result NaN
     double lsum = 0.0;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
          v += (size_t)gridDim.x * blockDim.x) {
         const int z = (int)(v / plane);
         const int nch = J.nchunks[z];
-        float s = 0.f;
+        float s = bad ? __int_as_float(0x7fc00000) : 0.f;
         for (int k = 0; k < nch; ++k) s += J.partial[(size_t)k * n + v];
         J.dose[v] = s;
         if (with_loss) {
@@ -260,29 +262,45 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 }
 
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
-                   int total_items, int* counter, int chunk, int with_loss, cudaStream_t s) {
-    static thread_local bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(fwd_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kFwdSmemBytes) != cudaSuccess)
-            return PBD_ERR_NO_SMEM;
-        attr_set = true;
+                   int total_items, int* counter, int chunk, int with_loss, int precision,
+                   cudaStream_t s) {
+    int K1 = 0, N1 = 0;
+    if (precision != PBD_PREC_FP32) {
+        for (int j = 0; j < n_jobs; ++j) {
+            int k1 = 0, n1 = 0;
+            PBD_TRY(tc_operand_dims(precision, jobs_host[j].nsx, jobs_host[j].nsy, &k1, &n1));
+            K1 = max(K1, k1);
+            N1 = max(N1, n1);
+        }
+    } else {
+        static thread_local bool attr_set = false;
+        if (!attr_set) {
+            if (cudaFuncSetAttribute(fwd_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kFwdSmemBytes) != cudaSuccess)
+                return PBD_ERR_NO_SMEM;
+            attr_set = true;
+        }
     }
-    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, sizeof(int), s)));
+    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
     fwd_schedule_kernel<<<n_jobs, 256, 0, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();
-    const int grid = max(1, min(total_items, 2 * num_sms()));
-    prof_mark(kProfFwd, 0, s);
-    fwd_simt_kernel<<<grid, NT, kFwdSmemBytes, s>>>(jobs_dev, items, total_items, counter);
-    PBD_LAUNCH_CHECK();
-    prof_mark(kProfFwd, 1, s);
+    if (precision == PBD_PREC_FP32) {
+        const int grid = max(1, min(total_items, 2 * num_sms()));
+        prof_mark(kProfFwd, 0, s);
+        fwd_simt_kernel<<<grid, NT, kFwdSmemBytes, s>>>(jobs_dev, items, total_items, counter);
+        PBD_LAUNCH_CHECK();
+        prof_mark(kProfFwd, 1, s);
+    } else {
+        PBD_TRY(launch_forward_tc_main(precision, jobs_dev, items, total_items, counter,
+                                       counter + 1, K1, N1, s));
+    }
     int max_blocks = 1;
     for (int j = 0; j < n_jobs; ++j) {
         const size_t n = (size_t)jobs_host[j].nx * jobs_host[j].ny * jobs_host[j].nz;
         max_blocks = max(max_blocks, (int)std::min<size_t>((n + 255) / 256, 4096));
     }
     const int fin_blocks = with_loss ? kLossBlocks : max_blocks;
-    fwd_finalize_kernel<<<dim3(fin_blocks, n_jobs), 256, 0, s>>>(jobs_dev, with_loss);
+    fwd_finalize_kernel<<<dim3(fin_blocks, n_jobs), 256, 0, s>>>(jobs_dev, with_loss, counter + 1);
     PBD_LAUNCH_CHECK();
     count_launch(3);
     return PBD_OK;

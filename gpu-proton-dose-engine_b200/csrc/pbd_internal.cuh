@@ -107,8 +107,15 @@ int num_sms();
 // forward (FP32 SIMT) -- fwd_simt.cu
 int fwd_chunk_layers(const pbd_field* f);
 int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items);
+// counter[0] = item counter, counter[1] = error word (set by a timed-out device wait).
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
-                   int total_items, int* counter, int chunk, int with_loss, cudaStream_t s);
+                   int total_items, int* counter, int chunk, int with_loss, int precision,
+                   cudaStream_t s);
+
+// forward (tcgen05) -- tc_fwd.cu
+int tc_operand_dims(int precision, int nsx, int nsy, int* K1, int* N1);
+int launch_forward_tc_main(int precision, JobDev* jobs, FwdItem* items, int total, int* counter,
+                           int* err, int K1, int N1, cudaStream_t s);
 
 // adjoint (FP32 SIMT) -- adj_simt.cu
 int adj_chunk_depths(const pbd_field* f);

@@ -1,0 +1,109 @@
+"""Tensor-core (tcgen05) forward against the float64 oracle, every precision mode.
+
+Tolerances (max |dD| / max D against float64):
+  tf32x3 (default):  1e-6   -- the north-star bound for the split forms
+  bf16x3:            5e-5   -- reported; the split with bf16 parts keeps ~16 mantissa bits
+  tf32:              5e-3   -- one TF32 product (10-bit mantissa)
+  bf16:              5e-2   -- one BF16 product (7-bit mantissa)
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, has_gpu, load_pkg
+from oracle import engine_ref as er
+from oracle import physics_ref as pr
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")]
+
+TOL = {"tf32x3": 1e-6, "bf16x3": 5e-5, "tf32": 5e-3, "bf16": 5e-2}
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def pb():
+    return load_pkg()
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "tf32", "bf16"])
+def test_tc_forward_cfg0(pb, prec):
+    wl = pb.workloads.build_workload(0)
+    lut = golden("luts_cfg0.npz")
+    prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
+    d = pb.engines.torch_separable(prob, "cuda", precision=prec).cpu().numpy()
+    err = rel(d, golden("dose_cfg0.npz")["dose"])
+    print(f"cfg0 {prec}: max_rel_err {err:.3e}")
+    assert err < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "tf32", "bf16"])
+def test_tc_forward_cfg1(pb, prec):
+    wl = pb.workloads.build_workload(1)
+    lut = golden("luts_cfg1.npz")
+    prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
+    d = pb.engines.torch_separable(prob, "cuda", precision=prec).cpu().numpy()
+    ref = er.separable_torch(prob.grid.x, prob.grid.y, prob.lattice.spot_x, prob.lattice.spot_y,
+                             wl["weights"], lut["idd"], lut["sigma"]).numpy()
+    err = rel(d, ref)
+    print(f"cfg1 {prec}: max_rel_err {err:.3e}")
+    assert err < TOL[prec]
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1, 1, 1, 1), (150, 70, 33, 61, 13, 5),
+                                   (37, 129, 9, 5, 64, 3), (200, 200, 3, 61, 61, 2)])
+def test_tc_forward_ragged(pb, shape):
+    nx, ny, nz, nsx, nsy, nl = shape
+    rng = np.random.default_rng(sum(shape) + 1)
+    M = pb.model
+    grid = M.DoseGrid(nx, ny, nz, 0.15, 0.2, 0.3, -(nx - 1) * 0.075, -(ny - 1) * 0.1, 0.0)
+    w = rng.uniform(0.1, 1.0, (nl, nsy, nsx))
+    lat = M.SpotLattice(nsx, nsy, nl, 0.25, 0.3, x0=0.07, y0=-0.11, weights=w)
+    idd = rng.uniform(0.0, 5.0, (nl, nz))
+    idd[rng.random((nl, nz)) < 0.3] = 0.0
+    sig = rng.uniform(0.2, 0.8, (nl, nz))
+    prob = M.PBProblem(grid, lat, idd, sig)
+    d = pb.engines.torch_separable(prob, "cuda", precision="tf32x3").cpu().numpy()
+    ref = er.separable_f64(grid.x, grid.y, lat.spot_x, lat.spot_y, w, idd, sig)
+    if np.max(np.abs(ref)) == 0:
+        assert np.all(d == 0)
+    else:
+        assert rel(d, ref) < TOL["tf32x3"]
+
+
+def test_tc_rejects_large_lattice(pb):
+    M = pb.model
+    grid = M.DoseGrid(16, 16, 4, 0.2, 0.2, 0.2)
+    lat = M.SpotLattice(65, 3, 1, 0.25, 0.25, weights=np.ones((1, 3, 65)))
+    prob = M.PBProblem(grid, lat, np.ones((1, 4)), np.ones((1, 4)))
+    with pytest.raises(RuntimeError):
+        pb.engines.torch_separable(prob, "cuda", precision="tf32x3")
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32")   # the FP32 path chunks it
+    assert d.shape == (4, 16, 16)
+
+
+def test_tc_loss_grad_and_batch(pb):
+    import torch
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    ref_plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
+    tc_plan = pb.engines.DosePlan(prob, tables="device", precision="tf32x3")
+    mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
+    m = torch.as_tensor(mask, device="cuda")
+    p = torch.as_tensor(presc * 100.0, device="cuda")
+    a = ref_plan.loss_grad(m, p)
+    b = tc_plan.loss_grad(m, p)
+    assert rel(b["dose"].cpu().numpy(), a["dose"].cpu().numpy()) < 1e-6
+    assert rel(b["grad_w"].cpu().numpy(), a["grad_w"].cpu().numpy()) < 1e-5
+    scen = [(0, 0, 0, 1.0), (0.3, -0.3, 0.3, 1.035)]
+    b32 = pb.robust.ScenarioBatch([prob], scen, precision="fp32")
+    btc = pb.robust.ScenarioBatch([prob], scen, precision="tf32x3")
+    b32.run()
+    btc.run()
+    torch.cuda.synchronize()
+    for d0, d1 in zip(b32.doses, btc.doses):
+        assert rel(d1.cpu().numpy(), d0.cpu().numpy()) < 1e-6
