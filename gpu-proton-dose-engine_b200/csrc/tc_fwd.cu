@@ -365,17 +365,26 @@ size_t tc_smem_bytes(int K1, int N1) {
 template <int MODE>
 int launch_mode(JobDev* jobs, FwdItem* items, int total, int* counter, int* err, int K1, int N1,
                 cudaStream_t s) {
-    static thread_local bool attr = false;
+    static thread_local int max_dyn = 0;
+    if (max_dyn == 0) {
+        int dev = 0, optin = 0;
+        cudaFuncAttributes fa;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+                cudaSuccess ||
+            cudaFuncGetAttributes(&fa, fwd_tc_kernel<MODE>) != cudaSuccess)
+            return PBD_ERR_CUDA;
+        const int avail = optin - (int)fa.sharedSizeBytes;
+        if (avail <= 0 || cudaFuncSetAttribute(fwd_tc_kernel<MODE>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               avail) != cudaSuccess)
+            return PBD_ERR_NO_SMEM;
+        max_dyn = avail;
+    }
     // At least 116 KiB so that one CTA (and its 256 TMEM columns) occupies an SM: a second
     // resident CTA would only wait in tcgen05.alloc for the first to finish.
     const size_t smem = std::max<size_t>(tc_smem_bytes<MODE>(K1, N1), 116u * 1024u);
-    if (smem > 227u * 1024u) return PBD_ERR_NO_SMEM;
-    if (!attr) {
-        if (cudaFuncSetAttribute(fwd_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 227 * 1024) != cudaSuccess)
-            return PBD_ERR_NO_SMEM;
-        attr = true;
-    }
+    if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
     const int grid = std::max(1, std::min(total, num_sms()));
     prof_mark(kProfFwd, 0, s);
     fwd_tc_kernel<MODE><<<grid, TNT, smem, s>>>(jobs, items, total, counter, err, K1, N1);

@@ -36,11 +36,13 @@
 extern "C" {
 #endif
 
-/* Error codes; pencil_beam.cu:647-653 (same values for the shared meanings). */
+/* Error codes; pencil_beam.cu:647-653.  The values the reference defines keep their meaning
+ * (-3, its z-grid mismatch, cannot occur here: tables are built at the grid's depths);
+ * new codes start at -7. */
 #define PBD_OK                0
 #define PBD_ERR_NULL_ARG     -1
 #define PBD_ERR_BAD_DIM      -2
-#define PBD_ERR_BAD_VALUE    -3   /* NaN / non-positive sigma, spacing or step */
+#define PBD_ERR_BAD_VALUE   -10   /* non-finite or out-of-range value (spacing, step, mode) */
 #define PBD_ERR_CUDA         -4
 #define PBD_ERR_UNSUPPORTED  -5
 #define PBD_ERR_NO_SMEM      -6

@@ -50,8 +50,8 @@ def test_field_validation_codes(pb, lib):
     assert lib.pbd_field_validate(None) == -1
     assert lib.pbd_field_validate(ctypes.byref(field(pb, nx=0))) == -2
     assert lib.pbd_field_validate(ctypes.byref(field(pb, n_layers=-1))) == -2
-    assert lib.pbd_field_validate(ctypes.byref(field(pb, dx=float("nan")))) == -3
-    assert lib.pbd_field_validate(ctypes.byref(field(pb, dx_spot=0.0))) == -3
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, dx=float("nan")))) == -10
+    assert lib.pbd_field_validate(ctypes.byref(field(pb, dx_spot=0.0))) == -10
     assert lib.pbd_field_validate(ctypes.byref(field(pb, n_sx=5000))) == -5
     for code in range(-12, 1):
         assert lib.pbd_strerror(code)
@@ -61,7 +61,7 @@ def test_entry_points_validate_before_device_work(pb, lib):
     f = field(pb)
     sz = ctypes.c_size_t(0)
     assert lib.pbd_forward_workspace(ctypes.byref(f), 0, ctypes.byref(sz)) == 0 and sz.value > 0
-    assert lib.pbd_forward_workspace(ctypes.byref(f), 99, ctypes.byref(sz)) == -3
+    assert lib.pbd_forward_workspace(ctypes.byref(f), 99, ctypes.byref(sz)) == -10
     fake = 0x1000
     # null arrays, missing / short workspace -> errors, and nothing launched
     assert lib.pbd_forward(ctypes.byref(f), None, fake, fake, fake, 0, fake, 1 << 30, None) == -1
@@ -73,7 +73,7 @@ def test_entry_points_validate_before_device_work(pb, lib):
     assert lib.pbd_adjoint_workspace(ctypes.byref(big), 0, ctypes.byref(sz)) == -5
     assert lib.pbd_loss_grad(ctypes.byref(f), fake, fake, fake, None, None, fake, fake, fake, fake,
                              fake, fake, fake, 0, None, 0, None) == -1
-    assert lib.pbd_set_schedule(65, 0) == -3
+    assert lib.pbd_set_schedule(65, 0) == -10
     assert lib.pbd_set_schedule(0, 0) == 0
 
 
@@ -93,7 +93,7 @@ def test_lut_spec_validation(pb, lib):
     sz = ctypes.c_size_t(0)
     assert lib.pbd_lut_workspace(ctypes.byref(s), 8, ctypes.byref(sz)) == 0 and sz.value > 0
     bad = pb.physics.lut_spec(64, 0.0, -0.2)
-    assert lib.pbd_lut_workspace(ctypes.byref(bad), 8, ctypes.byref(sz)) == -3
+    assert lib.pbd_lut_workspace(ctypes.byref(bad), 8, ctypes.byref(sz)) == -10
     assert lib.pbd_lut_workspace(ctypes.byref(s), 0, ctypes.byref(sz)) == -2
     with pytest.raises(ValueError):
         pb.physics.lut_spec(64, 0.0, 0.2, idd_model=pb.physics.IDDModel(straggling_model="x"))
