@@ -10,11 +10,18 @@
 // The Gaussian factors are generated by the CTA's 256 threads straight into shared memory
 // in the UMMA canonical K-major layout (no swizzle; 16-byte chunk planes of all rows, so
 // a warp's stores are 512 contiguous bytes); the stage-1 accumulator is read back from
-// TMEM, scaled, rounded and stored as stage 2's B operand; D stays in TMEM across the
-// item's layers and is written once.  One thread issues the MMAs; completion is signalled
-// through mbarriers by tcgen05.commit.  Every wait is bounded (2 s of %globaltimer): on
-// expiry the CTA sets the workspace error word, drains, frees its TMEM and leaves, and the
-// finalize pass turns the output into NaN.
+// TMEM, scaled, rounded and stored as stage 2's B operand.  One thread issues the MMAs;
+// completion is signalled through mbarriers by tcgen05.commit.  Every wait is bounded
+// (2 s of %globaltimer): on expiry the CTA sets the workspace error word, drains, frees
+// its TMEM and leaves, and the finalize pass turns the output into NaN.
+//
+// Accumulation.  The tensor core's FP32 accumulation aligns and truncates, so its error
+// grows with the number of MMA steps into one accumulator.  Each (layer, slice) therefore
+// starts fresh accumulators, and the large hi*hi products and the two small cross
+// products go to separate ones (6 + 12 steps at K = 48; the small accumulator is ~2^-11 of
+// the large one).  Big + small are added in FP32 registers, and the layers of an item are
+// summed there too (IEEE round to nearest): D is read back from TMEM once per layer while
+// the next layer's stage 1 runs.
 //
 // Precision modes (accumulation always FP32):
 //   TF32X3  a b ~ ah bh + ah bl + al bh with ah = tf32(a), al = tf32(a - ah)  (~1e-7)
@@ -30,7 +37,7 @@ namespace pbd {
 namespace {
 
 constexpr int TNT = 256;
-constexpr uint32_t kTmemCols = 256;   // D: 128 columns, stage-1 accumulator: <= 64
+constexpr uint32_t kTmemCols = 512;   // stage 2 big/small 2 x 128, stage 1 big/small 2 x 64
 constexpr uint64_t kWaitNs = 2000000000ull;
 
 template <int MODE> struct Prec;
@@ -109,6 +116,37 @@ struct Bufs {
 };
 
 template <int MODE>
+struct Ops {
+    using P = Prec<MODE>;
+    // One stage: big products (hi x hi) into t_big, the two cross products into t_small.
+    // Each accumulator starts fresh (acc = 0) for every (layer, slice): the tensor core's
+    // FP32 accumulation truncates, so its error grows with the steps per accumulator.
+    __device__ static void issue(uint32_t t_big, uint32_t t_small, uint8_t* const* a,
+                                 uint8_t* const* b, uint32_t plane_a, uint32_t plane_b,
+                                 int ksteps, uint32_t idesc) {
+        uint32_t acc_b = 0, acc_s = 0;
+        for (int st = 0; st < ksteps; ++st) {
+            const uint32_t oa = (uint32_t)st * 2u * plane_a, ob = (uint32_t)st * 2u * plane_b;
+            const uint64_t da_hi = tc::smem_desc(tc::smem_u32(a[0]) + oa, plane_a, 128);
+            const uint64_t db_hi = tc::smem_desc(tc::smem_u32(b[0]) + ob, plane_b, 128);
+            mma(t_big, da_hi, db_hi, idesc, acc_b);
+            acc_b = 1;
+            if (P::NPROD == 3) {
+                const uint64_t da_lo = tc::smem_desc(tc::smem_u32(a[1]) + oa, plane_a, 128);
+                const uint64_t db_lo = tc::smem_desc(tc::smem_u32(b[1]) + ob, plane_b, 128);
+                mma(t_small, da_hi, db_lo, idesc, acc_s);
+                acc_s = 1;
+                mma(t_small, da_lo, db_hi, idesc, 1u);
+            }
+        }
+    }
+    __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+        if (P::EB == 4) tc::mma_tf32(d, a, b, idesc, acc);
+        else tc::mma_bf16(d, a, b, idesc, acc);
+    }
+};
+
+template <int MODE>
 __global__ void __launch_bounds__(TNT, 1)
 fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items, int total,
               int* counter, int* err, int K1, int N1) {
@@ -144,14 +182,40 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tD = tmem_base_s, tD1 = tmem_base_s + 128u;
+    // TMEM columns: stage-2 big / small [0,128) [128,256); stage-1 big / small [256,320) [320,384)
+    const uint32_t tDb = tmem_base_s, tDs = tmem_base_s + 128u;
+    const uint32_t tUb = tmem_base_s + 256u, tUs = tmem_base_s + 320u;
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     const uint32_t idesc1 = tc::instr_desc(128, N1, P::FMT);
     const uint32_t idesc2 = tc::instr_desc(128, 128, P::FMT);
     const uint32_t plane128 = 128u * 16u, plane_n1 = (uint32_t)N1 * 16u;
+    const int half = warp >> 2;          // which 64 columns this warp reads back
+    const int trow = 32 * (warp & 3) + lane;
 
     uint32_t ph1 = 0, ph2 = 0;
     bool mma1_pending = false, mma2_pending = false, failed = false;
+    float dsum[64];
+
+    // Wait for the stage-2 MMAs of the previous layer and add its D into the registers.
+    auto drain_stage2 = [&]() -> bool {
+        const bool ok = wait_bar(&bar[1], ph2);
+        if (ok) { ph2 ^= 1; mma2_pending = false; }
+        if (__syncthreads_or(!ok)) return false;
+        tc::fence_after_sync();
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+            uint32_t rb[16], rs[16];
+            tc::tmem_ld16(tDb + lane_base + (uint32_t)(half * 64 + c0), rb);
+            if (P::NPROD == 3) tc::tmem_ld16(tDs + lane_base + (uint32_t)(half * 64 + c0), rs);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                float v = __uint_as_float(rb[q]);
+                if (P::NPROD == 3) v += __uint_as_float(rs[q]);
+                dsum[c0 + q] += v;
+            }
+        }
+        return true;
+    };
 
     for (;;) {
         if (tid == 0) s_item = atomicAdd(counter, 1);
@@ -165,7 +229,8 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
         const int nz = J.nz, nx = J.nx, ny = J.ny, nsx = J.nsx, nsy = J.nsy;
         const int z = it.z, y0 = it.ty * kTile, x0 = it.tx * kTile;
         const double cx = 0.5 * (double)(nsx - 1), cy = 0.5 * (double)(nsy - 1);
-        bool first = true;
+#pragma unroll
+        for (int q = 0; q < 64; ++q) dsum[q] = 0.f;
 
         for (int l = it.lb; l < it.le && !failed; ++l) {
             const double c = J.idd[(size_t)l * nz + z];
@@ -211,30 +276,15 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                uint32_t acc = 0;
-                for (int st = 0; st < K1 / P::KSTEP; ++st) {
-#pragma unroll
-                    for (int pr = 0; pr < P::NPROD; ++pr) {
-                        const int ai = pr == 2 ? 1 : 0, bi = pr == 1 ? 1 : 0;
-                        const uint64_t da = tc::smem_desc(
-                            tc::smem_u32(B.a1[ai]) + (uint32_t)st * 2u * plane128, plane128, 128);
-                        const uint64_t db = tc::smem_desc(
-                            tc::smem_u32(B.b1[bi]) + (uint32_t)st * 2u * plane_n1, plane_n1, 128);
-                        if (P::EB == 4) tc::mma_tf32(tD1, da, db, idesc1, acc);
-                        else tc::mma_bf16(tD1, da, db, idesc1, acc);
-                        acc = 1;
-                    }
-                }
+                Ops<MODE>::issue(tUb, tUs, B.a1, B.b1, plane128, plane_n1, K1 / P::KSTEP, idesc1);
                 tc::commit(&bar[0]);
             }
             mma1_pending = true;
 
-            // ---- stage-2 A operand: Gy (128 y-rows, K2); wait until MMA2(prev) read A2/B2 ----
-            if (mma2_pending) {
-                const bool ok = wait_bar(&bar[1], ph2);
-                if (ok) { ph2 ^= 1; mma2_pending = false; }
-                if (__syncthreads_or(!ok)) { failed = true; break; }
-            }
+            // ---- previous layer's stage 2 done: D into registers, A2/B2 free ----
+            if (mma2_pending && !drain_stage2()) { failed = true; break; }
+
+            // ---- stage-2 A operand: Gy (128 y-rows, K2) ----
             const int g2 = K2 / P::EPC;
             for (int e = tid; e < 128 * g2; e += TNT) {
                 const int row = e & 127, g = e >> 7;
@@ -253,7 +303,7 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                 if (NARR == 2) *reinterpret_cast<uint4*>(B.a2[1] + off) = lo;
             }
 
-            // ---- U = s * stage-1 result -> B2 (128 x-rows, K2) ----
+            // ---- U = s * (stage-1 big + small) -> B2 (128 x-rows, K2) ----
             {
                 const bool ok = wait_bar(&bar[0], ph1);
                 if (ok) { ph1 ^= 1; mma1_pending = false; }
@@ -261,21 +311,25 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             }
             tc::fence_after_sync();
             {
-                const int row = 32 * (warp & 3) + lane;
-                const int half = warp >> 2, ncol = N1 / 2;
+                const int ncol = N1 / 2;
                 for (int c0 = half * ncol; c0 < (half + 1) * ncol; c0 += 8) {
-                    uint32_t r[8];
-                    tc::tmem_ld8(tD1 + lane_base + (uint32_t)c0, r);
+                    uint32_t rb[8], rs[8];
+                    tc::tmem_ld8(tUb + lane_base + (uint32_t)c0, rb);
+                    if (P::NPROD == 3) tc::tmem_ld8(tUs + lane_base + (uint32_t)c0, rs);
                     tc::tmem_wait_ld();
                     float v[8];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]) * scale;
+                    for (int q = 0; q < 8; ++q) {
+                        float u = __uint_as_float(rb[q]);
+                        if (P::NPROD == 3) u += __uint_as_float(rs[q]);
+                        v[q] = u * scale;
+                    }
 #pragma unroll
                     for (int part = 0; part < 8 / P::EPC; ++part) {
                         uint4 hi, lo;
                         split_chunk<MODE>(v + part * P::EPC, hi, lo);
                         const int g = (c0 + part * P::EPC) / P::EPC;
-                        const uint32_t off = (uint32_t)g * plane128 + (uint32_t)row * 16u;
+                        const uint32_t off = (uint32_t)g * plane128 + (uint32_t)trow * 16u;
                         *reinterpret_cast<uint4*>(B.b2[0] + off) = hi;
                         if (NARR == 2) *reinterpret_cast<uint4*>(B.b2[1] + off) = lo;
                     }
@@ -286,56 +340,30 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                uint32_t acc = first ? 0u : 1u;
-                for (int st = 0; st < K2 / P::KSTEP; ++st) {
-#pragma unroll
-                    for (int pr = 0; pr < P::NPROD; ++pr) {
-                        const int ai = pr == 2 ? 1 : 0, bi = pr == 1 ? 1 : 0;
-                        const uint64_t da = tc::smem_desc(
-                            tc::smem_u32(B.a2[ai]) + (uint32_t)st * 2u * plane128, plane128, 128);
-                        const uint64_t db = tc::smem_desc(
-                            tc::smem_u32(B.b2[bi]) + (uint32_t)st * 2u * plane128, plane128, 128);
-                        if (P::EB == 4) tc::mma_tf32(tD, da, db, idesc2, acc);
-                        else tc::mma_bf16(tD, da, db, idesc2, acc);
-                        acc = 1;
-                    }
-                }
+                Ops<MODE>::issue(tDb, tDs, B.a2, B.b2, plane128, plane128, K2 / P::KSTEP, idesc2);
                 tc::commit(&bar[1]);
             }
             mma2_pending = true;
-            first = false;
         }
         if (failed) break;
 
-        // ---- epilogue: D (lanes = y, columns = x) -> partial slice of this chunk ----
-        if (mma2_pending) {
-            const bool ok = wait_bar(&bar[1], ph2);
-            if (ok) { ph2 ^= 1; mma2_pending = false; }
-            if (__syncthreads_or(!ok)) { failed = true; break; }
-        }
-        tc::fence_after_sync();
+        // ---- epilogue: last layer's D into the registers, then the partial slice ----
+        if (mma2_pending && !drain_stage2()) { failed = true; break; }
         {
-            const int yy = 32 * (warp & 3) + lane, half = warp >> 2;
-            const int y = y0 + yy;
+            const int y = y0 + trow;
             const size_t n3 = (size_t)nz * ny * nx;
             float* out = J.partial + (size_t)it.chunk * n3 + (size_t)z * ny * nx + (size_t)y * nx;
-            for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 16) {
-                uint32_t r[16];
-                tc::tmem_ld16(tD + lane_base + (uint32_t)c0, r);
-                tc::tmem_wait_ld();
-                if (y < ny) {
-                    const int xb = x0 + c0;
-                    if (xb + 16 <= nx && (nx & 3) == 0) {
+            if (y < ny) {
+                const int xb = x0 + half * 64;
+                if (xb + 64 <= nx && (nx & 3) == 0) {
 #pragma unroll
-                        for (int q = 0; q < 16; q += 4)
-                            *reinterpret_cast<float4*>(out + xb + q) =
-                                make_float4(__uint_as_float(r[q]), __uint_as_float(r[q + 1]),
-                                            __uint_as_float(r[q + 2]), __uint_as_float(r[q + 3]));
-                    } else {
+                    for (int q = 0; q < 64; q += 4)
+                        *reinterpret_cast<float4*>(out + xb + q) =
+                            make_float4(dsum[q], dsum[q + 1], dsum[q + 2], dsum[q + 3]);
+                } else {
 #pragma unroll
-                        for (int q = 0; q < 16; ++q)
-                            if (xb + q < nx) out[xb + q] = __uint_as_float(r[q]);
-                    }
+                    for (int q = 0; q < 64; ++q)
+                        if (xb + q < nx) out[xb + q] = dsum[q];
                 }
             }
         }
@@ -381,7 +409,7 @@ int launch_mode(JobDev* jobs, FwdItem* items, int total, int* counter, int* err,
             return PBD_ERR_NO_SMEM;
         max_dyn = avail;
     }
-    // At least 116 KiB so that one CTA (and its 256 TMEM columns) occupies an SM: a second
+    // At least 116 KiB so that one CTA (and its 512 TMEM columns) occupies an SM: a second
     // resident CTA would only wait in tcgen05.alloc for the first to finish.
     const size_t smem = std::max<size_t>(tc_smem_bytes<MODE>(K1, N1), 116u * 1024u);
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
