@@ -75,6 +75,8 @@ _SIGS = {
     "pbd_loss_grad": (c_int, [POINTER(Field), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
+    "pbd_forward_noalloc": (c_int, [POINTER(Field), c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                    c_void_p]),
     "pbd_forward_batch_workspace": (c_int, [POINTER(Job), c_int, c_int, POINTER(c_size_t)]),
     "pbd_forward_batch": (c_int, [POINTER(Job), c_int, c_int, c_void_p, c_size_t, c_void_p]),
 }

@@ -28,6 +28,7 @@ SOURCES = {
     "fwd_simt.cu": [],
     "adj_simt.cu": [],
     "tc_fwd.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -146,6 +146,20 @@ PBD_API int pbd_forward(const pbd_field *f, const float *w, const double *idd, c
                 float *dose, int precision, void *workspace, size_t workspace_bytes,
                 void *stream);
 
+/* ---- forward dose without any device allocation ----------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory: a
+ * real-time adaptive-therapy loop that reserves its memory once at start-up and must not
+ * block or fail on an allocation mid-treatment, or a host that owns the GPU through its
+ * own memory pool.  Same inputs and output as pbd_forward, but no workspace argument:
+ * the scratch is a fixed 1 MiB array inside the library (held by every GPU that loads
+ * it, until exit).  Limits: n_layers <= 64 and nz * ceil(nx/128) * ceil(ny/128) work
+ * items must fit the 1 MiB (about 32,000 items); otherwise PBD_ERR_UNSUPPORTED or
+ * PBD_ERR_WORKSPACE.  The first call on a device resolves the array's device address,
+ * so make it before any stream capture.  Calls share the array: two calls that overlap
+ * on the GPU race, so order them (same stream) or do not overlap them. */
+PBD_API int pbd_forward_noalloc(const pbd_field *f, const float *w, const double *idd,
+                                const double *sigma, float *dose, int precision, void *stream);
+
 /* ---- adjoint (no counterpart in the reference, which has no gradient) --------------
  * Given grad_dose = dL/dD (nz, ny, nx), writes grad_w = dL/dW (L, nsy, nsx) and
  * grad_range = dL/d(range shift) (L), the latter through didd_dr and dsigma_dr
