@@ -29,6 +29,7 @@ SOURCES = {
     "adj_simt.cu": [],
     "tc_fwd.cu": [],
     "noalloc.cu": [],
+    "adj_tc.cu": [],
 }
 
 

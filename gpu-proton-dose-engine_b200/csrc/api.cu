@@ -111,7 +111,8 @@ struct Ws {
     int* fnch;
     float* fpart;
     double* loss_part;
-    AdjItem* aitems;
+    void* aitems;        // AdjItem (FP32 path) or FwdItem (tensor-core path), 32 B each
+    int adj_tc;          // 1: tensor-core adjoint, (layer, slice) dL/dW slots
     int* anch;
     float* apart;
     float* dc;
@@ -119,10 +120,11 @@ struct Ws {
     int f_items, a_items, f_chunk, a_chunk;
 };
 
-int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, void* base, Ws& w, size_t* used) {
+int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, void* base, Ws& w,
+             size_t* used) {
     Carve c(base);
     w.jobs = c.take<JobDev>(2);
-    w.counters = c.take<int>(4);
+    w.counters = c.take<int>(8);
     w.f_chunk = choose_fwd_chunk(f);
     w.a_chunk = choose_adj_chunk(f);
     w.fitems = nullptr; w.fnch = nullptr; w.fpart = nullptr; w.loss_part = nullptr;
@@ -136,11 +138,23 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, void* base, Ws& 
         w.fpart = c.take<float>(pe);
     }
     if (loss) w.loss_part = c.take<double>(kLossBlocks);
+    w.adj_tc = 0;
     if (adj) {
         size_t pe = 0;
-        PBD_TRY(adj_plan_sizes(f, w.a_chunk, &pe, &w.a_items));
-        w.aitems = c.take<AdjItem>(w.a_items);
-        w.anch = c.take<int>(f->n_layers);
+        int n1 = 0;
+        if (tc_adjoint_dims(precision, f, &n1) == PBD_OK) {
+            // tensor-core adjoint: (slice, layer-chunk) items, one dL/dW slot per (layer, slice)
+            w.adj_tc = 1;
+            w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : 8;
+            w.a_items = f->nz * ((f->n_layers + w.a_chunk - 1) / w.a_chunk);
+            pe = (size_t)f->n_layers * f->nz * f->n_sy * f->n_sx;
+            w.aitems = c.take<FwdItem>(w.a_items);
+            w.anch = c.take<int>(f->nz);
+        } else {
+            PBD_TRY(adj_plan_sizes(f, w.a_chunk, &pe, &w.a_items));
+            w.aitems = c.take<AdjItem>(w.a_items);
+            w.anch = c.take<int>(f->n_layers);
+        }
         w.apart = c.take<float>(pe);
         w.dc = c.take<float>((size_t)f->n_layers * f->nz);
         w.dsg = c.take<float>((size_t)f->n_layers * f->nz);
@@ -302,7 +316,7 @@ int pbd_forward_workspace(const pbd_field* f, int precision, size_t* bytes) {
     PBD_TRY(check_field_precision(f, precision));
     if (!bytes) return PBD_ERR_NULL_ARG;
     Ws w;
-    return carve_ws(f, true, false, false, nullptr, w, bytes);
+    return carve_ws(f, true, false, false, precision, nullptr, w, bytes);
 }
 
 int pbd_forward(const pbd_field* f, const float* w, const double* idd, const double* sigma,
@@ -312,9 +326,9 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
     if (!w || !idd || !sigma || !dose) return PBD_ERR_NULL_ARG;
     size_t need = 0;
     Ws ws;
-    PBD_TRY(carve_ws(f, true, false, false, nullptr, ws, &need));
+    PBD_TRY(carve_ws(f, true, false, false, precision, nullptr, ws, &need));
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
-    PBD_TRY(carve_ws(f, true, false, false, workspace, ws, &need));
+    PBD_TRY(carve_ws(f, true, false, false, precision, workspace, ws, &need));
     cudaStream_t s = (cudaStream_t)stream;
     JobPair p;
     memset(&p, 0, sizeof(p));
@@ -332,17 +346,28 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
                           precision, s);
 }
 
+static int run_adjoint(const Ws& ws, int precision, const JobDev* A, int with_range,
+                       int finalize_loss, cudaStream_t s) {
+    if (ws.adj_tc)
+        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, static_cast<FwdItem*>(ws.aitems),
+                                 ws.a_items, ws.counters + 2, ws.a_chunk, with_range,
+                                 finalize_loss, s);
+    return launch_adjoint(ws.jobs + 1, A, 1, static_cast<AdjItem*>(ws.aitems), ws.a_items,
+                          ws.counters + 2, ws.a_chunk, with_range, finalize_loss, s);
+}
+
 int pbd_adjoint_workspace(const pbd_field* f, int precision, size_t* bytes) {
     PBD_TRY(host_validate_field(f));
     PBD_TRY(check_field_precision(f, precision));
     PBD_TRY(adjoint_supported(f));
     if (!bytes) return PBD_ERR_NULL_ARG;
     Ws w;
-    return carve_ws(f, false, true, false, nullptr, w, bytes);
+    return carve_ws(f, false, true, false, precision, nullptr, w, bytes);
 }
 
 static void fill_adj_view(const pbd_field* f, const Ws& ws, JobDev& A) {
-    A.max_chunks = (f->nz + ws.a_chunk - 1) / ws.a_chunk;
+    A.max_chunks = ws.adj_tc ? (f->n_layers + ws.a_chunk - 1) / ws.a_chunk
+                             : (f->nz + ws.a_chunk - 1) / ws.a_chunk;
     A.item_base = 0;
     A.max_items = ws.a_items;
     A.partial = ws.apart;
@@ -363,9 +388,9 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
     if (with_range && (!didd_dr || !dsigma_dr)) return PBD_ERR_NULL_ARG;
     size_t need = 0;
     Ws ws;
-    PBD_TRY(carve_ws(f, false, true, false, nullptr, ws, &need));
+    PBD_TRY(carve_ws(f, false, true, false, precision, nullptr, ws, &need));
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
-    PBD_TRY(carve_ws(f, false, true, false, workspace, ws, &need));
+    PBD_TRY(carve_ws(f, false, true, false, precision, workspace, ws, &need));
     cudaStream_t s = (cudaStream_t)stream;
     JobPair p;
     memset(&p, 0, sizeof(p));
@@ -380,8 +405,7 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 2, ws.a_chunk,
-                          with_range, 0, s);
+    return run_adjoint(ws, precision, &A, with_range, 0, s);
 }
 
 int pbd_loss_grad_workspace(const pbd_field* f, int precision, size_t* bytes) {
@@ -390,7 +414,7 @@ int pbd_loss_grad_workspace(const pbd_field* f, int precision, size_t* bytes) {
     PBD_TRY(adjoint_supported(f));
     if (!bytes) return PBD_ERR_NULL_ARG;
     Ws w;
-    return carve_ws(f, true, true, true, nullptr, w, bytes);
+    return carve_ws(f, true, true, true, precision, nullptr, w, bytes);
 }
 
 int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const double* sigma,
@@ -407,9 +431,9 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     if (with_range && (!didd_dr || !dsigma_dr)) return PBD_ERR_NULL_ARG;
     size_t need = 0;
     Ws ws;
-    PBD_TRY(carve_ws(f, true, true, true, nullptr, ws, &need));
+    PBD_TRY(carve_ws(f, true, true, true, precision, nullptr, ws, &need));
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
-    PBD_TRY(carve_ws(f, true, true, true, workspace, ws, &need));
+    PBD_TRY(carve_ws(f, true, true, true, precision, workspace, ws, &need));
     cudaStream_t s = (cudaStream_t)stream;
     JobPair p;
     memset(&p, 0, sizeof(p));
@@ -430,8 +454,7 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     count_launch(1);
     PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 1,
                            precision, s));
-    return launch_adjoint(ws.jobs + 1, &A, 1, ws.aitems, ws.a_items, ws.counters + 2, ws.a_chunk,
-                          with_range, 1, s);
+    return run_adjoint(ws, precision, &A, with_range, 1, s);
 }
 
 int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, size_t* bytes) {

@@ -245,6 +245,13 @@ __global__ void fwd_finalize_kernel(const JobDev* __restrict__ jobs, int with_lo
 
 }  // namespace
 
+int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs,
+                          cudaStream_t s) {
+    fwd_schedule_kernel<<<n_jobs, 256, 0, s>>>(jobs_dev, items, chunk);
+    PBD_LAUNCH_CHECK();
+    return PBD_OK;
+}
+
 int fwd_chunk_layers(const pbd_field* f) {
     // Default: ~4 layers per item keeps items small next to the ~2 CTAs per SM.
     (void)f;

@@ -112,6 +112,15 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
                    int total_items, int* counter, int chunk, int with_loss, int precision,
                    cudaStream_t s);
 
+// (slice, tile, layer-chunk) work items sorted longest-first, one CTA per job.
+int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
+
+// adjoint (tcgen05) -- adj_tc.cu; items are (slice, layer chunk) records as for the forward
+int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
+int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
+                      FwdItem* items, int total_items, int* counter, int chunk, int with_range,
+                      int finalize_loss, cudaStream_t s);
+
 // forward (tcgen05) -- tc_fwd.cu
 int tc_operand_dims(int precision, int nsx, int nsy, int* K1, int* N1);
 int launch_forward_tc_main(int precision, JobDev* jobs, FwdItem* items, int total, int* counter,

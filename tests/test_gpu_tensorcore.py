@@ -107,3 +107,78 @@ def test_tc_loss_grad_and_batch(pb):
     torch.cuda.synchronize()
     for d0, d1 in zip(b32.doses, btc.doses):
         assert rel(d1.cpu().numpy(), d0.cpu().numpy()) < 1e-6
+
+
+# ----------------------------------------------------------------------- adjoint
+def _oracle_grads(prob, w, idd, sig, didd, dsig, mask, presc):
+    import torch
+    from oracle import engine_ref as er
+    wt = torch.tensor(np.asarray(w, np.float64), requires_grad=True)
+    it = torch.tensor(np.asarray(idd, np.float64), requires_grad=True)
+    st = torch.tensor(np.asarray(sig, np.float64), requires_grad=True)
+    d = er.separable_torch(prob.grid.x, prob.grid.y, prob.lattice.spot_x, prob.lattice.spot_y,
+                           wt, it, st)
+    er.masked_quadratic_loss(d, torch.as_tensor(mask, dtype=torch.float64),
+                             torch.as_tensor(presc, dtype=torch.float64)).backward()
+    gr = (it.grad.numpy() * didd).sum(1) + (st.grad.numpy() * dsig).sum(1)
+    return wt.grad.numpy(), gr
+
+
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+def test_tc_adjoint_cfg0(pb, prec):
+    import torch
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    plan = pb.engines.DosePlan(prob, tables="device", precision=prec)
+    mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
+    presc = presc * 100.0
+    out = plan.loss_grad(torch.as_tensor(mask, device="cuda"), torch.as_tensor(presc, device="cuda"))
+    gw_ref, gr_ref = _oracle_grads(prob, wl["weights"], plan.idd.cpu().numpy(),
+                                   plan.sigma.cpu().numpy(), plan.didd.cpu().numpy(),
+                                   plan.dsig.cpu().numpy(), mask, presc)
+    ew = rel(out["grad_w"].cpu().numpy(), gw_ref)
+    er_ = rel(out["grad_range"].cpu().numpy(), gr_ref)
+    print(f"cfg0 adjoint {prec}: grad_w {ew:.3e} grad_range {er_:.3e}")
+    assert ew < 1e-4 and er_ < 1e-4
+    gw2, gr2 = plan.adjoint(out["grad_dose"])
+    assert rel(gw2.cpu().numpy(), out["grad_w"].cpu().numpy()) < 1e-6
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3"])
+def test_tc_adjoint_clinical(pb, prec):
+    import torch
+    wl = pb.workloads.build_workload(2)
+    lut = golden("luts_cfg1.npz")
+    prob = pb.model.problem_from_workload(wl, energies=lut["energies"])
+    plan = pb.engines.DosePlan(prob, tables="device", precision=prec)
+    out = plan.loss_grad(torch.as_tensor(wl["mask"], device="cuda"),
+                         torch.as_tensor(wl["presc"], device="cuda"))
+    gw_ref, gr_ref = _oracle_grads(prob, wl["weights"], plan.idd.cpu().numpy(),
+                                   plan.sigma.cpu().numpy(), plan.didd.cpu().numpy(),
+                                   plan.dsig.cpu().numpy(), wl["mask"], wl["presc"])
+    ew = rel(out["grad_w"].cpu().numpy(), gw_ref)
+    er_ = rel(out["grad_range"].cpu().numpy(), gr_ref)
+    print(f"clinical adjoint {prec}: grad_w {ew:.3e} grad_range {er_:.3e}")
+    assert ew < 1e-4 and er_ < 1e-4
+
+
+def test_tc_adjoint_wide_lattice_uses_fp32_adjoint(pb):
+    """51 spots in x exceed the TF32 tensor-core adjoint's shared memory: the FP32 adjoint
+    serves that field, with the tensor-core forward."""
+    import torch
+    M = pb.model
+    rng = np.random.default_rng(9)
+    grid = M.DoseGrid(64, 64, 24, 0.2, 0.2, 0.25, -6.3, -6.3, 0.0)
+    en = pr.layer_energies(3, 3.0, 5.0)
+    w = rng.uniform(0.5, 1.5, (3, 11, 51))
+    lat = M.SpotLattice(51, 11, 3, 0.25, 0.25, energies=en, weights=w)
+    idd, sig = pr.layer_luts(grid.z, en)
+    prob = M.PBProblem(grid, lat, idd, sig)
+    plan = pb.engines.DosePlan(prob, tables="device", precision="tf32x3")
+    g = torch.randn(grid.shape, device="cuda", dtype=torch.float32,
+                    generator=torch.Generator(device="cuda").manual_seed(3))
+    gw, _ = plan.adjoint(g)
+    ref = pb.engines.DosePlan(prob, tables="device", precision="fp32").adjoint(g)[0]
+    assert rel(gw.cpu().numpy(), ref.cpu().numpy()) < 1e-6
