@@ -322,8 +322,10 @@ def main():
     per_launch_flop = flops_eval / 2.0
     achieved = per_launch_flop / (dom_ms * 1e-3) / 1e12
     peak = float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops")))
-    kname = "adj_simt_kernel" if dom == "adjoint" else \
-        ("fwd_simt_kernel" if prec == "fp32" else "fwd_tc_kernel")
+    if dom == "adjoint":
+        kname = "adj_simt_kernel" if prec == "fp32" else "adj_tc_kernel"
+    else:
+        kname = "fwd_simt_kernel" if prec == "fp32" else "fwd_tc_kernel"
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": read_traffic(kname), "kernel": kname,
             "kernel_ms_per_launch": dom_ms, "flop_per_launch": per_launch_flop,

@@ -34,16 +34,25 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
+constexpr int kActStage = 40 * 1024;
+
 __global__ void adj_schedule_kernel(JobDev* jobs, AdjItem* items, int chunk) {
     const JobDev J = jobs[blockIdx.x];
+    extern __shared__ unsigned char sact[];
     __shared__ int cnt[kMaxChunkCost + 1];
     __shared__ int cur[kMaxChunkCost + 1];
     __shared__ int total;
     for (int c = threadIdx.x; c <= kMaxChunkCost; c += blockDim.x) cnt[c] = 0;
+    const bool staged = J.nl * J.nz <= kActStage;
+    if (staged)
+        for (int e = threadIdx.x; e < J.nl * J.nz; e += blockDim.x) sact[e] = J.idd[e] != 0.0;
     __syncthreads();
+    auto active = [&](int l, int z) {
+        return staged ? sact[l * J.nz + z] != 0 : J.idd[(size_t)l * J.nz + z] != 0.0;
+    };
     for (int l = threadIdx.x; l < J.nl; l += blockDim.x) {
         int a = 0;
-        for (int z = 0; z < J.nz; ++z) a += J.idd[(size_t)l * J.nz + z] != 0.0;
+        for (int z = 0; z < J.nz; ++z) a += active(l, z);
         const int nch = (a + chunk - 1) / chunk;
         J.nchunks[l] = nch;
         for (int k = 0; k < nch; ++k) atomicAdd(&cnt[min(chunk, a - k * chunk)], 1);
@@ -58,7 +67,7 @@ __global__ void adj_schedule_kernel(JobDev* jobs, AdjItem* items, int chunk) {
     for (int l = threadIdx.x; l < J.nl; l += blockDim.x) {
         int k = 0, in_chunk = 0, zb = 0, last = 0;
         for (int z = 0; z <= J.nz; ++z) {
-            const bool act = z < J.nz && J.idd[(size_t)l * J.nz + z] != 0.0;
+            const bool act = z < J.nz && active(l, z);
             if (act) {
                 if (in_chunk == 0) zb = z;
                 ++in_chunk;
@@ -321,7 +330,7 @@ int launch_adjoint(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, AdjIte
         attr_set = true;
     }
     PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, sizeof(int), s)));
-    adj_schedule_kernel<<<n_jobs, 256, 0, s>>>(jobs_dev, items, chunk);
+    adj_schedule_kernel<<<n_jobs, 256, kActStage, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();
     const int grid = max(1, min(total_items, num_sms()));
     prof_mark(kProfAdj, 0, s);

@@ -14,7 +14,7 @@
 //
 // Work item = (slice z, chunk of <= C active layers): G^T for the slice is rounded and
 // split into shared memory once per item.  dL/dW of a pair goes to its own (layer, slice)
-// slot and the finalize kernel sums the slots of a layer in slice order (deterministic).
+// slot and the finalize kernel sums the slots of a layer in a fixed order (deterministic).
 // One thread issues MMAs, tcgen05.commit signals mbarriers, every wait is bounded (2 s)
 // and on expiry the CTA sets the error word, drains, frees TMEM and leaves.
 // Grids of at most 128 x 128 voxels per slice; lattices up to 64 x 64 spots (48 in x
@@ -234,8 +234,10 @@ adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             const double c = J.idd[(size_t)l * nz + z];
             if (c == 0.0) continue;
             const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
-            const double a2 = kLog2e / (2.0 * s * s);
-            const double inv_s3 = 1.0 / (s * s * s), inv_s = 1.0 / s;
+            // d is formed in FP64 (voxel and spot coordinates of up to ~25 cm); d^2 and the
+            // exponent in FP32 (relative rounding ~1e-7 of the exponent)
+            const float a2 = (float)(kLog2e / (2.0 * s * s));
+            const float inv_s3 = (float)(1.0 / (s * s * s)), inv_s = (float)(1.0 / s);
 
             if (pend2) {
                 if (!drain()) { failed = true; break; }
@@ -253,8 +255,9 @@ adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                         if (j < nsy) {
                             const double d = (J.oy + (double)(y0 + q) * J.dy) -
                                              (J.sy0 + ((double)j - cy) * J.dsy);
-                            const float e = ex2_approx((float)(-(d * d) * a2));
-                            val = deriv ? e * (float)(d * d * inv_s3 - inv_s) : e;
+                            const float df = (float)d, dd = df * df;
+                            const float e = ex2_approx(-dd * a2);
+                            val = deriv ? e * fmaf(dd, inv_s3, -inv_s) : e;
                         }
                         v[q] = val;
                     }
@@ -288,8 +291,9 @@ adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                     if (i < nsx) {
                         const int x = gi * EPC + q;
                         const double d = (J.ox + (double)x * J.dx) - (J.sx0 + ((double)i - cx) * J.dsx);
-                        const float g = ex2_approx((float)(-(d * d) * a2));
-                        val = deriv ? g * (float)(d * d * inv_s3 - inv_s) : g;
+                        const float df = (float)d, dd = df * df;
+                        const float g = ex2_approx(-dd * a2);
+                        val = deriv ? g * fmaf(dd, inv_s3, -inv_s) : g;
                     }
                     v[q] = val;
                 }
@@ -363,24 +367,59 @@ adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
     if (warp == 0) tc::tmem_dealloc(tmem_base_s, kTmemCols);
 }
 
-// dL/dW_l = sum over active slices of the (l, z) slots, in slice order; dL/dR_l in FP64;
-// the loss total.  One block per (layer, job).
+// dL/dW_l = sum over active slices of the (l, z) slots in a fixed order (deterministic);
+// dL/dR_l in FP64; the loss total.  Grid (spot blocks of 128, layers, jobs): each block
+// first compacts the layer's active slices into shared memory, then every thread sums its
+// (j, i) entry over them with four independent accumulators (the loads of one slice are
+// coalesced).
 __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with_range,
                                        int finalize_loss, const int* __restrict__ err) {
-    const JobDev& J = jobs[blockIdx.y];
-    const int l = blockIdx.x;
+    const JobDev& J = jobs[blockIdx.z];
+    const int l = blockIdx.y;
     if (l >= J.nl) return;
     const int per = J.nsy * J.nsx;
     const bool bad = *err != 0;
     const double* idd = J.idd + (size_t)l * J.nz;
-    for (int r = threadIdx.x; r < per; r += blockDim.x) {
-        float s = bad ? __int_as_float(0x7fc00000) : 0.f;
-        for (int z = 0; z < J.nz; ++z)
-            if (idd[z] != 0.0) s += J.partial[((size_t)l * J.nz + z) * per + r];
-        J.grad_w[(size_t)l * per + r] = s;
+    __shared__ int zl[1024];
+    __shared__ int wcount[4];
+    __shared__ int nact;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    for (int zc = 0; zc < J.nz; zc += 1024) {
+        __syncthreads();
+        if (threadIdx.x == 0) nact = 0;
+        __syncthreads();
+        // order-preserving compaction of the active slices, 128 at a time (4 warp ballots)
+        for (int zb = zc; zb < min(J.nz, zc + 1024); zb += 128) {
+            const int z = zb + threadIdx.x;
+            const bool act = z < J.nz && z < zc + 1024 && idd[z] != 0.0;
+            const unsigned bal = __ballot_sync(0xffffffffu, act);
+            if (lane == 0) wcount[warp] = __popc(bal);
+            __syncthreads();
+            int off = nact;
+            for (int w = 0; w < warp; ++w) off += wcount[w];
+            if (act) zl[off + __popc(bal & ((1u << lane) - 1u))] = z;
+            __syncthreads();
+            if (threadIdx.x == 0) nact += wcount[0] + wcount[1] + wcount[2] + wcount[3];
+            __syncthreads();
+        }
+        if (r < per) {
+            const float* base = J.partial + (size_t)l * J.nz * per + r;
+            int k = 0;
+            for (; k + 4 <= nact; k += 4) {
+                a0 += base[(size_t)zl[k] * per];
+                a1 += base[(size_t)zl[k + 1] * per];
+                a2 += base[(size_t)zl[k + 2] * per];
+                a3 += base[(size_t)zl[k + 3] * per];
+            }
+            for (; k < nact; ++k) a0 += base[(size_t)zl[k] * per];
+        }
     }
-    if (with_range) {
-        __shared__ double redd[256];
+    if (r < per)
+        J.grad_w[(size_t)l * per + r] = bad ? __int_as_float(0x7fc00000) : (a0 + a1) + (a2 + a3);
+    if (with_range && blockIdx.x == 0) {
+        __shared__ double redd[128];
         double acc = 0.0;
         for (int z = threadIdx.x; z < J.nz; z += blockDim.x) {
             const size_t o = (size_t)l * J.nz + z;
@@ -395,7 +434,7 @@ __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with
         }
         if (threadIdx.x == 0) J.grad_range[l] = bad ? __int_as_float(0x7fc00000) : (float)redd[0];
     }
-    if (finalize_loss && l == 0 && threadIdx.x == 0) {
+    if (finalize_loss && l == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
         double s = 0.0;
         for (int b = 0; b < kLossBlocks; ++b) s += J.loss_part[b];
         *J.loss = s;
@@ -485,10 +524,13 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
             break;
     }
     PBD_TRY(rc);
-    int max_l = 1;
-    for (int j = 0; j < n_jobs; ++j) max_l = std::max(max_l, jobs_host[j].nl);
-    adj_tc_finalize_kernel<<<dim3(max_l, n_jobs), 256, 0, s>>>(jobs_dev, with_range, finalize_loss,
-                                                              counter + 1);
+    int max_l = 1, max_per = 1;
+    for (int j = 0; j < n_jobs; ++j) {
+        max_l = std::max(max_l, jobs_host[j].nl);
+        max_per = std::max(max_per, jobs_host[j].nsy * jobs_host[j].nsx);
+    }
+    adj_tc_finalize_kernel<<<dim3((max_per + 127) / 128, max_l, n_jobs), 128, 0, s>>>(
+        jobs_dev, with_range, finalize_loss, counter + 1);
     PBD_LAUNCH_CHECK();
     count_launch(3);
     return PBD_OK;

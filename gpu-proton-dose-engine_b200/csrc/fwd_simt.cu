@@ -33,17 +33,34 @@ __device__ __forceinline__ float ex2_approx(float x) {
 
 // Scheduler: one CTA per job.  Items are written to the job's segment of the flat
 // item array, bucket-sorted by cost (descending); unused slots get cost 0.
+// Activity flags (IDD != 0) of a job staged in shared memory when they fit.
+constexpr int kActStage = 40 * 1024;
+
+__device__ __forceinline__ bool active(const JobDev& J, const unsigned char* sact, bool staged,
+                                       int l, int z) {
+    return staged ? sact[l * J.nz + z] != 0 : J.idd[(size_t)l * J.nz + z] != 0.0;
+}
+
+__device__ __forceinline__ bool stage_activity(const JobDev& J, unsigned char* sact) {
+    const bool staged = J.nl * J.nz <= kActStage;
+    if (staged)
+        for (int e = threadIdx.x; e < J.nl * J.nz; e += blockDim.x) sact[e] = J.idd[e] != 0.0;
+    __syncthreads();
+    return staged;
+}
+
 __global__ void fwd_schedule_kernel(JobDev* jobs, FwdItem* items, int chunk) {
     const JobDev J = jobs[blockIdx.x];
+    extern __shared__ unsigned char sact[];
     __shared__ int cnt[kMaxChunkCost + 1];
     __shared__ int cur[kMaxChunkCost + 1];
     __shared__ int total;
     const int ntiles = J.ntx * J.nty;
     for (int c = threadIdx.x; c <= kMaxChunkCost; c += blockDim.x) cnt[c] = 0;
-    __syncthreads();
+    const bool staged = stage_activity(J, sact);
     for (int z = threadIdx.x; z < J.nz; z += blockDim.x) {
         int a = 0;
-        for (int l = 0; l < J.nl; ++l) a += J.idd[(size_t)l * J.nz + z] != 0.0;
+        for (int l = 0; l < J.nl; ++l) a += active(J, sact, staged, l, z);
         const int nch = (a + chunk - 1) / chunk;
         J.nchunks[z] = nch;
         for (int k = 0; k < nch; ++k) atomicAdd(&cnt[min(chunk, a - k * chunk)], ntiles);
@@ -58,7 +75,7 @@ __global__ void fwd_schedule_kernel(JobDev* jobs, FwdItem* items, int chunk) {
     for (int z = threadIdx.x; z < J.nz; z += blockDim.x) {
         int k = 0, in_chunk = 0, lb = 0, last = 0;
         for (int l = 0; l <= J.nl; ++l) {
-            const bool act = l < J.nl && J.idd[(size_t)l * J.nz + z] != 0.0;
+            const bool act = l < J.nl && active(J, sact, staged, l, z);
             if (act) {
                 if (in_chunk == 0) lb = l;
                 ++in_chunk;
@@ -247,7 +264,7 @@ __global__ void fwd_finalize_kernel(const JobDev* __restrict__ jobs, int with_lo
 
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs,
                           cudaStream_t s) {
-    fwd_schedule_kernel<<<n_jobs, 256, 0, s>>>(jobs_dev, items, chunk);
+    fwd_schedule_kernel<<<n_jobs, 256, kActStage, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();
     return PBD_OK;
 }
@@ -289,7 +306,7 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
         }
     }
     PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
-    fwd_schedule_kernel<<<n_jobs, 256, 0, s>>>(jobs_dev, items, chunk);
+    fwd_schedule_kernel<<<n_jobs, 256, kActStage, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();
     if (precision == PBD_PREC_FP32) {
         const int grid = max(1, min(total_items, 2 * num_sms()));

@@ -164,7 +164,7 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             const double c = J.idd[(size_t)l * nz + z];
             if (c == 0.0) continue;
             const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
-            const double a2 = kLog2e / (2.0 * s * s);
+            const float a2 = (float)(kLog2e / (2.0 * s * s));   // exponent scale, FP32
             const float scale = (float)(c * kInv2Pi / (s * s));
             const float* wl = J.w + (size_t)l * nsy * nsx;
 
@@ -178,7 +178,8 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                 for (int q = 0; q < P::EPC; ++q) {
                     const int i = g * P::EPC + q;
                     const double d = xv - (J.sx0 + ((double)i - cx) * J.dsx);
-                    v[q] = i < nsx ? ex2_approx((float)(-(d * d) * a2)) : 0.f;
+                    const float df = (float)d;
+                    v[q] = i < nsx ? ex2_approx(-(df * df) * a2) : 0.f;
                 }
                 uint4 hi, lo;
                 split_chunk<MODE>(v, hi, lo);
@@ -222,7 +223,8 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                 for (int q = 0; q < P::EPC; ++q) {
                     const int j = g * P::EPC + q;
                     const double d = yv - (J.sy0 + ((double)j - cy) * J.dsy);
-                    v[q] = j < nsy ? ex2_approx((float)(-(d * d) * a2)) : 0.f;
+                    const float df = (float)d;
+                    v[q] = j < nsy ? ex2_approx(-(df * df) * a2) : 0.f;
                 }
                 uint4 hi, lo;
                 split_chunk<MODE>(v, hi, lo);
