@@ -247,15 +247,17 @@ adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                 const int j = m & 63;
                 const bool deriv = m >= 64;
                 constexpr int VPS = P::EB == 4 ? 16 : 32;   // values per 16-column store
+                const double ysj = J.sy0 + ((double)j - cy) * J.dsy;
+                const float dyf = (float)J.dy;
                 for (int y0 = half * 64; y0 < half * 64 + 64; y0 += VPS) {
+                    // one FP64 difference per chunk, then FP32 steps of dy
+                    const float base = (float)((J.oy + (double)y0 * J.dy) - ysj);
                     float v[VPS];
 #pragma unroll
                     for (int q = 0; q < VPS; ++q) {
                         float val = 0.f;
                         if (j < nsy) {
-                            const double d = (J.oy + (double)(y0 + q) * J.dy) -
-                                             (J.sy0 + ((double)j - cy) * J.dsy);
-                            const float df = (float)d, dd = df * df;
+                            const float df = fmaf((float)q, dyf, base), dd = df * df;
                             const float e = ex2_approx(-dd * a2);
                             val = deriv ? e * fmaf(dd, inv_s3, -inv_s) : e;
                         }
@@ -284,14 +286,15 @@ adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
                 const int n = e % R2, gi = e / R2;
                 const int i = n < N1 ? n : n - N1;
                 const bool deriv = n >= N1;
+                const float base = (float)((J.ox + (double)(gi * EPC) * J.dx) -
+                                           (J.sx0 + ((double)i - cx) * J.dsx));
+                const float dxf = (float)J.dx;
                 float v[EPC];
 #pragma unroll
                 for (int q = 0; q < EPC; ++q) {
                     float val = 0.f;
                     if (i < nsx) {
-                        const int x = gi * EPC + q;
-                        const double d = (J.ox + (double)x * J.dx) - (J.sx0 + ((double)i - cx) * J.dsx);
-                        const float df = (float)d, dd = df * df;
+                        const float df = fmaf((float)q, dxf, base), dd = df * df;
                         const float g = ex2_approx(-dd * a2);
                         val = deriv ? g * fmaf(dd, inv_s3, -inv_s) : g;
                     }

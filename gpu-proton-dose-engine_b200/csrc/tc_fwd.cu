@@ -173,12 +173,17 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             for (int e = tid; e < 128 * g1; e += TNT) {
                 const int row = e & 127, g = e >> 7;
                 const double xv = J.ox + (double)(x0 + row) * J.dx;
+                // one FP64 difference per chunk (taken at the chunk's middle spot, so that
+                // |base - d| <= EPC/2 pitches), then one FP32 fma per spot: d is rounded
+                // once, and base's own rounding stays below 1e-7 cm for nearby spots
+                constexpr int MID = P::EPC / 2;
+                const float base = (float)(xv - (J.sx0 + ((double)(g * P::EPC + MID) - cx) * J.dsx));
+                const float dsf = (float)J.dsx;
                 float v[P::EPC];
 #pragma unroll
                 for (int q = 0; q < P::EPC; ++q) {
                     const int i = g * P::EPC + q;
-                    const double d = xv - (J.sx0 + ((double)i - cx) * J.dsx);
-                    const float df = (float)d;
+                    const float df = fmaf(-(float)(q - MID), dsf, base);
                     v[q] = i < nsx ? ex2_approx(-(df * df) * a2) : 0.f;
                 }
                 uint4 hi, lo;
@@ -218,12 +223,14 @@ fwd_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items
             for (int e = tid; e < 128 * g2; e += TNT) {
                 const int row = e & 127, g = e >> 7;
                 const double yv = J.oy + (double)(y0 + row) * J.dy;
+                constexpr int MID = P::EPC / 2;
+                const float base = (float)(yv - (J.sy0 + ((double)(g * P::EPC + MID) - cy) * J.dsy));
+                const float dsf = (float)J.dsy;
                 float v[P::EPC];
 #pragma unroll
                 for (int q = 0; q < P::EPC; ++q) {
                     const int j = g * P::EPC + q;
-                    const double d = yv - (J.sy0 + ((double)j - cy) * J.dsy);
-                    const float df = (float)d;
+                    const float df = fmaf(-(float)(q - MID), dsf, base);
                     v[q] = j < nsy ? ex2_approx(-(df * df) * a2) : 0.f;
                 }
                 uint4 hi, lo;

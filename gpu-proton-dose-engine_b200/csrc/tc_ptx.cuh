@@ -173,10 +173,11 @@ __host__ __device__ constexpr uint32_t instr_desc(int m, int n, uint32_t ab_fmt)
 }
 
 // ---- operand rounding -----------------------------------------------------------------
+// Round a finite float to TF32 (10 explicit mantissa bits), to nearest with ties away
+// from zero, with integer ops: add half a TF32 ulp to the magnitude bits and clear the
+// 13 low bits (a carry into the exponent is the correct rounding).
 __device__ __forceinline__ uint32_t to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
+    return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
 }
 
 }  // namespace tc
