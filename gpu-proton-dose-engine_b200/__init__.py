@@ -20,10 +20,10 @@ Modules
 """
 import sys as _sys
 
-from . import workloads, _lib, physics, model, engines, robust  # noqa: F401
+from . import workloads, _lib, physics, model, engines, robust, tuning  # noqa: F401
 
 __version__ = "0.1.0"
 
 _sys.modules.setdefault("pbdose_b200", _sys.modules[__name__])
-for _name in ("workloads", "_lib", "physics", "model", "engines", "robust"):
+for _name in ("workloads", "_lib", "physics", "model", "engines", "robust", "tuning"):
     _sys.modules.setdefault("pbdose_b200." + _name, _sys.modules[__name__ + "." + _name])

@@ -31,7 +31,7 @@ __global__ void install_jobs_kernel(JobPair p, JobDev* dst) {
 
 struct JobLite {
     int nx, ny, nz, nsx, nsy, nl;
-    int item_base, max_items, max_chunks, pad_;
+    int item_base, max_items, max_chunks, direct;   // direct: items write the output slice
     double ox, oy, dx, dy, sx0, sy0, dsx, dsy;
     const float* w;
     const double* idd;
@@ -59,7 +59,7 @@ __global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_bas
     J.ox = a.ox; J.oy = a.oy; J.dx = a.dx; J.dy = a.dy;
     J.sx0 = a.sx0; J.sy0 = a.sy0; J.dsx = a.dsx; J.dsy = a.dsy;
     J.w = a.w; J.idd = a.idd; J.sigma = a.sigma; J.dose = a.dose;
-    J.partial = partial_base + a.partial_off;
+    J.partial = a.direct ? a.dose : partial_base + a.partial_off;
     J.nchunks = nchunk_base + a.nchunk_off;
     dst[k] = J;
 }
@@ -457,36 +457,64 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     return run_adjoint(ws, precision, &A, with_range, 1, s);
 }
 
-int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, size_t* bytes) {
-    if (!jobs || !bytes) return PBD_ERR_NULL_ARG;
+// Planning of a batched launch (host).  When every job has at most kMaxChunkCost layers,
+// one work item covers all layers of a (job, slice, tile) and writes the output slice
+// directly ("direct" mode: no partial sums, no partial buffer; the many jobs keep the
+// grid balanced).  Otherwise items hold `chunk` layers and partial slices are summed.
+struct BatchPlan {
+    int chunk, direct, items;
+    size_t nch, part;
+};
+
+static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan* bp) {
+    if (!jobs) return PBD_ERR_NULL_ARG;
     if (n_jobs <= 0) return PBD_ERR_BAD_DIM;
     if (n_jobs > PBD_MAX_JOBS) return PBD_ERR_TOO_MANY;
     PBD_TRY(check_precision(precision));
-    Carve c(nullptr);
-    c.take<JobDev>(n_jobs);
-    c.take<int>(2);
-    size_t items = 0, nch = 0, part = 0;
+    int max_l = 0, chunk = kMaxChunkCost;
     for (int k = 0; k < n_jobs; ++k) {
         PBD_TRY(host_validate_field(&jobs[k].field));
         PBD_TRY(check_field_precision(&jobs[k].field, precision));
+        max_l = max_l > jobs[k].field.n_layers ? max_l : jobs[k].field.n_layers;
         const int ch = choose_fwd_chunk(&jobs[k].field);
+        chunk = ch < chunk ? ch : chunk;
+    }
+    bp->direct = (max_l <= kMaxChunkCost && g_fwd_chunk == 0) ? 1 : 0;
+    bp->chunk = bp->direct ? max_l : chunk;
+    size_t items = 0;
+    bp->nch = 0;
+    bp->part = 0;
+    for (int k = 0; k < n_jobs; ++k) {
         size_t pe = 0;
         int it = 0;
-        PBD_TRY(fwd_plan_sizes(&jobs[k].field, ch, &pe, &it));
+        PBD_TRY(fwd_plan_sizes(&jobs[k].field, bp->chunk, &pe, &it));
         items += it;
-        nch += jobs[k].field.nz;
-        part += pe;
+        bp->nch += jobs[k].field.nz;
+        bp->part += bp->direct ? 0 : pe;
     }
     if (items > (size_t)1 << 30) return PBD_ERR_UNSUPPORTED;
-    c.take<FwdItem>(items);
-    c.take<int>(nch);
-    c.take<float>(part);
+    bp->items = (int)items;
+    return PBD_OK;
+}
+
+int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, size_t* bytes) {
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    BatchPlan bp;
+    PBD_TRY(plan_batch(jobs, n_jobs, precision, &bp));
+    Carve c(nullptr);
+    c.take<JobDev>(n_jobs);
+    c.take<int>(2);
+    c.take<FwdItem>(bp.items);
+    c.take<int>(bp.nch);
+    c.take<float>(bp.part);
     *bytes = c.used + 256;
     return PBD_OK;
 }
 
 int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* workspace,
                       size_t workspace_bytes, void* stream) {
+    BatchPlan bp;
+    PBD_TRY(plan_batch(jobs, n_jobs, precision, &bp));
     size_t need = 0;
     PBD_TRY(pbd_forward_batch_workspace(jobs, n_jobs, precision, &need));
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
@@ -499,23 +527,18 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     t.n = n_jobs;
     int item_base = 0;
     size_t nch_off = 0, part_off = 0;
-    int chunk = kMaxChunkCost;
     JobDev host_view[PBD_MAX_JOBS];
-    for (int k = 0; k < n_jobs; ++k) {
-        const pbd_field* f = &jobs[k].field;
-        const int ch = choose_fwd_chunk(f);
-        chunk = ch < chunk ? ch : chunk;
-    }
     for (int k = 0; k < n_jobs; ++k) {
         const pbd_field* f = &jobs[k].field;
         size_t pe = 0;
         int it = 0;
-        PBD_TRY(fwd_plan_sizes(f, chunk, &pe, &it));
+        PBD_TRY(fwd_plan_sizes(f, bp.chunk, &pe, &it));
         JobLite& a = t.j[k];
         a.nx = f->nx; a.ny = f->ny; a.nz = f->nz; a.nsx = f->n_sx; a.nsy = f->n_sy;
         a.nl = f->n_layers;
         a.item_base = item_base; a.max_items = it;
-        a.max_chunks = (f->n_layers + chunk - 1) / chunk;
+        a.max_chunks = bp.direct ? 1 : (f->n_layers + bp.chunk - 1) / bp.chunk;
+        a.direct = bp.direct;
         a.ox = f->ox; a.oy = f->oy; a.dx = f->dx; a.dy = f->dy;
         a.sx0 = f->x0; a.sy0 = f->y0; a.dsx = f->dx_spot; a.dsy = f->dy_spot;
         a.w = jobs[k].w; a.idd = jobs[k].idd; a.sigma = jobs[k].sigma; a.dose = jobs[k].dose;
@@ -523,7 +546,7 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
         fill_job(f, &host_view[k]);
         item_base += it;
         nch_off += f->nz;
-        part_off += pe;
+        part_off += bp.direct ? 0 : pe;
     }
     Carve c(workspace);
     JobDev* jd = c.take<JobDev>(n_jobs);
@@ -535,7 +558,8 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, chunk, 0, precision, s);
+    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, bp.chunk, 0, precision,
+                          s);
 }
 
 }  // extern "C"

@@ -10,6 +10,7 @@ dose needs the built library and a CUDA device.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import time
 from typing import Optional
@@ -112,6 +113,9 @@ class DosePlan:
                                  device=self.device)
         self.energies = None if L.energies is None else np.asarray(L.energies, dtype=np.float64)
         self.ws = _Workspace(self.device)
+        self.schedule = None          # (layers per forward item, adjoint item size) or None
+        self._tuned = False           # cached tuning lookup (False = not looked up yet)
+        self._tuning_off = False
         self.tables_mode = tables
         self.range_shift = None
         if tables == "problem":
@@ -142,9 +146,23 @@ class DosePlan:
                             fd_step=self.fd_step, device=self.device)
         self.idd, self.sigma, self.didd, self.dsig = t.idd, t.sigma, t.didd_dr, t.dsigma_dr
         self.range_shift = None if range_shift is None else rs.clone()
+        self._tuned = False
 
     def active_pairs(self) -> int:
         return int((self.idd != 0).sum().item())
+
+    def _sched(self):
+        """Work-item sizes for this plan's calls: an explicit ``schedule``, else the tuned one
+        for this geometry (looked up once per set of tables), else the library default."""
+        from . import tuning
+        if self._tuning_off:
+            return contextlib.nullcontext()
+        s = self.schedule
+        if s is None:
+            if self._tuned is False:
+                self._tuned = tuning.lookup(self, "loss_grad")
+            s = self._tuned
+        return tuning.schedule(*s) if s else contextlib.nullcontext()
 
     # -- weights -----------------------------------------------------------------
     def _weights(self, w):
@@ -165,11 +183,12 @@ class DosePlan:
         sigma = self.sigma if sigma is None else sigma
         if out is None:
             out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
-        nbytes = _lib.query("pbd_forward_workspace", ctypes.byref(self.field), self.precision)
-        ws = self.ws.get("fwd", nbytes)
-        _lib.call("pbd_forward", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(idd),
-                  _lib.ptr(sigma), _lib.ptr(out), self.precision, _lib.ptr(ws), ws.numel(),
-                  _lib.stream_handle(self.device))
+        with self._sched():
+            nbytes = _lib.query("pbd_forward_workspace", ctypes.byref(self.field), self.precision)
+            ws = self.ws.get("fwd", nbytes)
+            _lib.call("pbd_forward", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(idd),
+                      _lib.ptr(sigma), _lib.ptr(out), self.precision, _lib.ptr(ws), ws.numel(),
+                      _lib.stream_handle(self.device))
         return out
 
     # -- adjoint -------------------------------------------------------------------
@@ -185,13 +204,14 @@ class DosePlan:
         g = grad_dose.to(self.device, torch.float32).contiguous()
         gw = torch.empty_like(w)
         gr = torch.zeros(w.shape[0], dtype=torch.float32, device=self.device) if with_range else None
-        nbytes = _lib.query("pbd_adjoint_workspace", ctypes.byref(self.field), self.precision)
-        ws = self.ws.get("adj", nbytes)
-        _lib.call("pbd_adjoint", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(idd),
-                  _lib.ptr(sigma), _lib.ptr(didd if with_range else None),
-                  _lib.ptr(dsig if with_range else None), _lib.ptr(g), _lib.ptr(gw),
-                  _lib.ptr(gr), self.precision, _lib.ptr(ws), ws.numel(),
-                  _lib.stream_handle(self.device))
+        with self._sched():
+            nbytes = _lib.query("pbd_adjoint_workspace", ctypes.byref(self.field), self.precision)
+            ws = self.ws.get("adj", nbytes)
+            _lib.call("pbd_adjoint", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(idd),
+                      _lib.ptr(sigma), _lib.ptr(didd if with_range else None),
+                      _lib.ptr(dsig if with_range else None), _lib.ptr(g), _lib.ptr(gw),
+                      _lib.ptr(gr), self.precision, _lib.ptr(ws), ws.numel(),
+                      _lib.stream_handle(self.device))
         return gw, gr
 
     # -- fused loss gradient -------------------------------------------------------
@@ -204,14 +224,17 @@ class DosePlan:
         w = self._weights(w)
         o = outputs or self.alloc_outputs()
         with_range = self.didd is not None
-        nbytes = _lib.query("pbd_loss_grad_workspace", ctypes.byref(self.field), self.precision)
-        ws = self.ws.get("lossgrad", nbytes)
-        _lib.call("pbd_loss_grad", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(self.idd),
-                  _lib.ptr(self.sigma), _lib.ptr(self.didd if with_range else None),
-                  _lib.ptr(self.dsig if with_range else None), _lib.ptr(mask), _lib.ptr(presc),
-                  _lib.ptr(o["dose"]), _lib.ptr(o["grad_dose"]), _lib.ptr(o["loss"]),
-                  _lib.ptr(o["grad_w"]), _lib.ptr(o["grad_range"] if with_range else None),
-                  self.precision, _lib.ptr(ws), ws.numel(), _lib.stream_handle(self.device))
+        with self._sched():
+            nbytes = _lib.query("pbd_loss_grad_workspace", ctypes.byref(self.field),
+                                self.precision)
+            ws = self.ws.get("lossgrad", nbytes)
+            _lib.call("pbd_loss_grad", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(self.idd),
+                      _lib.ptr(self.sigma), _lib.ptr(self.didd if with_range else None),
+                      _lib.ptr(self.dsig if with_range else None), _lib.ptr(mask),
+                      _lib.ptr(presc), _lib.ptr(o["dose"]), _lib.ptr(o["grad_dose"]),
+                      _lib.ptr(o["loss"]), _lib.ptr(o["grad_w"]),
+                      _lib.ptr(o["grad_range"] if with_range else None), self.precision,
+                      _lib.ptr(ws), ws.numel(), _lib.stream_handle(self.device))
         if not with_range:
             o = dict(o, grad_range=None)
         return o

@@ -31,7 +31,8 @@ class Scenario:
 class ScenarioBatch:
     """Fields x scenarios on one device, forward dose of every job per ``run()``."""
 
-    def __init__(self, problems, scenarios, *, precision="fp32", device=None):
+    def __init__(self, problems, scenarios, *, precision="fp32", device=None,
+                 with_grad: bool = False, fd_step: float = 0.005):
         torch = _lib.require_cuda()
         self.torch = torch
         self.device = torch.device(device or "cuda")
@@ -44,14 +45,18 @@ class ScenarioBatch:
         self.jobs = (_lib.Job * n_jobs)()
         self.keep = []
         self.doses = []
+        self.tables = []
+        self.weights = []
         k = 0
         for p in self.problems:
             g, L = p.grid, p.lattice
             w = torch.as_tensor(np.ascontiguousarray(L.ensure_weights(), dtype=np.float32),
                                 device=self.device)
+            self.weights.append(w)
             for s in self.scenarios:
                 t = ph.build_tables(g.nz, g.oz - s.dz, g.dz, L.energies, depth_scale=s.scale,
-                                    anchor_surface=True, device=self.device)
+                                    anchor_surface=True, device=self.device,
+                                    fd_step=fd_step if with_grad else 0.0)
                 d = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device=self.device)
                 f = p.field_descriptor()
                 f.x0 = L.x0 + s.dx
@@ -59,6 +64,7 @@ class ScenarioBatch:
                 self.jobs[k] = _lib.Job(field=f, w=_lib.ptr(w), idd=_lib.ptr(t.idd),
                                         sigma=_lib.ptr(t.sigma), dose=_lib.ptr(d))
                 self.keep += [w, t.idd, t.sigma]
+                self.tables.append(t)
                 self.doses.append(d)
                 k += 1
         self.n_jobs = n_jobs
@@ -95,3 +101,97 @@ class ScenarioBatch:
     def job_problem(self, k) -> tuple:
         """(problem, scenario) of job ``k``."""
         return self.problems[k // len(self.scenarios)], self.scenarios[k % len(self.scenarios)]
+
+    # -- plain per-job loop (the comparison the batch is measured against) -------------
+    def loop_forward(self, precision="fp32"):
+        """One ``pbd_forward`` call per job on the current stream (shared workspace, calls
+        ordered on the stream), e.g. the plain FP32 kernel looped over the scenarios."""
+        prec = _lib.precision_code(precision)
+        need = max(_lib.query("pbd_forward_workspace", ctypes.byref(self.jobs[k].field), prec)
+                   for k in range(self.n_jobs))
+        ws = self._ws("loop", need)
+        out = []
+        for k in range(self.n_jobs):
+            j = self.jobs[k]
+            d = self._loop_out(k)
+            _lib.call("pbd_forward", ctypes.byref(j.field), j.w, j.idd, j.sigma, _lib.ptr(d),
+                      prec, _lib.ptr(ws), ws.numel(), _lib.stream_handle(self.device))
+            out.append(d)
+        return out
+
+    def _loop_out(self, k):
+        if not hasattr(self, "_loop_doses"):
+            self._loop_doses = [torch_empty_like(d) for d in self.doses]
+        return self._loop_doses[k]
+
+    def _ws(self, name, nbytes):
+        bufs = self.__dict__.setdefault("_wsbufs", {})
+        b = bufs.get(name)
+        if b is None or b.numel() < nbytes:
+            b = self.torch.empty(max(nbytes, 256), dtype=self.torch.uint8, device=self.device)
+            bufs[name] = b
+        return b
+
+    # -- gradients of every job ----------------------------------------------------------
+    def alloc_grad_outputs(self):
+        torch = self.torch
+        outs = []
+        for k in range(self.n_jobs):
+            f = self.jobs[k].field
+            outs.append({"grad_dose": torch.empty((f.nz, f.ny, f.nx), dtype=torch.float32,
+                                                  device=self.device),
+                         "loss": torch.zeros((), dtype=torch.float64, device=self.device),
+                         "grad_w": torch.empty((f.n_layers, f.n_sy, f.n_sx), dtype=torch.float32,
+                                               device=self.device),
+                         "grad_range": torch.zeros(f.n_layers, dtype=torch.float32,
+                                                   device=self.device)})
+        self.grad_outputs = outs
+        return outs
+
+    def loss_grad_all(self, mask, presc):
+        """Forward, masked quadratic loss and adjoint of every (field, scenario) job, one
+        ``pbd_loss_grad`` call per job on the current stream with a shared workspace.
+        ``mask`` / ``presc``: one (nz, ny, nx) pair for all jobs (same grid)."""
+        if not getattr(self, "grad_outputs", None):
+            self.alloc_grad_outputs()
+        need = max(_lib.query("pbd_loss_grad_workspace", ctypes.byref(self.jobs[k].field),
+                              self.precision) for k in range(self.n_jobs))
+        ws = self._ws("grad", need)
+        st = _lib.stream_handle(self.device)
+        for k in range(self.n_jobs):
+            j, t, o = self.jobs[k], self.tables[k], self.grad_outputs[k]
+            if t.didd_dr is None:
+                raise RuntimeError("build the batch with with_grad=True for gradients")
+            _lib.call("pbd_loss_grad", ctypes.byref(j.field), j.w, j.idd, j.sigma,
+                      _lib.ptr(t.didd_dr), _lib.ptr(t.dsigma_dr), _lib.ptr(mask), _lib.ptr(presc),
+                      j.dose, _lib.ptr(o["grad_dose"]), _lib.ptr(o["loss"]), _lib.ptr(o["grad_w"]),
+                      _lib.ptr(o["grad_range"]), self.precision, _lib.ptr(ws), ws.numel(), st)
+        return self.grad_outputs
+
+    def capture_loss_grad(self, mask, presc):
+        """Capture ``loss_grad_all`` into a CUDA graph (replay with ``replay_loss_grad``)."""
+        torch = self.torch
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.loss_grad_all(mask, presc)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.loss_grad_all(mask, presc)
+        self.grad_graph = g
+        return g
+
+    def replay_loss_grad(self):
+        self.grad_graph.replay()
+        return self.grad_outputs
+
+
+def torch_empty_like(t):
+    return t.new_empty(t.shape)
+
+
+def robust_problems(fields):
+    """PBProblem of each workload field (``workloads.robust_fields``), tables on the device."""
+    from .model import problem_from_workload
+    return [problem_from_workload(f) for f in fields]
