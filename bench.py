@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--precision", default=None)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="clinical", choices=["clinical", "robust", "precision"],
+                    help="clinical: the headline gradient workload; robust: 4 fields x 25 "
+                    "scenarios batched; precision: forward error vs FP64 per precision mode")
     return ap.parse_args()
 
 
@@ -224,11 +227,152 @@ def reference_arm(args):
     return 0
 
 
+# --------------------------------------------------------------------------- side workloads
+def _timed(torch, dev, fn, steps, flush):
+    """Mean ms of ``fn`` over ``steps`` calls, CUDA events around each call, L2 flushed
+    (256 MiB write) before each one, outside the events."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record()
+        fn()
+        ev[k][1].record()
+    torch.cuda.synchronize(dev)
+    return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+
+def robust_bench(args):
+    """4 uneven fields x 25 setup/range scenarios (100 doses on 128^3) per step.
+
+    Three legs, each timed with L2 flushed between steps: a loop of one plain FP32
+    ``pbd_forward`` per job (the per-scenario baseline), the batched forward of every job
+    in one persistent launch replayed from a CUDA graph, and the loss gradient of every
+    job (``pbd_loss_grad`` per job) replayed from a CUDA graph."""
+    import torch
+    pb = importlib.import_module("gpu-proton-dose-engine_b200")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    prec = args.precision or "tf32x3"
+    fields = pb.workloads.robust_fields()
+    scen = pb.workloads.robust_scenarios()
+    probs = pb.robust.robust_problems(fields)
+    sb = pb.robust.ScenarioBatch(probs, scen, precision=prec, device=dev, with_grad=True)
+    g = fields[0]["grid"]
+    m_np, p_np = pb.workloads.target_loss_arrays(g)
+    m = torch.as_tensor(m_np, device=dev)
+    p = torch.as_tensor(p_np, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    lib = pb._lib
+    K, W = args.steps, max(args.warmup, 3)
+    clocks = ClockSampler(0)
+    clocks.start()
+    for _ in range(W):
+        sb.loop_forward("fp32")
+    t_loop = _timed(torch, dev, lambda: sb.loop_forward("fp32"), K, flush)
+    sb.capture()
+    for _ in range(W):
+        sb.replay()
+    n0 = lib.launch_count()
+    t_batch = _timed(torch, dev, sb.replay, K, flush)
+    sb.capture_loss_grad(m, p)
+    for _ in range(W):
+        sb.replay_loss_grad()
+    t_grad = _timed(torch, dev, sb.replay_loss_grad, K, flush)
+    clk = clocks.stop()
+    # graph replays do not pass through the host launch counter: count one replay's kernels
+    n1 = lib.launch_count()
+    sb.run()
+    torch.cuda.synchronize(dev)
+    per_batch = lib.launch_count() - n1
+    sb.loss_grad_all(m, p)
+    torch.cuda.synchronize(dev)
+    per_grad = lib.launch_count() - n1 - per_batch
+    del n0
+    worst = 0.0
+    sb.loop_forward("fp32")
+    sb.run()
+    torch.cuda.synchronize(dev)
+    for a, b in zip(sb.doses, sb._loop_doses):
+        worst = max(worst, float((a.double() - b.double()).abs().max() / b.double().abs().max()))
+    n = sb.n_jobs
+    line = {"workload": "robust", "metric": "robust scenario doses/s, 4 fields x 25 scenarios "
+            "on 128^3", "value": n * 1e3 / t_batch, "unit": "doses/s", "n_gpus": 1, "steps": K,
+            "warmup": W, "ms_per_step": t_batch, "higher_is_better": True, "dtype": prec,
+            "data": "synthetic",
+            "config": {"workload": "4 fields (21x21x16, 33x33x28, 41x41x40, 51x41x48 spots x "
+                       "layers) x 25 scenarios, 128^3 voxels of 2 mm", "jobs": n,
+                       "precision": prec, "l2": "flushed between steps"},
+            "legs_ms": {"fp32_loop_per_job_forward": t_loop, "batched_forward_graph": t_batch,
+                        "per_job_loss_grad_graph": t_grad},
+            "speedup_batched_vs_fp32_loop": t_loop / t_batch,
+            "grad_evals_per_s": n * 1e3 / t_grad,
+            "gpu_launches_per_replay": {"batched_forward": per_batch, "loss_grad": per_grad},
+            "batched_vs_fp32_loop_max_rel": worst, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def precision_bench(args):
+    """Forward of the 200x200x256 / 61x61x60 field in every precision mode: time per call
+    (L2 flushed between calls) and error against the FP64 oracle on the host."""
+    import torch
+    from oracle import engine_ref as er
+    pb = importlib.import_module("gpu-proton-dose-engine_b200")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    wl = pb.workloads.build_workload(4)
+    prob = pb.model.problem_from_workload(wl)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    K, W = args.steps, max(args.warmup, 3)
+    base = pb.engines.DosePlan(prob, tables="device", precision="fp32", device=dev)
+    idd = base.idd.cpu().numpy()
+    sig = base.sigma.cpu().numpy()
+    g, L = prob.grid, prob.lattice
+    t0 = time.perf_counter()
+    ref = er.separable_torch(g.x, g.y, L.spot_x, L.spot_y, wl["weights"], idd, sig,
+                              layer_chunk=2).numpy()
+    t_ref = time.perf_counter() - t0
+    active = base.active_pairs()
+    flop = 2 * active * (L.n_sx * L.n_sy * g.ny + g.nx * L.n_sx * g.ny)
+    clocks = ClockSampler(0)
+    clocks.start()
+    modes = {}
+    for mode in ("fp32", "tf32x3", "bf16x3", "tf32", "bf16"):
+        plan = base if mode == "fp32" else pb.engines.DosePlan(prob, tables="device",
+                                                                precision=mode, device=dev)
+        plan.idd, plan.sigma = base.idd, base.sigma
+        out = torch.empty(plan.shape, dtype=torch.float32, device=dev)
+        for _ in range(W):
+            plan.forward(out=out)
+        ms = _timed(torch, dev, lambda: plan.forward(out=out), K, flush)
+        err = pb.engines.relative_error(out, ref)
+        modes[mode] = {"ms": ms, "tflops_credited": flop / (ms * 1e-3) / 1e12,
+                       "max_rel_err": err["max_rel_err_global"],
+                       "rms_rel_err": err["rms_rel_global"]}
+    clk = clocks.stop()
+    line = {"workload": "precision", "metric": "forward ms and error vs FP64 oracle per precision "
+            "mode", "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": K, "warmup": W,
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "grid": [g.nx, g.ny, g.nz], "spots": L.n_spots,
+                       "layers": L.n_layers, "active_pairs": active, "credited_flop": flop,
+                       "l2": "flushed between calls",
+                       "oracle": f"torch CPU float64 port, {t_ref:.1f} s"},
+            "modes": modes, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # --------------------------------------------------------------------------- our arm
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "robust":
+        return robust_bench(args)
+    if args.workload == "precision":
+        return precision_bench(args)
     import torch
     import torch.distributed as dist
 
