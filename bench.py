@@ -41,7 +41,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default=None)
+    ap.add_argument("--precision", default=None,
+                    help="fp32 | tf32x3 | bf16x3 | tf32 | bf16; the clinical workload defaults "
+                    "to tf32x3 (tcgen05, <= 1e-6 of max against FP64)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="clinical", choices=["clinical", "robust", "precision"],
@@ -94,6 +96,14 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait (<= 10 s) for its first sample so that the
+        # timed region, which can be well under a second, is covered
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -385,7 +395,7 @@ def main():
                                 device_id=dev)
     pb, wl = workload_arrays()
     lib = pb._lib
-    prec = args.precision or pb.engines.DEFAULT_PRECISION
+    prec = args.precision or "tf32x3"
     prob = pb.model.problem_from_workload(wl)
     plan = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
     active = plan.active_pairs()
