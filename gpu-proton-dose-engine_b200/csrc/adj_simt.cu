@@ -276,11 +276,14 @@ __global__ void adj_finalize_kernel(const JobDev* __restrict__ jobs, int with_ra
     const JobDev& J = jobs[blockIdx.y];
     const int per_layer = J.nsy * J.nsx;
     const size_t n = (size_t)J.nl * per_layer;
+    // a timed-out wait of a tensor-core forward leaves dL/dD invalid: poison the results
+    const bool bad = J.fwd_err != nullptr && *J.fwd_err != 0;
+    const float nan = __int_as_float(0x7fc00000);
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
          e += (size_t)gridDim.x * blockDim.x) {
         const int l = (int)(e / per_layer), r = (int)(e % per_layer);
         const int nch = J.nchunks[l];
-        float s = 0.f;
+        float s = bad ? nan : 0.f;
         for (int k = 0; k < nch; ++k)
             s += J.partial[((size_t)l * J.max_chunks + k) * per_layer + r];
         J.grad_w[e] = s;
@@ -294,13 +297,13 @@ __global__ void adj_finalize_kernel(const JobDev* __restrict__ jobs, int with_ra
                     if (J.idd[o] == 0.0) continue;
                     acc += (double)J.dc[o] * J.didd_dr[o] + (double)J.dsg[o] * J.dsig_dr[o];
                 }
-                J.grad_range[l] = (float)acc;
+                J.grad_range[l] = bad ? nan : (float)acc;
             }
         }
         if (finalize_loss && threadIdx.x == 0) {
             double s = 0.0;
-            for (int b = 0; b < kLossBlocks; ++b) s += J.loss_part[b];
-            *J.loss = s;
+            for (int b = 0; b < J.n_loss_part; ++b) s += J.loss_part[b];
+            *J.loss = bad ? (double)nan : s;
         }
     }
 }

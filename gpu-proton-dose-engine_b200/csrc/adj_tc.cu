@@ -381,7 +381,7 @@ __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with
     const int l = blockIdx.y;
     if (l >= J.nl) return;
     const int per = J.nsy * J.nsx;
-    const bool bad = *err != 0;
+    const bool bad = *err != 0 || (J.fwd_err != nullptr && *J.fwd_err != 0);
     const double* idd = J.idd + (size_t)l * J.nz;
     __shared__ int zl[1024];
     __shared__ int wcount[4];
@@ -439,8 +439,8 @@ __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with
     }
     if (finalize_loss && l == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
         double s = 0.0;
-        for (int b = 0; b < kLossBlocks; ++b) s += J.loss_part[b];
-        *J.loss = s;
+        for (int b = 0; b < J.n_loss_part; ++b) s += J.loss_part[b];
+        *J.loss = bad ? (double)__int_as_float(0x7fc00000) : s;
     }
 }
 

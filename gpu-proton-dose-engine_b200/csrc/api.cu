@@ -37,7 +37,7 @@ struct JobLite {
     const double* idd;
     const double* sigma;
     float* dose;
-    size_t partial_off, nchunk_off;
+    size_t partial_off, nchunk_off, arrive_off;
 };
 
 struct JobTable {
@@ -46,7 +46,8 @@ struct JobTable {
 };
 static_assert(sizeof(JobTable) < 32000, "kernel parameter limit");
 
-__global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_base, int* nchunk_base) {
+__global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_base, int* nchunk_base,
+                                     int* arrive_base) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= t.n) return;
     const JobLite& a = t.j[k];
@@ -61,6 +62,7 @@ __global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_bas
     J.w = a.w; J.idd = a.idd; J.sigma = a.sigma; J.dose = a.dose;
     J.partial = a.direct ? a.dose : partial_base + a.partial_off;
     J.nchunks = nchunk_base + a.nchunk_off;
+    J.arrive = arrive_base + a.arrive_off;
     dst[k] = J;
 }
 
@@ -75,8 +77,8 @@ struct ProfState {
 };
 thread_local ProfState g_prof;
 
-int choose_fwd_chunk(const pbd_field* f) {
-    int c = g_fwd_chunk > 0 ? g_fwd_chunk : fwd_chunk_layers(f);
+int choose_fwd_chunk(const pbd_field* f, int precision) {
+    int c = g_fwd_chunk > 0 ? g_fwd_chunk : fwd_chunk_layers(f, precision);
     return c < 1 ? 1 : (c > kMaxChunkCost ? kMaxChunkCost : c);
 }
 int choose_adj_chunk(const pbd_field* f) {
@@ -106,7 +108,11 @@ int adjoint_supported(const pbd_field* f) {
 // Workspace of the single-job paths.
 struct Ws {
     JobDev* jobs;        // [0] forward view, [1] adjoint view
-    int* counters;       // [0] forward items, [1] forward error word, [2] adjoint items
+    int* counters;       // [0] forward items, [1] forward error word, [2] adjoint items,
+                         // [3] adjoint error word; then the forward's arrival counters
+    int* farr;           // tensor-core forward: per (slice, tile) arrival counters
+    size_t n_fcount;     // ints the forward clears at launch (counters + arrivals)
+    int n_loss_part;
     FwdItem* fitems;
     int* fnch;
     float* fpart;
@@ -124,8 +130,13 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
              size_t* used) {
     Carve c(base);
     w.jobs = c.take<JobDev>(2);
-    w.counters = c.take<int>(8);
-    w.f_chunk = choose_fwd_chunk(f);
+    const int tiles = ((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile);
+    const size_t narr = fwd ? (size_t)f->nz * tiles * kTcFwdWarps : 0;
+    w.counters = c.take<int>(8 + narr);
+    w.farr = w.counters ? w.counters + 8 : nullptr;
+    w.n_fcount = 8 + narr;
+    w.n_loss_part = precision == PBD_PREC_FP32 ? kLossBlocks : f->nz * tiles * kTcFwdWarps;
+    w.f_chunk = choose_fwd_chunk(f, precision);
     w.a_chunk = choose_adj_chunk(f);
     w.fitems = nullptr; w.fnch = nullptr; w.fpart = nullptr; w.loss_part = nullptr;
     w.aitems = nullptr; w.anch = nullptr; w.apart = nullptr; w.dc = nullptr; w.dsg = nullptr;
@@ -137,7 +148,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
         w.fnch = c.take<int>(f->nz);
         w.fpart = c.take<float>(pe);
     }
-    if (loss) w.loss_part = c.take<double>(kLossBlocks);
+    if (loss) w.loss_part = c.take<double>(w.n_loss_part);
     w.adj_tc = 0;
     if (adj) {
         size_t pe = 0;
@@ -338,12 +349,12 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
     J.w = w; J.idd = idd; J.sigma = sigma; J.dose = dose;
     J.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
     J.item_base = 0; J.max_items = ws.f_items;
-    J.partial = ws.fpart; J.nchunks = ws.fnch;
+    J.partial = ws.fpart; J.nchunks = ws.fnch; J.arrive = ws.farr;
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 0,
-                          precision, s);
+    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
+                          ws.f_chunk, 0, precision, 1, s);
 }
 
 static int run_adjoint(const Ws& ws, int precision, const JobDev* A, int with_range,
@@ -443,17 +454,19 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     F.w = w; F.idd = idd; F.sigma = sigma; F.didd_dr = didd_dr; F.dsig_dr = dsigma_dr;
     F.dose = dose; F.mask = mask; F.presc = presc; F.grad_dose = grad_dose;
     F.loss_part = ws.loss_part; F.loss = loss; F.grad_w = grad_w; F.grad_range = grad_range;
+    F.n_loss_part = ws.n_loss_part;
     JobDev A = F;
     F.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
     F.item_base = 0; F.max_items = ws.f_items;
-    F.partial = ws.fpart; F.nchunks = ws.fnch;
+    F.partial = ws.fpart; F.nchunks = ws.fnch; F.arrive = ws.farr;
     fill_adj_view(f, ws, A);
+    A.fwd_err = ws.counters + 1;
     p.j[1] = A;
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.f_chunk, 1,
-                           precision, s));
+    PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
+                           ws.f_chunk, 1, precision, 0, s));
     return run_adjoint(ws, precision, &A, with_range, 1, s);
 }
 
@@ -463,7 +476,7 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
 // grid balanced).  Otherwise items hold `chunk` layers and partial slices are summed.
 struct BatchPlan {
     int chunk, direct, items;
-    size_t nch, part;
+    size_t nch, part, arr;
 };
 
 static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan* bp) {
@@ -476,7 +489,7 @@ static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan*
         PBD_TRY(host_validate_field(&jobs[k].field));
         PBD_TRY(check_field_precision(&jobs[k].field, precision));
         max_l = max_l > jobs[k].field.n_layers ? max_l : jobs[k].field.n_layers;
-        const int ch = choose_fwd_chunk(&jobs[k].field);
+        const int ch = choose_fwd_chunk(&jobs[k].field, precision);
         chunk = ch < chunk ? ch : chunk;
     }
     bp->direct = (max_l <= kMaxChunkCost && g_fwd_chunk == 0) ? 1 : 0;
@@ -484,12 +497,16 @@ static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan*
     size_t items = 0;
     bp->nch = 0;
     bp->part = 0;
+    bp->arr = 0;
     for (int k = 0; k < n_jobs; ++k) {
         size_t pe = 0;
         int it = 0;
         PBD_TRY(fwd_plan_sizes(&jobs[k].field, bp->chunk, &pe, &it));
         items += it;
         bp->nch += jobs[k].field.nz;
+        const pbd_field& f = jobs[k].field;
+        bp->arr += (size_t)f.nz * ((f.nx + kTile - 1) / kTile) * ((f.ny + kTile - 1) / kTile) *
+                   kTcFwdWarps;
         bp->part += bp->direct ? 0 : pe;
     }
     if (items > (size_t)1 << 30) return PBD_ERR_UNSUPPORTED;
@@ -503,7 +520,7 @@ int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, 
     PBD_TRY(plan_batch(jobs, n_jobs, precision, &bp));
     Carve c(nullptr);
     c.take<JobDev>(n_jobs);
-    c.take<int>(2);
+    c.take<int>(2 + bp.arr);
     c.take<FwdItem>(bp.items);
     c.take<int>(bp.nch);
     c.take<float>(bp.part);
@@ -526,7 +543,7 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     memset(&t, 0, sizeof(t));
     t.n = n_jobs;
     int item_base = 0;
-    size_t nch_off = 0, part_off = 0;
+    size_t nch_off = 0, part_off = 0, arr_off = 0;
     JobDev host_view[PBD_MAX_JOBS];
     for (int k = 0; k < n_jobs; ++k) {
         const pbd_field* f = &jobs[k].field;
@@ -542,24 +559,26 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
         a.ox = f->ox; a.oy = f->oy; a.dx = f->dx; a.dy = f->dy;
         a.sx0 = f->x0; a.sy0 = f->y0; a.dsx = f->dx_spot; a.dsy = f->dy_spot;
         a.w = jobs[k].w; a.idd = jobs[k].idd; a.sigma = jobs[k].sigma; a.dose = jobs[k].dose;
-        a.partial_off = part_off; a.nchunk_off = nch_off;
+        a.partial_off = part_off; a.nchunk_off = nch_off; a.arrive_off = arr_off;
         fill_job(f, &host_view[k]);
         item_base += it;
         nch_off += f->nz;
+        arr_off += (size_t)f->nz * ((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile) *
+                   kTcFwdWarps;
         part_off += bp.direct ? 0 : pe;
     }
     Carve c(workspace);
     JobDev* jd = c.take<JobDev>(n_jobs);
-    int* counter = c.take<int>(2);
+    int* counter = c.take<int>(2 + arr_off);
     FwdItem* items = c.take<FwdItem>(item_base);
     int* nchb = c.take<int>(nch_off);
     float* partb = c.take<float>(part_off);
     cudaStream_t s = (cudaStream_t)stream;
-    install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb);
+    install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb, counter + 2);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, bp.chunk, 0, precision,
-                          s);
+    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, 2 + arr_off, bp.chunk,
+                          0, precision, 1, s);
 }
 
 }  // extern "C"

@@ -269,10 +269,12 @@ int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_job
     return PBD_OK;
 }
 
-int fwd_chunk_layers(const pbd_field* f) {
-    // Default: ~4 layers per item keeps items small next to the ~2 CTAs per SM.
+int fwd_chunk_layers(const pbd_field* f, int precision) {
+    // FP32: ~4 layers per item keeps items small next to the ~2 CTAs per SM.  Tensor cores:
+    // the pipeline runs across unit boundaries, so larger units only save partial slices
+    // (16 measured best on the 128^3 / 41 x 41 x 40 field; the autotuner refines it).
     (void)f;
-    return 4;
+    return precision == PBD_PREC_FP32 ? 4 : 16;
 }
 
 int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items) {
@@ -286,37 +288,29 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 }
 
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
-                   int total_items, int* counter, int chunk, int with_loss, int precision,
-                   cudaStream_t s) {
-    int K1 = 0, N1 = 0;
+                   int total_items, int* counter, size_t n_counter_ints, int chunk, int with_loss,
+                   int precision, int poison, cudaStream_t s) {
     if (precision != PBD_PREC_FP32) {
-        for (int j = 0; j < n_jobs; ++j) {
-            int k1 = 0, n1 = 0;
-            PBD_TRY(tc_operand_dims(precision, jobs_host[j].nsx, jobs_host[j].nsy, &k1, &n1));
-            K1 = max(K1, k1);
-            N1 = max(N1, n1);
-        }
-    } else {
-        static thread_local bool attr_set = false;
-        if (!attr_set) {
-            if (cudaFuncSetAttribute(fwd_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kFwdSmemBytes) != cudaSuccess)
-                return PBD_ERR_NO_SMEM;
-            attr_set = true;
-        }
+        PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, n_counter_ints * sizeof(int), s)));
+        return launch_forward_tc(precision, jobs_dev, jobs_host, n_jobs, counter, chunk,
+                                 with_loss, poison, s);
+    }
+    static thread_local bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(fwd_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kFwdSmemBytes) != cudaSuccess)
+            return PBD_ERR_NO_SMEM;
+        attr_set = true;
     }
     PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
     fwd_schedule_kernel<<<n_jobs, 256, kActStage, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();
-    if (precision == PBD_PREC_FP32) {
+    {
         const int grid = max(1, min(total_items, 2 * num_sms()));
         prof_mark(kProfFwd, 0, s);
         fwd_simt_kernel<<<grid, NT, kFwdSmemBytes, s>>>(jobs_dev, items, total_items, counter);
         PBD_LAUNCH_CHECK();
         prof_mark(kProfFwd, 1, s);
-    } else {
-        PBD_TRY(launch_forward_tc_main(precision, jobs_dev, items, total_items, counter,
-                                       counter + 1, K1, N1, s));
     }
     int max_blocks = 1;
     for (int j = 0; j < n_jobs; ++j) {

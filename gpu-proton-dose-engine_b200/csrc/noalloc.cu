@@ -103,5 +103,5 @@ extern "C" int pbd_forward_noalloc(const pbd_field* f, const float* w, const dou
     noalloc_install_kernel<<<1, 32, 0, s>>>(J, jd);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(jd, &J, 1, it, items, counters, chunk, 0, precision, s);
+    return launch_forward(jd, &J, 1, it, items, counters, 2, chunk, 0, precision, 1, s);
 }

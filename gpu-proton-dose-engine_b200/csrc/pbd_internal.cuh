@@ -22,7 +22,7 @@ struct JobDev {
     int ntx, nty;                 // lateral tiles of 128 x 128 voxels
     int max_chunks;               // forward: layer chunks per depth slice; adjoint: z chunks per layer
     int item_base, max_items;     // slice of the flat item array owned by this job
-    int pad_;
+    int n_loss_part;              // loss partial sums written by the forward (summed in order)
     double ox, oy, dx, dy;        // voxel centres x = ox + k dx
     double sx0, sy0, dsx, dsy;    // spot centres xs = sx0 + (i - (nsx-1)/2) dsx
     const float* w;               // (nl, nsy, nsx)
@@ -33,6 +33,8 @@ struct JobDev {
     float* dose;                  // (nz, ny, nx)
     float* partial;               // forward: (max_chunks, nz, ny, nx); adjoint: (nl, max_chunks, nsy, nsx)
     int* nchunks;                 // forward: (nz); adjoint: (nl)
+    int* arrive;                  // tensor-core forward: chunks of each (slice, tile) written so far
+    const int* fwd_err;           // adjoint view: the forward's error word (poisons the results)
     const float* mask;            // loss
     const float* presc;
     float* grad_dose;             // (nz, ny, nx): written by the loss, read by the adjoint
@@ -52,6 +54,8 @@ constexpr int kSpotChunk = 64;      // spots per lattice chunk in the FP32 forwa
 constexpr int kAdjMaxSpots = 64;    // adjoint lattice limit per axis
 constexpr int kMaxChunkCost = 64;   // largest layers-per-item / z-per-item
 constexpr int kLossBlocks = 296;    // fixed grid of the loss reduction (deterministic order)
+constexpr int kTcFwdWarps = 8;      // math warps of the tensor-core forward: each owns 32 rows x
+                                    // 64 columns of a tile, its own arrival counter and loss partial
 
 // ---------------------------------------------------------------------------
 // small helpers
@@ -105,12 +109,15 @@ int host_validate_field(const pbd_field* f);
 int num_sms();
 
 // forward (FP32 SIMT) -- fwd_simt.cu
-int fwd_chunk_layers(const pbd_field* f);
+int fwd_chunk_layers(const pbd_field* f, int precision);
 int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items);
 // counter[0] = item counter, counter[1] = error word (set by a timed-out device wait).
+// FP32 path: schedule + persistent kernel + finalize.  Tensor-core precisions go to
+// launch_forward_tc after clearing `n_counter_ints` ints from `counter` (the counters and
+// the jobs' arrival arrays, laid out contiguously by the caller).
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
-                   int total_items, int* counter, int chunk, int with_loss, int precision,
-                   cudaStream_t s);
+                   int total_items, int* counter, size_t n_counter_ints, int chunk, int with_loss,
+                   int precision, int poison, cudaStream_t s);
 
 // (slice, tile, layer-chunk) work items sorted longest-first, one CTA per job.
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
@@ -121,10 +128,15 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
                       FwdItem* items, int total_items, int* counter, int chunk, int with_range,
                       int finalize_loss, cudaStream_t s);
 
-// forward (tcgen05) -- tc_fwd.cu
+// forward (tcgen05) -- tc_fwd.cu.  Work units (slice, layer chunk, tile) are enumerated
+// z-major; counter[0] = unit counter, counter[1] = error word; every job's `arrive` array
+// (nz * tiles ints, only read when a slice spans several chunks) must be zero at launch.
+// `poison`: a follow-up kernel turns every job's dose into NaN if a device wait ran out.
 int tc_operand_dims(int precision, int nsx, int nsy, int* K1, int* N1);
-int launch_forward_tc_main(int precision, JobDev* jobs, FwdItem* items, int total, int* counter,
-                           int* err, int K1, int N1, cudaStream_t s);
+int tc_forward_units(const JobDev* jobs_host, int n_jobs, int chunk, int* cmax, int* tmax,
+                     int* n_units);
+int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
+                      int* counter, int chunk, int with_loss, int poison, cudaStream_t s);
 
 // adjoint (FP32 SIMT) -- adj_simt.cu
 int adj_chunk_depths(const pbd_field* f);
