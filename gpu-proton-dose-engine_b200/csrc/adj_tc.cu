@@ -1,7 +1,8 @@
-// adj_tc.cu -- adjoint of the separable dose on the tensor cores (tcgen05).
+// adj_tc.cu -- adjoint of the separable dose on the tensor cores (tcgen05), warp-specialised
+// and software-pipelined across (layer, slice) pairs.
 //
-// Same mathematics as adj_simt.cu.  With G = dL/dD[z] and unnormalised Gaussians of
-// width s = sigma_l(z), for every active (layer l, slice z):
+// Same mathematics as adj_simt.cu.  With G = dL/dD[z] and unnormalised Gaussians of width
+// s = sigma_l(z), for every active (layer l, slice z):
 //
 //   stage 1   Y[m, x] = sum_y A[m, y] G[y, x]        A = [Gy | Gy']^T, m < 64: j, m >= 64: j'
 //             M = 128 (m), N = 128 (x), K = 128 (y); A generated into TMEM, G^T in smem
@@ -10,16 +11,40 @@
 //
 // P = Q[j, i] gives dL/dW_l += IDD P / (2 pi s^2) and dL/dIDD = <P, W> / (2 pi s^2);
 // Q[j, i'] + Q[j', i] gives dL/dsigma = IDD <., W> / (2 pi s^2) (G' = dG/ds).  The
-// Gaussian factors are regenerated per (layer, slice); nothing is stored.
+// Gaussian factors are regenerated per pair; nothing Gaussian is stored in HBM.
 //
-// Work item = (slice z, chunk of <= C active layers): G^T for the slice is rounded and
-// split into shared memory once per item.  dL/dW of a pair goes to its own (layer, slice)
-// slot and the finalize kernel sums the slots of a layer in a fixed order (deterministic).
-// One thread issues MMAs, tcgen05.commit signals mbarriers, every wait is bounded (2 s)
-// and on expiry the CTA sets the error word, drains, frees TMEM and leaves.
-// Grids of at most 128 x 128 voxels per slice; lattices up to 64 x 64 spots (48 in x
-// for the TF32 modes, whose operands take twice the shared memory).
+// Precision.  The contraction runs in split BF16 (hi + lo, three products, FP32
+// accumulation) for every split or TF32 mode and in plain BF16 for the BF16 mode: the
+// gradients need 1e-4 and the split form keeps ~16 mantissa bits (measured ~1e-6 of the
+// largest gradient), and BF16 operands halve the MMA count and the on-chip footprint
+// against TF32, which is what lets the pipeline below double-buffer.
+//
+// CTA = 8 math warps, a scheduler warp, two MMA warps (one per stage); one CTA per SM.
+//  * Scheduler warp: units (slice z, chunk of <= C active layers) from an atomic counter
+//    in z-major order; one step per active layer into an 8-slot ring (full / empty
+//    mbarriers).
+//  * Math warps, per pair n (buffer b = n & 1), without block barriers:
+//      at a unit's first pair: G^T of the slice, split, into smem (the previous unit's last
+//          stage 1 is complete: it was waited for before this pair)
+//      G   A = [Gy | Gy']^T -> TMEM A[b] (tcgen05.st); arrive on ops1
+//      DR  pair n-1's Q from TMEM: Q / (2 pi s^2) into three (layer, slice) slots --
+//          P = Q[j, i], A = Q[j, i'], B = Q[j', i] -- stored transposed ([i][j]) so that a
+//          warp's 32 lanes write 128 contiguous bytes
+//      B   [Gx | Gx'] -> smem (read by stage 2 only, whose previous use DR waited for);
+//          each Gaussian value and its derivative come from one exp
+//      E1  Y of pair n from TMEM, split, back into TMEM A[b]; arrive on ops2
+//  * MMA warp 1: stage 1 after ops1 (A from TMEM, "TS" form), commit to mma1.
+//    MMA warp 2: stage 2 after ops2 (A = split Y from TMEM), commit to mma2.
+//  Stage 2 of pair n-1 runs under G of pair n; stage 1 of pair n under DR and B.
+//
+// dL/dW_l = sum over active slices of IDD * slot P in slice order, and the dot products
+// <slot, W> for dL/dIDD and dL/dsigma, are formed by two small follow-up kernels in a fixed
+// order (deterministic).  Every wait is bounded (2 s of %globaltimer); a warp whose wait
+// runs out sets the error word and leaves, the others' waits then run out in turn, and
+// the finalize pass turns the gradients into NaN.
+// Grids of at most 128 x 128 voxels per slice; lattices up to 64 x 64 spots.
 #include <algorithm>
+#include <math.h>
 
 #include "pbd_internal.cuh"
 #include "tc_common.cuh"
@@ -28,365 +53,554 @@ namespace pbd {
 namespace {
 using namespace tcc;
 
-constexpr int TNT = 256;
-constexpr uint32_t kTmemCols = 512;   // A [0,256), Y [256,384), Q [384, 384 + 2 N1)
+constexpr int kMathWarps = 8;
+constexpr int kMath = 32 * kMathWarps;     // 256 math threads: warpgroups 0 and 1
+constexpr int kSchedWarp = kMathWarps;     // warpgroup 2: warp 8 schedules, warp 9 issues
+constexpr int kS1Warp = kMathWarps + 1;    // stage 1, warp 10 stage 2, warp 11 idle
+constexpr int kS2Warp = kMathWarps + 2;
+constexpr int kThreads = kMath + 128;
+constexpr int kRing = 8;
+constexpr uint32_t kCols = 512;
+// Register split (setmaxnreg) as in the forward: 8 * 32 * 208 + 4 * 32 * 80 <= 384 * 168.
+constexpr int kMathRegs = 208, kCtrlRegs = 80;
+constexpr int kLaunchRegsNeeded = (kMath * kMathRegs + 128 * kCtrlRegs + kThreads - 1) / kThreads;
+// TMEM columns: A[0] [0,128), A[1] [128,256) (bf16 pairs: hi [0,64), lo [64,128) of each),
+// Y [256,384), Q [384, 384 + 2 N1)
+constexpr uint32_t kColA = 0, kColY = 256, kColQ = 384;
+constexpr uint32_t kLoOff = 64;
 
-template <int MODE>
-struct AdjOps {
-    using P = Prec<MODE>;
-    // TMEM columns per MMA k-step (8 tf32, or 16 bf16 packed two per column) and the
-    // offset of the lo part of an A operand.
-    static constexpr uint32_t kColsPerStep = 8;
-    static constexpr uint32_t kLoOff = P::EB == 4 ? 128u : 64u;
+enum : int { kFirst = 1, kLast = 2, kEnd = 4 };
 
-    __device__ static void mma(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-        if (P::EB == 4) tc::mma_tf32_ts(d, a, b, idesc, acc);
-        else tc::mma_bf16_ts(d, a, b, idesc, acc);
-    }
-    // D = A (TMEM, K = 128) x B^T (smem, K-major, `rows` rows) with the 3 or 1 products.
-    __device__ static void issue(uint32_t d, uint32_t a, uint8_t* const* b, uint32_t plane_b,
-                                 uint32_t idesc) {
-        uint32_t acc = 0;
-        for (int st = 0; st < 128 / P::KSTEP; ++st) {
-            const uint32_t ac = a + (uint32_t)st * kColsPerStep;
-            const uint32_t ob = (uint32_t)st * 2u * plane_b;
-            const uint64_t bh = tc::smem_desc(tc::smem_u32(b[0]) + ob, plane_b, 128);
-            if (P::NPROD == 3) {
-                const uint64_t bl = tc::smem_desc(tc::smem_u32(b[1]) + ob, plane_b, 128);
-                mma(d, ac, bl, idesc, acc);          // small products first
-                mma(d, ac + kLoOff, bh, idesc, 1u);
-                acc = 1;
-            }
-            mma(d, ac, bh, idesc, acc);
-            acc = 1;
-        }
-    }
+struct Step {
+    int job, z, l, flags;
+    float a2, inv_s, inv_s3, nrm;   // exponent scale, 1/s, 1/s^3, 1/(2 pi s^2)
 };
 
-// Round 16 (tf32) or 32 (bf16) values to hi / lo words for a TMEM store of 16 columns.
-template <int MODE>
-__device__ __forceinline__ void pack16(const float* v, uint32_t (&hi)[16], uint32_t (&lo)[16]) {
-    using P = Prec<MODE>;
-    if constexpr (P::EB == 4) {
+struct Params {
+    const JobDev* jobs;
+    int n_jobs, chunk, cmax, n_units;
+    int* counter;        // [0] unit counter, [1] error word
+    int N1;              // x-lattice padded to 16
+};
+
+struct Layout {
+    uint32_t gth, gtl, b2, b2_lo;
+};
+
+template <int NARR>
+__device__ __forceinline__ Layout make_layout(int N1) {
+    const uint32_t gt = 128u * 128u * 2u, b2 = 2u * (uint32_t)N1 * 128u * 2u;
+    Layout L;
+    L.gth = 0;
+    L.gtl = NARR == 2 ? gt : 0u;
+    L.b2 = (uint32_t)NARR * gt;
+    L.b2_lo = NARR == 2 ? b2 : 0u;
+    return L;
+}
+
+// Split 8 floats into packed bf16 hi / lo words (lo = bf16 of the remainder).
+template <int NARR>
+__device__ __forceinline__ void split8(const float* v, uint4& hi, uint4& lo) {
+    uint32_t h[4], l[4];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            hi[q] = tc::to_tf32(v[q]);
-            lo[q] = P::NPROD == 3 ? tc::to_tf32(v[q] - __uint_as_float(hi[q])) : 0u;
+    for (int q = 0; q < 4; ++q) {
+        const uint32_t ha = bf16_bits(v[2 * q]), hb = bf16_bits(v[2 * q + 1]);
+        h[q] = ha | (hb << 16);
+        if (NARR == 2) {
+            const float ra = v[2 * q] - __uint_as_float(ha << 16);
+            const float rb = v[2 * q + 1] - __uint_as_float(hb << 16);
+            l[q] = bf16_bits(ra) | (bf16_bits(rb) << 16);
+        } else {
+            l[q] = 0u;
         }
-    } else {
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const uint32_t ha = bf16_bits(v[2 * q]), hb = bf16_bits(v[2 * q + 1]);
-            hi[q] = ha | (hb << 16);
-            if (P::NPROD == 3) {
-                const float ra = v[2 * q] - __uint_as_float(ha << 16);
-                const float rb = v[2 * q + 1] - __uint_as_float(hb << 16);
-                lo[q] = bf16_bits(ra) | (bf16_bits(rb) << 16);
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// ------------------------------------------------------------------------------------------
+// Scheduler warp: units (z, chunk) -> one step per active layer.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint64_t* full,
+                                               uint64_t* empty) {
+    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    int k = 0;
+    bool ok = true;
+    auto push = [&](int src, const Step& st) -> bool {
+        const int slot = k % kRing, n = k / kRing;
+        const bool w = wait_bar(&empty[slot], (uint32_t)((n & 1) ^ 1));
+        if (!__all_sync(FULL, w)) return false;
+        if (lane == src) {
+            ring[slot] = st;
+            tc::mbar_arrive(&full[slot]);
+        }
+        __syncwarp();
+        ++k;
+        return true;
+    };
+    for (;;) {
+        int u = 0;
+        if (lane == 0) u = atomicAdd(P.counter, 1);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= P.n_units) break;
+        int v = u;
+        const int job = v % P.n_jobs; v /= P.n_jobs;
+        const int c = v % P.cmax;
+        const int z = v / P.cmax;
+        const JobDev& J = P.jobs[job];
+        const int nz = J.nz, nl = J.nl;
+        if (z >= nz) continue;
+        const double* idd = J.idd;
+        int tot = 0;
+        for (int b = 0; b < nl; b += 32) {
+            const int l = b + lane;
+            const bool a = l < nl && idd[(size_t)l * nz + z] != 0.0;
+            tot += __popc(__ballot_sync(FULL, a));
+        }
+        const int r0 = c * P.chunk;
+        if (r0 >= tot) continue;   // no chunk c here (slices no layer reaches carry no gradient)
+        const int r1 = min(tot, r0 + P.chunk);
+        int rank = 0;
+        for (int b = 0; b < nl && rank < r1 && ok; b += 32) {
+            const int l = b + lane;
+            const double iv = l < nl ? idd[(size_t)l * nz + z] : 0.0;
+            const bool a = iv != 0.0;
+            const unsigned bal = __ballot_sync(FULL, a);
+            const int my = rank + __popc(bal & ((1u << lane) - 1u));
+            const bool mine = a && my >= r0 && my < r1;
+            Step st{};
+            if (mine) {
+                const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
+                st.job = job; st.z = z; st.l = l;
+                st.flags = (my == r0 ? kFirst : 0) | (my == r1 - 1 ? kLast : 0);
+                st.a2 = (float)(kLog2e / (2.0 * s * s));
+                st.inv_s = (float)(1.0 / s);
+                st.inv_s3 = (float)(1.0 / (s * s * s));
+                st.nrm = (float)(kInv2Pi / (s * s));
+            }
+            unsigned emit = __ballot_sync(FULL, mine);
+            while (emit) {
+                const int src = __ffs(emit) - 1;
+                emit &= emit - 1u;
+                if (!push(src, st)) { ok = false; break; }
+            }
+            rank += __popc(bal);
+        }
+        if (!ok) break;
+    }
+    if (ok) {
+        Step st{};
+        st.flags = kEnd;
+        (void)push(0, st);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// MMA warps.  stage 1: Y = A[b] (TMEM, K = y) x G^T (smem rows x); stage 2: Q = Y split
+// (TMEM A[b], K = x) x B2^T (smem rows n).  One accumulator per stage (gradients carry a
+// 1e-4 tolerance), the three products of a k-step issued back to back.
+// ------------------------------------------------------------------------------------------
+template <int MODE>
+__device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint32_t sbase,
+                                         uint32_t tb, int stage, const Step* ring,
+                                         uint64_t* full, uint64_t* empty, uint64_t* bars) {
+    using Pr = Prec<MODE>;
+    const int lane = threadIdx.x & 31;
+    uint64_t* ops = bars + (stage == 1 ? 0 : 1);
+    uint64_t* done = bars + (stage == 1 ? 2 : 3);
+    const uint32_t R2 = 2u * (uint32_t)P.N1;
+    const uint32_t idesc = tc::instr_desc(128, stage == 1 ? 128 : (int)R2, Pr::FMT);
+    const uint32_t plane_b = stage == 1 ? 128u * 16u : R2 * 16u;
+    int k = 0, n = 0;
+    bool ok = true;
+    for (;;) {
+        const int slot = k % kRing;
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1));
+        const int flags = ring[slot].flags;
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[slot]);
+        ++k;
+        if (!__all_sync(0xffffffffu, ok)) break;
+        if (flags & kEnd) break;
+        ok = wait_bar(ops, (uint32_t)(n & 1));
+        if (!__all_sync(0xffffffffu, ok)) break;
+        tc::fence_after_sync();
+        if (lane == 0) {
+            const uint32_t a = tb + kColA + (uint32_t)(n & 1) * 128u;
+            const uint32_t d = tb + (stage == 1 ? kColY : kColQ);
+            uint32_t bh, bl;
+            if (stage == 1) {
+                bh = sbase + L.gth;
+                bl = sbase + L.gtl;
             } else {
-                lo[q] = 0u;
+                bh = sbase + L.b2;
+                bl = bh + L.b2_lo;
+            }
+            for (int st = 0; st < 128 / 16; ++st) {
+                const uint32_t ob = (uint32_t)st * 2u * plane_b;
+                const uint32_t ac = a + (uint32_t)st * 8u;
+                const uint64_t dh = tc::smem_desc(bh + ob, plane_b, 128);
+                if (Pr::NPROD == 3) {
+                    const uint64_t dl = tc::smem_desc(bl + ob, plane_b, 128);
+                    tc::mma_bf16_ts(d, ac, dl, idesc, st > 0 ? 1u : 0u);
+                    tc::mma_bf16_ts(d, ac + kLoOff, dh, idesc, 1u);
+                    tc::mma_bf16_ts(d, ac, dh, idesc, 1u);
+                } else {
+                    tc::mma_bf16_ts(d, ac, dh, idesc, st > 0 ? 1u : 0u);
+                }
+            }
+            tc::commit(done);
+        }
+        __syncwarp();
+        ++n;
+    }
+    if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
+    if (n > 0) (void)wait_bar(done, (uint32_t)((n - 1) & 1));
+}
+
+// ------------------------------------------------------------------------------------------
+// Math warps.
+// ------------------------------------------------------------------------------------------
+template <int MODE>
+__device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uint8_t* smem,
+                                           uint32_t tb, const Step* ring, uint64_t* full,
+                                           uint64_t* empty, uint64_t* bars) {
+    using Pr = Prec<MODE>;
+    constexpr int NARR = Pr::NPROD == 3 ? 2 : 1;
+    uint64_t* ops1 = bars + 0;
+    uint64_t* ops2 = bars + 1;
+    uint64_t* mma1 = bars + 2;
+    uint64_t* mma2 = bars + 3;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int sp = warp & 3, half = warp >> 2;
+    const uint32_t lane_base = (uint32_t)(32 * sp) << 16;
+    const int m = 32 * sp + lane;          // TMEM lane: row m of A, Y, Q
+    const int jrow = m & 63;
+    const bool deriv = m >= 64;
+    const int N1 = P.N1, R2 = 2 * N1;
+    const uint32_t planeR2 = (uint32_t)R2 * 16u;
+
+    uint32_t ph1 = 0, ph2 = 0;
+    bool ok = true;
+    Step prev{};
+    bool have_prev = false;
+    int k = 0, n = 0;
+    float ybase = 0.f;                     // (y0 of this thread's columns) - ys_j, per unit
+
+    for (;;) {
+        const int slot = k % kRing;
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1));
+        const Step cur = ring[slot];
+        if (cur.flags != kEnd && (cur.job < 0 || cur.job >= P.n_jobs)) ok = false;
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[slot]);
+        ++k;
+        if (!__all_sync(0xffffffffu, ok)) break;
+        if (cur.flags & kEnd) break;
+        const JobDev& J = P.jobs[cur.job];
+        const int nx = J.nx, ny = J.ny, nsx = J.nsx, nsy = J.nsy;
+        const int b = n & 1;
+        const float a2 = cur.a2, inv_s = cur.inv_s, inv_s3 = cur.inv_s3;
+
+        // ---- unit start: G^T of the slice (rows x, K = y; zero outside the grid) ----
+        if (cur.flags & kFirst) {
+            const float* g = J.grad_dose + (size_t)cur.z * ny * nx;
+#pragma unroll 2
+            for (int r = 0; r < 8; ++r) {
+                const int e = tid + r * kMath;
+                const int x = e & 127, c = e >> 7;
+                float v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int y = c * 8 + q;
+                    v[q] = (y < ny && x < nx) ? g[(size_t)y * nx + x] : 0.f;
+                }
+                uint4 hi, lo;
+                split8<NARR>(v, hi, lo);
+                const uint32_t off = (uint32_t)c * 2048u + (uint32_t)x * 16u;
+                *reinterpret_cast<uint4*>(smem + L.gth + off) = hi;
+                if (NARR == 2) *reinterpret_cast<uint4*>(smem + L.gtl + off) = lo;
+            }
+            const double cy = 0.5 * (double)(nsy - 1);
+            ybase = (float)((J.oy + (double)(64 * half) * J.dy) - (J.sy0 + ((double)jrow - cy) * J.dsy));
+        }
+
+        // ---- G: A = [Gy | Gy']^T -> TMEM A[b] (row m, y columns [64 half, +64)) ----
+        {
+            const float dyf = (float)J.dy;
+            const bool valid = jrow < nsy;
+            uint32_t hi[2][16], lo[2][16];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                float v2[2];
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const float d = fmaf((float)(2 * q + t), dyf, ybase), dd = d * d;
+                    const float e = ex2_approx(-dd * a2);
+                    v2[t] = valid ? (deriv ? e * fmaf(dd, inv_s3, -inv_s) : e) : 0.f;
+                }
+                const uint32_t ha = bf16_bits(v2[0]), hb = bf16_bits(v2[1]);
+                hi[q >> 4][q & 15] = ha | (hb << 16);
+                if (NARR == 2)
+                    lo[q >> 4][q & 15] = bf16_bits(v2[0] - __uint_as_float(ha << 16)) |
+                                         (bf16_bits(v2[1] - __uint_as_float(hb << 16)) << 16);
+            }
+            const uint32_t col = kColA + (uint32_t)b * 128u + (uint32_t)(32 * half);
+            tc::tmem_st16(tb + lane_base + col, hi[0]);
+            tc::tmem_st16(tb + lane_base + col + 16u, hi[1]);
+            if (NARR == 2) {
+                tc::tmem_st16(tb + lane_base + col + kLoOff, lo[0]);
+                tc::tmem_st16(tb + lane_base + col + kLoOff + 16u, lo[1]);
+            }
+        }
+        tc::tmem_wait_st();
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(ops1);
+
+        // ---- DR: Q of the previous pair -> the three slots ----
+        if (have_prev) {
+            ok = ok && wait_bar(mma2, ph2);
+            if (ok) ph2 ^= 1;
+            if (!__all_sync(0xffffffffu, ok)) break;
+            tc::fence_after_sync();
+            const JobDev& Jp = P.jobs[prev.job];
+            const int pnsx = Jp.nsx, pnsy = Jp.nsy;
+            const size_t per = (size_t)pnsy * pnsx;
+            // which slot this warp's quarter of Q feeds (warp-uniform): (j, i) -> P,
+            // (j, i') -> A, (j', i) -> B; the (j', i') quarter is not needed.  tcgen05.ld is
+            // warp-collective, so the whole warp loads and only the lanes of real rows store.
+            const int which = deriv ? (half == 0 ? 2 : -1) : half;
+            if (which >= 0) {
+                float* slot_base = Jp.partial + (size_t)which * Jp.nl * Jp.nz * per +
+                                   ((size_t)prev.l * Jp.nz + prev.z) * per;
+                const bool row_ok = jrow < pnsy;
+                for (int c0 = 0; c0 < N1; c0 += 16) {
+                    uint32_t r[16];
+                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(half * N1 + c0), r);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int i = c0 + q;
+                        if (row_ok && i < pnsx)
+                            slot_base[(size_t)i * pnsy + jrow] = prev.nrm * __uint_as_float(r[q]);
+                    }
+                }
+            }
+        }
+
+        // ---- B2 = [Gx | Gx'] -> smem (rows i and N1 + i, K = x).  Only stage 2 reads it,
+        // and the previous pair's stage 2 is complete (DR waited), so one buffer serves. ----
+        {
+            const uint32_t ob2 = L.b2;
+            const double cx = 0.5 * (double)(nsx - 1);
+            const float dxf = (float)J.dx;
+            const int items = N1 * 16;   // (i, x-chunk of 8)
+            for (int e = tid; e < items; e += kMath) {
+                const int i = e % N1, c = e / N1;
+                const float base = (float)((J.ox + (double)(8 * c) * J.dx) - (J.sx0 + ((double)i - cx) * J.dsx));
+                float g0[8], g1[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float d = fmaf((float)q, dxf, base), dd = d * d;
+                    const float ev = i < nsx ? ex2_approx(-dd * a2) : 0.f;
+                    g0[q] = ev;
+                    g1[q] = ev * fmaf(dd, inv_s3, -inv_s);
+                }
+                uint4 h0, l0, h1, l1;
+                split8<NARR>(g0, h0, l0);
+                split8<NARR>(g1, h1, l1);
+                const uint32_t o0 = ob2 + (uint32_t)c * planeR2 + (uint32_t)i * 16u;
+                const uint32_t o1 = o0 + (uint32_t)N1 * 16u;
+                *reinterpret_cast<uint4*>(smem + o0) = h0;
+                *reinterpret_cast<uint4*>(smem + o1) = h1;
+                if (NARR == 2) {
+                    *reinterpret_cast<uint4*>(smem + o0 + L.b2_lo) = l0;
+                    *reinterpret_cast<uint4*>(smem + o1 + L.b2_lo) = l1;
+                }
+            }
+        }
+        // ---- E1: Y of this pair -> split -> TMEM A[b] (row m, x columns [64 half, +64)) ----
+        ok = ok && wait_bar(mma1, ph1);
+        if (ok) ph1 ^= 1;
+        if (!__all_sync(0xffffffffu, ok)) break;
+        tc::fence_after_sync();
+        {
+            uint32_t r[4][16];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                tc::tmem_ld16(tb + lane_base + kColY + (uint32_t)(64 * half + 16 * c), r[c]);
+            tc::tmem_wait_ld();
+            uint32_t hi[2][16], lo[2][16];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const float va = __uint_as_float(r[q >> 3][(2 * q) & 15]);
+                const float vb = __uint_as_float(r[q >> 3][(2 * q + 1) & 15]);
+                const uint32_t ha = bf16_bits(va), hb = bf16_bits(vb);
+                hi[q >> 4][q & 15] = ha | (hb << 16);
+                if (NARR == 2)
+                    lo[q >> 4][q & 15] = bf16_bits(va - __uint_as_float(ha << 16)) |
+                                         (bf16_bits(vb - __uint_as_float(hb << 16)) << 16);
+            }
+            const uint32_t col = kColA + (uint32_t)b * 128u + (uint32_t)(32 * half);
+            tc::tmem_st16(tb + lane_base + col, hi[0]);
+            tc::tmem_st16(tb + lane_base + col + 16u, hi[1]);
+            if (NARR == 2) {
+                tc::tmem_st16(tb + lane_base + col + kLoOff, lo[0]);
+                tc::tmem_st16(tb + lane_base + col + kLoOff + 16u, lo[1]);
+            }
+        }
+        tc::tmem_wait_st();
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(ops2);
+        prev = cur;
+        have_prev = true;
+        ++n;
+    }
+    // last pair's Q
+    if (ok && have_prev) {
+        ok = wait_bar(mma2, ph2);
+        if (__all_sync(0xffffffffu, ok)) {
+            tc::fence_after_sync();
+            const JobDev& Jp = P.jobs[prev.job];
+            const int pnsx = Jp.nsx, pnsy = Jp.nsy;
+            const size_t per = (size_t)pnsy * pnsx;
+            // which slot this warp's quarter of Q feeds (warp-uniform): (j, i) -> P,
+            // (j, i') -> A, (j', i) -> B; the (j', i') quarter is not needed.  tcgen05.ld is
+            // warp-collective, so the whole warp loads and only the lanes of real rows store.
+            const int which = deriv ? (half == 0 ? 2 : -1) : half;
+            if (which >= 0) {
+                float* slot_base = Jp.partial + (size_t)which * Jp.nl * Jp.nz * per +
+                                   ((size_t)prev.l * Jp.nz + prev.z) * per;
+                const bool row_ok = jrow < pnsy;
+                for (int c0 = 0; c0 < N1; c0 += 16) {
+                    uint32_t r[16];
+                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(half * N1 + c0), r);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int i = c0 + q;
+                        if (row_ok && i < pnsx)
+                            slot_base[(size_t)i * pnsy + jrow] = prev.nrm * __uint_as_float(r[q]);
+                    }
+                }
             }
         }
     }
-}
-
-__device__ __forceinline__ float block_sum256(float v, float* red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    __syncthreads();
-    if (ln == 0) red[w] = v;
-    __syncthreads();
-    float s = 0.f;
-    if (threadIdx.x < 32) {
-        s = ln < TNT / 32 ? red[ln] : 0.f;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    }
-    return s;   // valid in thread 0
+    if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(TNT, 1)
-adj_tc_kernel(const JobDev* __restrict__ jobs, const FwdItem* __restrict__ items, int total,
-              int* counter, int* err, int N1) {
-    using P = Prec<MODE>;
-    using O = AdjOps<MODE>;
-    constexpr int NARR = P::NPROD == 3 ? 2 : 1;
-    constexpr int EPC = P::EPC;
+__global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
+    constexpr int NARR = Prec<MODE>::NPROD == 3 ? 2 : 1;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t full[kRing];
+    __shared__ __align__(8) uint64_t empty[kRing];
+    __shared__ __align__(8) uint64_t bars[4];   // ops1, ops2, mma1, mma2
+    __shared__ Step ring[kRing];
     __shared__ uint32_t tmem_base_s;
-    __shared__ int s_item;
-    __shared__ float red[2][TNT / 32];
 
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int R2 = 2 * N1;
-    const uint32_t gt_bytes = 128u * 128u * P::EB, b2_bytes = (uint32_t)R2 * 128u * P::EB;
-    uint8_t* GT[2];
-    uint8_t* B2[2];
-    GT[0] = smem;
-    GT[1] = smem + (NARR == 2 ? gt_bytes : 0);
-    B2[0] = smem + NARR * gt_bytes;
-    B2[1] = B2[0] + (NARR == 2 ? b2_bytes : 0);
-
+    const int warp = threadIdx.x >> 5;
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base_s, kTmemCols);
+        tc::tmem_alloc(&tmem_base_s, kCols);
         tc::tmem_relinquish();
     }
-    if (tid == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; ++i) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], kMathWarps + 2);   // math warps + both MMA warps
+        }
+        tc::mbar_init(&bars[0], kMathWarps);
+        tc::mbar_init(&bars[1], kMathWarps);
+        tc::mbar_init(&bars[2], 1);
+        tc::mbar_init(&bars[3], 1);
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tA = tmem_base_s, tY = tmem_base_s + 256u, tQ = tmem_base_s + 384u;
-    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
-    const uint32_t idesc1 = tc::instr_desc(128, 128, P::FMT);
-    const uint32_t idesc2 = tc::instr_desc(128, R2, P::FMT);
-    const uint32_t plane128 = 128u * 16u, planeR2 = (uint32_t)R2 * 16u;
-    const int half = warp >> 2;
-    const int m = 32 * (warp & 3) + lane;   // TMEM lane = row of A, Y, Q
 
-    uint32_t ph1 = 0, ph2 = 0;
-    bool pend1 = false, pend2 = false, failed = false;
-    // the pair whose stage-2 result is still in TMEM
-    int pl = -1;
-    float pc = 0.f, pnrm = 0.f;
-
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int it_idx = s_item;
-        __syncthreads();
-        if (it_idx >= total) break;
-        const FwdItem it = items[it_idx];
-        if (it.cost == 0) continue;
-        const JobDev& J = jobs[it.job];
-        const int nz = J.nz, nx = J.nx, ny = J.ny, nsx = J.nsx, nsy = J.nsy;
-        const int z = it.z;
-        const double cx = 0.5 * (double)(nsx - 1), cy = 0.5 * (double)(nsy - 1);
-
-        // Q of the previous pair -> dL/dW slot, dL/dIDD, dL/dsigma
-        auto drain = [&]() -> bool {
-            const bool ok = wait_bar(&bar[1], ph2);
-            if (ok) { ph2 ^= 1; pend2 = false; }
-            if (__syncthreads_or(!ok)) return false;
-            tc::fence_after_sync();
-            const float* wl = J.w + (size_t)pl * nsy * nsx;
-            float* slot = J.partial + ((size_t)pl * nz + z) * nsy * nsx;
-            const int j = m & 63;
-            const bool jrow = m < 64;
-            float dcv = 0.f, dsv = 0.f;
-            for (int c0 = 0; c0 < N1; c0 += 16) {
-                uint32_t r[16];
-                tc::tmem_ld16(tQ + lane_base + (uint32_t)(half * N1 + c0), r);
-                tc::tmem_wait_ld();
-                if (j < nsy && !(half == 1 && !jrow)) {
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) {
-                        const int i = c0 + q;
-                        if (i < nsx) {
-                            const float v = __uint_as_float(r[q]);
-                            const float wv = wl[(size_t)j * nsx + i];
-                            if (jrow && half == 0) {
-                                slot[(size_t)j * nsx + i] = pc * pnrm * v;
-                                dcv = fmaf(wv, v, dcv);
-                            } else {
-                                dsv = fmaf(wv, v, dsv);
-                            }
-                        }
-                    }
-                }
-            }
-            const float sdc = block_sum256(dcv, red[0]);
-            const float sds = block_sum256(dsv, red[1]);
-            if (tid == 0) {
-                J.dc[(size_t)pl * nz + z] = pnrm * sdc;
-                J.dsg[(size_t)pl * nz + z] = pc * pnrm * sds;
-            }
-            tc::fence_before_sync();
-            __syncthreads();
-            return true;
-        };
-
-        // ---- G^T of the slice: rows x, K = y (zero outside the grid) ----
-        {
-            const float* g = J.grad_dose + (size_t)z * ny * nx;
-            for (int e = tid; e < 128 * (128 / EPC); e += TNT) {
-                const int x = e & 127, gi = e >> 7;
-                float v[EPC];
-#pragma unroll
-                for (int q = 0; q < EPC; ++q) {
-                    const int y = gi * EPC + q;
-                    v[q] = (y < ny && x < nx) ? g[(size_t)y * nx + x] : 0.f;
-                }
-                uint4 hi, lo;
-                split_chunk<MODE>(v, hi, lo);
-                const uint32_t off = (uint32_t)gi * plane128 + (uint32_t)x * 16u;
-                *reinterpret_cast<uint4*>(GT[0] + off) = hi;
-                if (NARR == 2) *reinterpret_cast<uint4*>(GT[1] + off) = lo;
-            }
+    if (warp >= kMathWarps) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
+        if (warp == kSchedWarp) {
+            scheduler_warp(P, ring, full, empty);
+        } else if (warp == kS1Warp || warp == kS2Warp) {
+            const Layout L = make_layout<NARR>(P.N1);
+            mma_warp<MODE>(P, L, tc::smem_u32(smem), tmem_base_s, warp == kS1Warp ? 1 : 2, ring,
+                           full, empty, bars);
         }
-
-        for (int l = it.lb; l < it.le && !failed; ++l) {
-            const double c = J.idd[(size_t)l * nz + z];
-            if (c == 0.0) continue;
-            const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
-            // d is formed in FP64 (voxel and spot coordinates of up to ~25 cm); d^2 and the
-            // exponent in FP32 (relative rounding ~1e-7 of the exponent)
-            const float a2 = (float)(kLog2e / (2.0 * s * s));
-            const float inv_s3 = (float)(1.0 / (s * s * s)), inv_s = (float)(1.0 / s);
-
-            if (pend2) {
-                if (!drain()) { failed = true; break; }
-            }
-            // ---- A = [Gy | Gy']^T into TMEM: lane m, columns y ----
-            {
-                const int j = m & 63;
-                const bool deriv = m >= 64;
-                constexpr int VPS = P::EB == 4 ? 16 : 32;   // values per 16-column store
-                const double ysj = J.sy0 + ((double)j - cy) * J.dsy;
-                const float dyf = (float)J.dy;
-                for (int y0 = half * 64; y0 < half * 64 + 64; y0 += VPS) {
-                    // one FP64 difference per chunk, then FP32 steps of dy
-                    const float base = (float)((J.oy + (double)y0 * J.dy) - ysj);
-                    float v[VPS];
-#pragma unroll
-                    for (int q = 0; q < VPS; ++q) {
-                        float val = 0.f;
-                        if (j < nsy) {
-                            const float df = fmaf((float)q, dyf, base), dd = df * df;
-                            const float e = ex2_approx(-dd * a2);
-                            val = deriv ? e * fmaf(dd, inv_s3, -inv_s) : e;
-                        }
-                        v[q] = val;
-                    }
-                    uint32_t hi[16], lo[16];
-                    pack16<MODE>(v, hi, lo);
-                    const uint32_t col = (uint32_t)(P::EB == 4 ? y0 : y0 / 2);
-                    tc::tmem_st16(tA + lane_base + col, hi);
-                    if (NARR == 2) tc::tmem_st16(tA + lane_base + O::kLoOff + col, lo);
-                }
-                tc::tmem_wait_st();
-            }
-            tc::fence_async_smem();   // G^T (first pair of the item) visible to the MMA
-            tc::fence_before_sync();
-            __syncthreads();
-            if (tid == 0) {
-                tc::fence_after_sync();
-                O::issue(tY, tA, GT, plane128, idesc1);
-                tc::commit(&bar[0]);
-            }
-            pend1 = true;
-
-            // ---- B = [Gx | Gx'] in smem: rows n, K = x ----
-            for (int e = tid; e < R2 * (128 / EPC); e += TNT) {
-                const int n = e % R2, gi = e / R2;
-                const int i = n < N1 ? n : n - N1;
-                const bool deriv = n >= N1;
-                const float base = (float)((J.ox + (double)(gi * EPC) * J.dx) -
-                                           (J.sx0 + ((double)i - cx) * J.dsx));
-                const float dxf = (float)J.dx;
-                float v[EPC];
-#pragma unroll
-                for (int q = 0; q < EPC; ++q) {
-                    float val = 0.f;
-                    if (i < nsx) {
-                        const float df = fmaf((float)q, dxf, base), dd = df * df;
-                        const float g = ex2_approx(-dd * a2);
-                        val = deriv ? g * fmaf(dd, inv_s3, -inv_s) : g;
-                    }
-                    v[q] = val;
-                }
-                uint4 hi, lo;
-                split_chunk<MODE>(v, hi, lo);
-                const uint32_t off = (uint32_t)gi * planeR2 + (uint32_t)n * 16u;
-                *reinterpret_cast<uint4*>(B2[0] + off) = hi;
-                if (NARR == 2) *reinterpret_cast<uint4*>(B2[1] + off) = lo;
-            }
-
-            // ---- Y (stage 1 result) -> split -> A region of TMEM ----
-            {
-                const bool ok = wait_bar(&bar[0], ph1);
-                if (ok) { ph1 ^= 1; pend1 = false; }
-                if (__syncthreads_or(!ok)) { failed = true; break; }
-            }
-            tc::fence_after_sync();
-            {
-                constexpr int VPS = P::EB == 4 ? 16 : 32;
-                for (int x0 = half * 64; x0 < half * 64 + 64; x0 += VPS) {
-                    float v[VPS];
-                    {
-                        uint32_t r[16];
-                        tc::tmem_ld16(tY + lane_base + (uint32_t)x0, r);
-                        tc::tmem_wait_ld();
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
-                    }
-                    if (VPS == 32) {
-                        uint32_t r[16];
-                        tc::tmem_ld16(tY + lane_base + (uint32_t)(x0 + 16), r);
-                        tc::tmem_wait_ld();
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) v[16 + (q & 15)] = __uint_as_float(r[q]);
-                    }
-                    uint32_t hi[16], lo[16];
-                    pack16<MODE>(v, hi, lo);
-                    const uint32_t col = (uint32_t)(P::EB == 4 ? x0 : x0 / 2);
-                    tc::tmem_st16(tA + lane_base + col, hi);
-                    if (NARR == 2) tc::tmem_st16(tA + lane_base + O::kLoOff + col, lo);
-                }
-                tc::tmem_wait_st();
-            }
-            tc::fence_async_smem();
-            tc::fence_before_sync();
-            __syncthreads();
-            if (tid == 0) {
-                tc::fence_after_sync();
-                O::issue(tQ, tA, B2, planeR2, idesc2);
-                tc::commit(&bar[1]);
-            }
-            pend2 = true;
-            pl = l;
-            pc = (float)c;
-            pnrm = (float)(kInv2Pi / (s * s));
-        }
-        if (failed) break;
-        if (pend2) {
-            if (!drain()) { failed = true; break; }
-        }
+    } else {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kMathRegs));
+        const Layout L = make_layout<NARR>(P.N1);
+        math_warps<MODE>(P, L, smem, tmem_base_s, ring, full, empty, bars);
     }
 
-    if (failed) {
-        if (tid == 0) atomicExch(err, 1);
-        if (pend1) (void)wait_bar(&bar[0], ph1);
-        if (pend2) (void)wait_bar(&bar[1], ph2);
-    }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (warp == 0) tc::tmem_dealloc(tmem_base_s, kTmemCols);
+    if (warp == 0) tc::tmem_dealloc(tmem_base_s, kCols);
 }
 
-// dL/dW_l = sum over active slices of the (l, z) slots in a fixed order (deterministic);
+// <slot, W_l> for every active (layer, slice): dL/dIDD = <P slot, W>, dL/dsigma =
+// IDD <A slot + B slot, W>.  One block per (slice, layer, job); inactive pairs leave.
+__global__ void adj_tc_dots_kernel(const JobDev* __restrict__ jobs) {
+    const JobDev& J = jobs[blockIdx.z];
+    const int z = blockIdx.x, l = blockIdx.y;
+    if (z >= J.nz || l >= J.nl) return;
+    const double c = J.idd[(size_t)l * J.nz + z];
+    if (c == 0.0) return;
+    const int nsx = J.nsx, nsy = J.nsy;
+    const size_t per = (size_t)nsy * nsx, plane = (size_t)J.nl * J.nz * per;
+    const float* sp = J.partial + ((size_t)l * J.nz + z) * per;
+    const float* wl = J.w + (size_t)l * per;
+    float dc = 0.f, ds = 0.f;
+    for (int e = threadIdx.x; e < (int)per; e += blockDim.x) {
+        const int i = e / nsy, j = e % nsy;   // slots are [i][j]
+        const float w = wl[(size_t)j * nsx + i];
+        dc = fmaf(sp[e], w, dc);
+        ds = fmaf(sp[plane + e] + sp[2 * plane + e], w, ds);
+    }
+    __shared__ float red[2][8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dc += __shfl_xor_sync(0xffffffffu, dc, o);
+        ds += __shfl_xor_sync(0xffffffffu, ds, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = dc; red[1][w] = ds; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float a = 0.f, s = 0.f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += red[0][k]; s += red[1][k]; }
+        J.dc[(size_t)l * J.nz + z] = a;
+        J.dsg[(size_t)l * J.nz + z] = (float)c * s;
+    }
+}
+
+// dL/dW_l = sum over active slices of IDD * P slot, in slice order (deterministic);
 // dL/dR_l in FP64; the loss total.  Grid (spot blocks of 128, layers, jobs): each block
 // first compacts the layer's active slices into shared memory, then every thread sums its
-// (j, i) entry over them with four independent accumulators (the loads of one slice are
-// coalesced).
+// (j, i) entry over them with four independent accumulators.
 __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with_range,
                                        int finalize_loss, const int* __restrict__ err) {
     const JobDev& J = jobs[blockIdx.z];
     const int l = blockIdx.y;
     if (l >= J.nl) return;
-    const int per = J.nsy * J.nsx;
+    const int nsx = J.nsx, nsy = J.nsy;
+    const int per = nsy * nsx;
     const bool bad = *err != 0 || (J.fwd_err != nullptr && *J.fwd_err != 0);
     const double* idd = J.idd + (size_t)l * J.nz;
     __shared__ int zl[1024];
+    __shared__ float cz[1024];
     __shared__ int wcount[4];
     __shared__ int nact;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;   // (j, i) entry of grad_w
+    const int jj = r / max(nsx, 1), ii = r % max(nsx, 1);
+    const int sr = ii * nsy + jj;                          // same entry in a [i][j] slot
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
     for (int zc = 0; zc < J.nz; zc += 1024) {
@@ -396,27 +610,32 @@ __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with
         // order-preserving compaction of the active slices, 128 at a time (4 warp ballots)
         for (int zb = zc; zb < min(J.nz, zc + 1024); zb += 128) {
             const int z = zb + threadIdx.x;
-            const bool act = z < J.nz && z < zc + 1024 && idd[z] != 0.0;
+            const double iv = (z < J.nz && z < zc + 1024) ? idd[z] : 0.0;
+            const bool act = iv != 0.0;
             const unsigned bal = __ballot_sync(0xffffffffu, act);
             if (lane == 0) wcount[warp] = __popc(bal);
             __syncthreads();
             int off = nact;
             for (int w = 0; w < warp; ++w) off += wcount[w];
-            if (act) zl[off + __popc(bal & ((1u << lane) - 1u))] = z;
+            if (act) {
+                const int p = off + __popc(bal & ((1u << lane) - 1u));
+                zl[p] = z;
+                cz[p] = (float)iv;
+            }
             __syncthreads();
             if (threadIdx.x == 0) nact += wcount[0] + wcount[1] + wcount[2] + wcount[3];
             __syncthreads();
         }
         if (r < per) {
-            const float* base = J.partial + (size_t)l * J.nz * per + r;
+            const float* base = J.partial + (size_t)l * J.nz * per + sr;
             int k = 0;
             for (; k + 4 <= nact; k += 4) {
-                a0 += base[(size_t)zl[k] * per];
-                a1 += base[(size_t)zl[k + 1] * per];
-                a2 += base[(size_t)zl[k + 2] * per];
-                a3 += base[(size_t)zl[k + 3] * per];
+                a0 = fmaf(cz[k], base[(size_t)zl[k] * per], a0);
+                a1 = fmaf(cz[k + 1], base[(size_t)zl[k + 1] * per], a1);
+                a2 = fmaf(cz[k + 2], base[(size_t)zl[k + 2] * per], a2);
+                a3 = fmaf(cz[k + 3], base[(size_t)zl[k + 3] * per], a3);
             }
-            for (; k < nact; ++k) a0 += base[(size_t)zl[k] * per];
+            for (; k < nact; ++k) a0 = fmaf(cz[k], base[(size_t)zl[k] * per], a0);
         }
     }
     if (r < per)
@@ -446,14 +665,13 @@ __global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with
 
 template <int MODE>
 size_t adj_smem_bytes(int N1) {
-    using P = Prec<MODE>;
-    const int narr = P::NPROD == 3 ? 2 : 1;
-    return (size_t)narr * P::EB * (128u * 128u + 2u * (size_t)N1 * 128u);
+    using Pr = Prec<MODE>;
+    const size_t narr = Pr::NPROD == 3 ? 2 : 1;
+    return narr * 2u * (128u * 128u + 2u * (size_t)N1 * 128u);
 }
 
 template <int MODE>
-int launch_mode(JobDev* jobs, FwdItem* items, int total, int* counter, int* err, int N1,
-                cudaStream_t s) {
+int launch_mode(const Params& P0, cudaStream_t s) {
     static thread_local int max_dyn = 0;
     if (max_dyn == 0) {
         int dev = 0, optin = 0;
@@ -463,6 +681,8 @@ int launch_mode(JobDev* jobs, FwdItem* items, int total, int* counter, int* err,
                 cudaSuccess ||
             cudaFuncGetAttributes(&fa, adj_tc_kernel<MODE>) != cudaSuccess)
             return PBD_ERR_CUDA;
+        // the setmaxnreg split needs the full launch allotment, or its increase never returns
+        if (fa.numRegs < kLaunchRegsNeeded) return PBD_ERR_UNSUPPORTED;
         const int avail = optin - (int)fa.sharedSizeBytes;
         if (avail <= 0 || cudaFuncSetAttribute(adj_tc_kernel<MODE>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -470,12 +690,14 @@ int launch_mode(JobDev* jobs, FwdItem* items, int total, int* counter, int* err,
             return PBD_ERR_NO_SMEM;
         max_dyn = avail;
     }
+    const Params P = P0;
+    size_t smem = adj_smem_bytes<MODE>(P.N1);
     // >= 116 KiB: one CTA, and its 512 TMEM columns, per SM
-    const size_t smem = std::max<size_t>(adj_smem_bytes<MODE>(N1), 116u * 1024u);
+    smem = std::max<size_t>(smem, 116u * 1024u);
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
-    const int grid = std::max(1, std::min(total, num_sms()));
+    const int grid = std::max(1, std::min(P.n_units, num_sms()));
     prof_mark(kProfAdj, 0, s);
-    adj_tc_kernel<MODE><<<grid, TNT, smem, s>>>(jobs, items, total, counter, err, N1);
+    adj_tc_kernel<MODE><<<grid, kThreads, smem, s>>>(P);
     PBD_LAUNCH_CHECK();
     prof_mark(kProfAdj, 1, s);
     return PBD_OK;
@@ -485,53 +707,46 @@ int launch_mode(JobDev* jobs, FwdItem* items, int total, int* counter, int* err,
 
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1) {
     if (precision == PBD_PREC_FP32) return PBD_ERR_UNSUPPORTED;
-    if (f->nx > kTile || f->ny > kTile || f->n_sy > 64) return PBD_ERR_UNSUPPORTED;
+    if (f->nx > kTile || f->ny > kTile || f->n_sy > 64 || f->n_sx > 64) return PBD_ERR_UNSUPPORTED;
     *N1 = (f->n_sx + 15) / 16 * 16;
-    const bool wide = precision == PBD_PREC_TF32X3 || precision == PBD_PREC_TF32;
-    const int narr = (precision == PBD_PREC_TF32X3 || precision == PBD_PREC_BF16X3) ? 2 : 1;
-    const size_t eb = wide ? 4 : 2;
-    const size_t smem = (size_t)narr * eb * (128u * 128u + 2u * (size_t)(*N1) * 128u);
-    if (*N1 > 64 || smem > 227u * 1024u - 2048u) return PBD_ERR_UNSUPPORTED;
     return PBD_OK;
 }
 
+size_t tc_adjoint_slot_elems(const pbd_field* f) {
+    return 3u * (size_t)f->n_layers * f->nz * f->n_sy * f->n_sx;
+}
+
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      FwdItem* items, int total_items, int* counter, int chunk, int with_range,
-                      int finalize_loss, cudaStream_t s) {
-    int N1 = 0;
+                      int* counter, int chunk, int with_range, int finalize_loss, cudaStream_t s) {
+    Params P{};
+    P.jobs = jobs_dev;
+    P.n_jobs = n_jobs;
+    P.chunk = chunk;
+    P.counter = counter;
+    int cm = 1, nzm = 1, max_l = 1, max_per = 1;
     for (int j = 0; j < n_jobs; ++j) {
         pbd_field f{};
         f.nx = jobs_host[j].nx; f.ny = jobs_host[j].ny;
         f.n_sx = jobs_host[j].nsx; f.n_sy = jobs_host[j].nsy;
         int n1 = 0;
         PBD_TRY(tc_adjoint_dims(precision, &f, &n1));
-        N1 = std::max(N1, n1);
-    }
-    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
-    PBD_TRY(launch_slice_schedule(jobs_dev, items, chunk, n_jobs, s));
-    int rc = PBD_ERR_BAD_VALUE;
-    switch (precision) {
-        case PBD_PREC_TF32X3:
-            rc = launch_mode<PBD_PREC_TF32X3>(jobs_dev, items, total_items, counter, counter + 1, N1, s);
-            break;
-        case PBD_PREC_TF32:
-            rc = launch_mode<PBD_PREC_TF32>(jobs_dev, items, total_items, counter, counter + 1, N1, s);
-            break;
-        case PBD_PREC_BF16X3:
-            rc = launch_mode<PBD_PREC_BF16X3>(jobs_dev, items, total_items, counter, counter + 1, N1, s);
-            break;
-        case PBD_PREC_BF16:
-            rc = launch_mode<PBD_PREC_BF16>(jobs_dev, items, total_items, counter, counter + 1, N1, s);
-            break;
-        default:
-            break;
-    }
-    PBD_TRY(rc);
-    int max_l = 1, max_per = 1;
-    for (int j = 0; j < n_jobs; ++j) {
+        P.N1 = std::max(P.N1, n1);
+        cm = std::max(cm, (jobs_host[j].nl + chunk - 1) / chunk);
+        nzm = std::max(nzm, jobs_host[j].nz);
         max_l = std::max(max_l, jobs_host[j].nl);
         max_per = std::max(max_per, jobs_host[j].nsy * jobs_host[j].nsx);
     }
+    P.cmax = cm;
+    const long long units = (long long)nzm * cm * n_jobs;
+    if (units > (1LL << 30)) return PBD_ERR_UNSUPPORTED;
+    P.n_units = (int)units;
+    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
+    int rc = PBD_OK;
+    if (precision == PBD_PREC_BF16) rc = launch_mode<PBD_PREC_BF16>(P, s);
+    else rc = launch_mode<PBD_PREC_BF16X3>(P, s);
+    PBD_TRY(rc);
+    adj_tc_dots_kernel<<<dim3(nzm, max_l, n_jobs), 256, 0, s>>>(jobs_dev);
+    PBD_LAUNCH_CHECK();
     adj_tc_finalize_kernel<<<dim3((max_per + 127) / 128, max_l, n_jobs), 128, 0, s>>>(
         jobs_dev, with_range, finalize_loss, counter + 1);
     PBD_LAUNCH_CHECK();

@@ -154,13 +154,10 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
         size_t pe = 0;
         int n1 = 0;
         if (tc_adjoint_dims(precision, f, &n1) == PBD_OK) {
-            // tensor-core adjoint: (slice, layer-chunk) items, one dL/dW slot per (layer, slice)
+            // tensor-core adjoint: (slice, layer-chunk) units, three slots per (layer, slice)
             w.adj_tc = 1;
             w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : 8;
-            w.a_items = f->nz * ((f->n_layers + w.a_chunk - 1) / w.a_chunk);
-            pe = (size_t)f->n_layers * f->nz * f->n_sy * f->n_sx;
-            w.aitems = c.take<FwdItem>(w.a_items);
-            w.anch = c.take<int>(f->nz);
+            pe = tc_adjoint_slot_elems(f);
         } else {
             PBD_TRY(adj_plan_sizes(f, w.a_chunk, &pe, &w.a_items));
             w.aitems = c.take<AdjItem>(w.a_items);
@@ -360,9 +357,8 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
 static int run_adjoint(const Ws& ws, int precision, const JobDev* A, int with_range,
                        int finalize_loss, cudaStream_t s) {
     if (ws.adj_tc)
-        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, static_cast<FwdItem*>(ws.aitems),
-                                 ws.a_items, ws.counters + 2, ws.a_chunk, with_range,
-                                 finalize_loss, s);
+        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, ws.counters + 2, ws.a_chunk,
+                                 with_range, finalize_loss, s);
     return launch_adjoint(ws.jobs + 1, A, 1, static_cast<AdjItem*>(ws.aitems), ws.a_items,
                           ws.counters + 2, ws.a_chunk, with_range, finalize_loss, s);
 }

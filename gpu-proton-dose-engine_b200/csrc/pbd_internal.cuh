@@ -122,11 +122,13 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
 // (slice, tile, layer-chunk) work items sorted longest-first, one CTA per job.
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
 
-// adjoint (tcgen05) -- adj_tc.cu; items are (slice, layer chunk) records as for the forward
+// adjoint (tcgen05) -- adj_tc.cu.  Units (slice, chunk of `chunk` active layers) are
+// pulled z-major; `partial` holds three (layer, slice) slot planes of nsy * nsx floats
+// (tc_adjoint_slot_elems); counter[0] = unit counter, counter[1] = error word.
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
+size_t tc_adjoint_slot_elems(const pbd_field* f);
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      FwdItem* items, int total_items, int* counter, int chunk, int with_range,
-                      int finalize_loss, cudaStream_t s);
+                      int* counter, int chunk, int with_range, int finalize_loss, cudaStream_t s);
 
 // forward (tcgen05) -- tc_fwd.cu.  Work units (slice, layer chunk, tile) are enumerated
 // z-major; counter[0] = unit counter, counter[1] = error word; every job's `arrive` array

@@ -164,9 +164,9 @@ def test_tc_adjoint_clinical(pb, prec):
     assert ew < 1e-4 and er_ < 1e-4
 
 
-def test_tc_adjoint_wide_lattice_uses_fp32_adjoint(pb):
-    """51 spots in x exceed the TF32 tensor-core adjoint's shared memory: the FP32 adjoint
-    serves that field, with the tensor-core forward."""
+def test_tc_adjoint_wide_lattice(pb):
+    """51 spots in x (padded to 64): the tensor-core adjoint covers lattices up to 64 x 64
+    spots; its dL/dW agrees with the FP32 adjoint within the gradient tolerance."""
     import torch
     M = pb.model
     rng = np.random.default_rng(9)
@@ -181,4 +181,4 @@ def test_tc_adjoint_wide_lattice_uses_fp32_adjoint(pb):
                     generator=torch.Generator(device="cuda").manual_seed(3))
     gw, _ = plan.adjoint(g)
     ref = pb.engines.DosePlan(prob, tables="device", precision="fp32").adjoint(g)[0]
-    assert rel(gw.cpu().numpy(), ref.cpu().numpy()) < 1e-6
+    assert rel(gw.cpu().numpy(), ref.cpu().numpy()) < 1e-4
