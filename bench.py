@@ -415,54 +415,63 @@ def main():
         plan.loss_grad(m, p, outputs=out)
     torch.cuda.synchronize(dev)
 
-    # ---- device-resident timed region ----
     K = args.steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(K)]
-    barrier()
-    torch.cuda.synchronize(dev)
+
+    def timed(fn):
+        """Total ms of K calls of fn, CUDA events around each call, L2 flushed (256 MiB
+        write) before each one outside the events; max over ranks."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(K)]
+        barrier()
+        torch.cuda.synchronize(dev)
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record()
+            fn()
+            ev[k][1].record()
+        torch.cuda.synchronize(dev)
+        barrier()
+        t = sum(a.elapsed_time(b) for a, b in ev)
+        if world > 1:
+            tt = torch.tensor([t], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    # ---- device-resident, eager calls (per-kernel event profile, launch count) ----
     n0 = lib.launch_count()
     lib.profile_begin()
-    for k in range(K):
-        flush.zero_()
-        ev[k][0].record()
-        plan.loss_grad(m, p, outputs=out)
-        ev[k][1].record()
-    torch.cuda.synchronize(dev)
+    t_eager = timed(lambda: plan.loss_grad(m, p, outputs=out))
     prof = lib.profile_end()
-    launches = lib.launch_count() - n0
-    barrier()
-    t_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if world > 1:
-        t = torch.tensor([t_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-    value = world * K / (t_ms * 1e-3)
+    launches_per_eval = (lib.launch_count() - n0) / K
 
-    # ---- end to end through the public API, host buffers ----
+    # ---- device-resident, the same call replayed from a CUDA graph (headline) ----
+    g_dev = pb.engines.LossGradGraph(plan, m, p)
+    for _ in range(max(args.warmup, 3)):
+        g_dev.replay()
+    t_ms = timed(g_dev.replay)
+    value = world * K / (t_ms * 1e-3)
+    launches = int(round(launches_per_eval * K))
+
+    # ---- end to end through the public API, host buffers (pinned) ----
     w_host = torch.tensor(wl["weights"], dtype=torch.float32).pin_memory()
     gw_host = torch.empty_like(w_host).pin_memory()
     gr_host = torch.empty(wl["n_layers"], dtype=torch.float32).pin_memory()
     loss_host = torch.empty((), dtype=torch.float64).pin_memory()
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(K)]
-    barrier()
-    torch.cuda.synchronize(dev)
-    for k in range(K):
-        flush.zero_()
-        ev2[k][0].record()
+
+    def eager_e2e():
         o = plan.loss_grad(m, p, w=w_host, outputs=out)
         gw_host.copy_(o["grad_w"], non_blocking=True)
         gr_host.copy_(o["grad_range"], non_blocking=True)
         loss_host.copy_(o["loss"], non_blocking=True)
-        ev2[k][1].record()
-    torch.cuda.synchronize(dev)
-    barrier()
-    t2 = sum(a.elapsed_time(b) for a, b in ev2)
-    if world > 1:
-        t = torch.tensor([t2], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t2 = float(t.item())
+
+    t2_eager = timed(eager_e2e)
+    g_e2e = pb.engines.LossGradGraph(plan, m, p, host_w=w_host,
+                                     host_out={"grad_w": gw_host, "grad_range": gr_host,
+                                               "loss": loss_host})
+    for _ in range(max(args.warmup, 3)):
+        g_e2e.replay()
+    t2 = timed(g_e2e.replay)
     clk = clocks.stop()
     e2e = world * K / (t2 * 1e-3)
     h2d = w_host.numel() * 4
@@ -498,7 +507,11 @@ def main():
                        "l2": "flushed between steps (256 MiB write, outside the events)",
                        "parallelism": f"{world} independent evaluations (one per rank)"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "how": "DosePlan loss gradient replayed from a "
+                    "CUDA graph that uploads the weights and downloads dL/dW, dL/dR and L"},
+            "eager": {"value": world * K / (t_eager * 1e-3),
+                      "e2e": world * K / (t2_eager * 1e-3),
+                      "how": "one DosePlan.loss_grad call per step (host work per call)"},
             "gpu_launches": launches, "roofline": roof, "clocks": clk}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

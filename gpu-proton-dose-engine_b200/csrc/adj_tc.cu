@@ -38,8 +38,8 @@
 //  Stage 2 of pair n-1 runs under G of pair n; stage 1 of pair n under DR and B.
 //
 // dL/dW_l = sum over active slices of IDD * slot P in slice order, and the dot products
-// <slot, W> for dL/dIDD and dL/dsigma, are formed by two small follow-up kernels in a fixed
-// order (deterministic).  Every wait is bounded (2 s of %globaltimer); a warp whose wait
+// <slot, W> for dL/dIDD and dL/dsigma, are formed by one follow-up kernel in a fixed order
+// (deterministic).  Every wait is bounded (2 s of %globaltimer); a warp whose wait
 // runs out sets the error word and leaves, the others' waits then run out in turn, and
 // the finalize pass turns the gradients into NaN.
 // Grids of at most 128 x 128 voxels per slice; lattices up to 64 x 64 spots.
@@ -545,121 +545,130 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     if (warp == 0) tc::tmem_dealloc(tmem_base_s, kCols);
 }
 
-// <slot, W_l> for every active (layer, slice): dL/dIDD = <P slot, W>, dL/dsigma =
-// IDD <A slot + B slot, W>.  One block per (slice, layer, job); inactive pairs leave.
-__global__ void adj_tc_dots_kernel(const JobDev* __restrict__ jobs) {
-    const JobDev& J = jobs[blockIdx.z];
-    const int z = blockIdx.x, l = blockIdx.y;
-    if (z >= J.nz || l >= J.nl) return;
-    const double c = J.idd[(size_t)l * J.nz + z];
-    if (c == 0.0) return;
-    const int nsx = J.nsx, nsy = J.nsy;
-    const size_t per = (size_t)nsy * nsx, plane = (size_t)J.nl * J.nz * per;
-    const float* sp = J.partial + ((size_t)l * J.nz + z) * per;
-    const float* wl = J.w + (size_t)l * per;
-    float dc = 0.f, ds = 0.f;
-    for (int e = threadIdx.x; e < (int)per; e += blockDim.x) {
-        const int i = e / nsy, j = e % nsy;   // slots are [i][j]
-        const float w = wl[(size_t)j * nsx + i];
-        dc = fmaf(sp[e], w, dc);
-        ds = fmaf(sp[plane + e] + sp[2 * plane + e], w, ds);
-    }
-    __shared__ float red[2][8];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        dc += __shfl_xor_sync(0xffffffffu, dc, o);
-        ds += __shfl_xor_sync(0xffffffffu, ds, o);
-    }
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) { red[0][w] = dc; red[1][w] = ds; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float a = 0.f, s = 0.f;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += red[0][k]; s += red[1][k]; }
-        J.dc[(size_t)l * J.nz + z] = a;
-        J.dsg[(size_t)l * J.nz + z] = (float)c * s;
-    }
-}
+// After the main kernel: dL/dW, the per-pair dot products and dL/dR in one pass over the
+// slots.  Block (segment of kRedZ slices, layer l, job): its threads hold W_l (transposed to
+// the slots' [i][j] order) in registers and walk the segment's active slices in order,
+// accumulating IDD * P slot into a partial dL/dW and forming <P slot, W> (dL/dIDD) and
+// IDD <A + B slot, W> (dL/dsigma) per slice (warp shuffles, then the warps in order).  The
+// block that completes a layer's last segment (per-layer arrival counter) sums the segment
+// partials in segment order into dL/dW and forms dL/dR_l in FP64; the one completing layer
+// 0 also sums the loss partials.  Every sum is in a fixed order: deterministic.
+constexpr int kRedZ = 8;           // slices per block
+constexpr int kRedThreads = 256;
+constexpr int kRedPer = 16;        // entries per thread: nsy * nsx <= 64 * 64 = 16 * 256
 
-// dL/dW_l = sum over active slices of IDD * P slot, in slice order (deterministic);
-// dL/dR_l in FP64; the loss total.  Grid (spot blocks of 128, layers, jobs): each block
-// first compacts the layer's active slices into shared memory, then every thread sums its
-// (j, i) entry over them with four independent accumulators.
-__global__ void adj_tc_finalize_kernel(const JobDev* __restrict__ jobs, int with_range,
-                                       int finalize_loss, const int* __restrict__ err) {
+__global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
+    const JobDev* __restrict__ jobs, int with_range, int finalize_loss, const int* __restrict__ err,
+    int* layer_count) {
     const JobDev& J = jobs[blockIdx.z];
-    const int l = blockIdx.y;
+    const int seg = blockIdx.x, l = blockIdx.y;
     if (l >= J.nl) return;
-    const int nsx = J.nsx, nsy = J.nsy;
-    const int per = nsy * nsx;
+    const int nz = J.nz, nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;
+    const int nseg = (nz + kRedZ - 1) / kRedZ;
+    if (seg >= nseg) return;
+    const size_t plane = (size_t)J.nl * nz * per;
+    float* part = J.partial + 3 * plane;           // (nl, nseg, per) segment partials
+    const double* idd = J.idd + (size_t)l * nz;
+    const float* wl = J.w + (size_t)l * per;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    __shared__ float sdc[kRedZ][kRedThreads / 32], sds[kRedZ][kRedThreads / 32];
+    __shared__ int s_last;
+
+    float wv[kRedPer], acc[kRedPer];
+#pragma unroll
+    for (int k = 0; k < kRedPer; ++k) {
+        const int e = tid + k * kRedThreads;   // slot entry e = i * nsy + j
+        wv[k] = e < per ? wl[(size_t)(e % nsy) * nsx + e / nsy] : 0.f;
+        acc[k] = 0.f;
+    }
+    const int z0 = seg * kRedZ, z1 = min(nz, z0 + kRedZ);
+    for (int z = z0; z < z1; ++z) {
+        const double c = idd[z];
+        if (c == 0.0) continue;
+        const float cf = (float)c;
+        const float* pz = J.partial + ((size_t)l * nz + z) * per;
+        float pd = 0.f, ps = 0.f;
+#pragma unroll
+        for (int k = 0; k < kRedPer; ++k) {
+            const int e = tid + k * kRedThreads;
+            if (e < per) {
+                const float p = pz[e];
+                const float q = pz[plane + e] + pz[2 * plane + e];
+                acc[k] = fmaf(cf, p, acc[k]);
+                pd = fmaf(p, wv[k], pd);
+                ps = fmaf(q, wv[k], ps);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            pd += __shfl_xor_sync(0xffffffffu, pd, o);
+            ps += __shfl_xor_sync(0xffffffffu, ps, o);
+        }
+        if (lane == 0) { sdc[z - z0][warp] = pd; sds[z - z0][warp] = ps; }
+    }
+    __syncthreads();
+    if (tid < z1 - z0) {
+        const int z = z0 + tid;
+        const double c = idd[z];
+        if (c != 0.0) {
+            float a = 0.f, b = 0.f;
+            for (int w = 0; w < kRedThreads / 32; ++w) { a += sdc[tid][w]; b += sds[tid][w]; }
+            J.dc[(size_t)l * nz + z] = a;
+            J.dsg[(size_t)l * nz + z] = (float)c * b;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kRedPer; ++k) {
+        const int e = tid + k * kRedThreads;
+        if (e < per) part[((size_t)l * nseg + seg) * per + e] = acc[k];
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(&layer_count[l], 1) == nseg - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
     const bool bad = *err != 0 || (J.fwd_err != nullptr && *J.fwd_err != 0);
-    const double* idd = J.idd + (size_t)l * J.nz;
-    __shared__ int zl[1024];
-    __shared__ float cz[1024];
-    __shared__ int wcount[4];
-    __shared__ int nact;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;   // (j, i) entry of grad_w
-    const int jj = r / max(nsx, 1), ii = r % max(nsx, 1);
-    const int sr = ii * nsy + jj;                          // same entry in a [i][j] slot
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    for (int zc = 0; zc < J.nz; zc += 1024) {
-        __syncthreads();
-        if (threadIdx.x == 0) nact = 0;
-        __syncthreads();
-        // order-preserving compaction of the active slices, 128 at a time (4 warp ballots)
-        for (int zb = zc; zb < min(J.nz, zc + 1024); zb += 128) {
-            const int z = zb + threadIdx.x;
-            const double iv = (z < J.nz && z < zc + 1024) ? idd[z] : 0.0;
-            const bool act = iv != 0.0;
-            const unsigned bal = __ballot_sync(0xffffffffu, act);
-            if (lane == 0) wcount[warp] = __popc(bal);
-            __syncthreads();
-            int off = nact;
-            for (int w = 0; w < warp; ++w) off += wcount[w];
-            if (act) {
-                const int p = off + __popc(bal & ((1u << lane) - 1u));
-                zl[p] = z;
-                cz[p] = (float)iv;
+    const float nan = __int_as_float(0x7fc00000);
+#pragma unroll
+    for (int k = 0; k < kRedPer; ++k) {
+        const int e = tid + k * kRedThreads;
+        if (e < per) {
+            // four interleaved partial sums (segments s, s+4, ...) combined in a fixed order
+            const float* pe = part + (size_t)l * nseg * per + e;
+            float g0 = 0.f, g1 = 0.f, g2 = 0.f, g3 = 0.f;
+            int sgi = 0;
+            for (; sgi + 4 <= nseg; sgi += 4) {
+                g0 += __ldcg(pe + (size_t)sgi * per);
+                g1 += __ldcg(pe + (size_t)(sgi + 1) * per);
+                g2 += __ldcg(pe + (size_t)(sgi + 2) * per);
+                g3 += __ldcg(pe + (size_t)(sgi + 3) * per);
             }
-            __syncthreads();
-            if (threadIdx.x == 0) nact += wcount[0] + wcount[1] + wcount[2] + wcount[3];
-            __syncthreads();
-        }
-        if (r < per) {
-            const float* base = J.partial + (size_t)l * J.nz * per + sr;
-            int k = 0;
-            for (; k + 4 <= nact; k += 4) {
-                a0 = fmaf(cz[k], base[(size_t)zl[k] * per], a0);
-                a1 = fmaf(cz[k + 1], base[(size_t)zl[k + 1] * per], a1);
-                a2 = fmaf(cz[k + 2], base[(size_t)zl[k + 2] * per], a2);
-                a3 = fmaf(cz[k + 3], base[(size_t)zl[k + 3] * per], a3);
-            }
-            for (; k < nact; ++k) a0 = fmaf(cz[k], base[(size_t)zl[k] * per], a0);
+            for (; sgi < nseg; ++sgi) g0 += __ldcg(pe + (size_t)sgi * per);
+            J.grad_w[(size_t)l * per + (size_t)(e % nsy) * nsx + e / nsy] =
+                bad ? nan : (g0 + g1) + (g2 + g3);
         }
     }
-    if (r < per)
-        J.grad_w[(size_t)l * per + r] = bad ? __int_as_float(0x7fc00000) : (a0 + a1) + (a2 + a3);
-    if (with_range && blockIdx.x == 0) {
-        __shared__ double redd[128];
-        double acc = 0.0;
-        for (int z = threadIdx.x; z < J.nz; z += blockDim.x) {
-            const size_t o = (size_t)l * J.nz + z;
+    if (with_range) {
+        __shared__ double redd[kRedThreads];
+        double a = 0.0;
+        for (int z = tid; z < nz; z += kRedThreads) {
+            const size_t o = (size_t)l * nz + z;
             if (idd[z] != 0.0)
-                acc += (double)J.dc[o] * J.didd_dr[o] + (double)J.dsg[o] * J.dsig_dr[o];
+                a += (double)__ldcg(J.dc + o) * J.didd_dr[o] + (double)__ldcg(J.dsg + o) * J.dsig_dr[o];
         }
-        redd[threadIdx.x] = acc;
+        redd[tid] = a;
         __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if ((int)threadIdx.x < w) redd[threadIdx.x] += redd[threadIdx.x + w];
+        for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+            if (tid < w) redd[tid] += redd[tid + w];
             __syncthreads();
         }
-        if (threadIdx.x == 0) J.grad_range[l] = bad ? __int_as_float(0x7fc00000) : (float)redd[0];
+        if (tid == 0) J.grad_range[l] = bad ? nan : (float)redd[0];
     }
-    if (finalize_loss && l == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
-        double s = 0.0;
-        for (int b = 0; b < J.n_loss_part; ++b) s += J.loss_part[b];
-        *J.loss = bad ? (double)__int_as_float(0x7fc00000) : s;
+    if (finalize_loss && l == 0 && tid == 0) {
+        double sum = 0.0;
+        for (int b = 0; b < J.n_loss_part; ++b) sum += J.loss_part[b];
+        *J.loss = bad ? (double)nan : sum;
     }
 }
 
@@ -713,7 +722,9 @@ int tc_adjoint_dims(int precision, const pbd_field* f, int* N1) {
 }
 
 size_t tc_adjoint_slot_elems(const pbd_field* f) {
-    return 3u * (size_t)f->n_layers * f->nz * f->n_sy * f->n_sx;
+    const size_t per = (size_t)f->n_sy * f->n_sx;
+    const size_t nseg = ((size_t)f->nz + kRedZ - 1) / kRedZ;
+    return 3u * (size_t)f->n_layers * f->nz * per + (size_t)f->n_layers * nseg * per;
 }
 
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
@@ -740,17 +751,17 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     const long long units = (long long)nzm * cm * n_jobs;
     if (units > (1LL << 30)) return PBD_ERR_UNSUPPORTED;
     P.n_units = (int)units;
-    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
+    if (n_jobs != 1) return PBD_ERR_UNSUPPORTED;   // per-layer arrival counters of one job
+    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, (2 + (size_t)max_l) * sizeof(int), s)));
     int rc = PBD_OK;
     if (precision == PBD_PREC_BF16) rc = launch_mode<PBD_PREC_BF16>(P, s);
     else rc = launch_mode<PBD_PREC_BF16X3>(P, s);
     PBD_TRY(rc);
-    adj_tc_dots_kernel<<<dim3(nzm, max_l, n_jobs), 256, 0, s>>>(jobs_dev);
+    (void)max_per;
+    adj_tc_reduce_kernel<<<dim3((nzm + kRedZ - 1) / kRedZ, max_l, n_jobs), kRedThreads, 0, s>>>(
+        jobs_dev, with_range, finalize_loss, counter + 1, counter + 2);
     PBD_LAUNCH_CHECK();
-    adj_tc_finalize_kernel<<<dim3((max_per + 127) / 128, max_l, n_jobs), 128, 0, s>>>(
-        jobs_dev, with_range, finalize_loss, counter + 1);
-    PBD_LAUNCH_CHECK();
-    count_launch(3);
+    count_launch(2);
     return PBD_OK;
 }
 

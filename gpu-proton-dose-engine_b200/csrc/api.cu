@@ -120,6 +120,7 @@ struct Ws {
     void* aitems;        // AdjItem (FP32 path) or FwdItem (tensor-core path), 32 B each
     int adj_tc;          // 1: tensor-core adjoint, (layer, slice) dL/dW slots
     int* anch;
+    int* acnt;           // tensor-core adjoint: unit counter, error word, per-layer counters
     float* apart;
     float* dc;
     float* dsg;
@@ -140,6 +141,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
     w.a_chunk = choose_adj_chunk(f);
     w.fitems = nullptr; w.fnch = nullptr; w.fpart = nullptr; w.loss_part = nullptr;
     w.aitems = nullptr; w.anch = nullptr; w.apart = nullptr; w.dc = nullptr; w.dsg = nullptr;
+    w.acnt = nullptr;
     w.f_items = w.a_items = 0;
     if (fwd) {
         size_t pe = 0;
@@ -158,6 +160,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
             w.adj_tc = 1;
             w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : 8;
             pe = tc_adjoint_slot_elems(f);
+            w.acnt = c.take<int>(2 + (size_t)f->n_layers);
         } else {
             PBD_TRY(adj_plan_sizes(f, w.a_chunk, &pe, &w.a_items));
             w.aitems = c.take<AdjItem>(w.a_items);
@@ -357,8 +360,8 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
 static int run_adjoint(const Ws& ws, int precision, const JobDev* A, int with_range,
                        int finalize_loss, cudaStream_t s) {
     if (ws.adj_tc)
-        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, ws.counters + 2, ws.a_chunk,
-                                 with_range, finalize_loss, s);
+        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, ws.acnt, ws.a_chunk, with_range,
+                                 finalize_loss, s);
     return launch_adjoint(ws.jobs + 1, A, 1, static_cast<AdjItem*>(ws.aitems), ws.a_items,
                           ws.counters + 2, ws.a_chunk, with_range, finalize_loss, s);
 }

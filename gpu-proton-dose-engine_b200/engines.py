@@ -249,6 +249,41 @@ class DosePlan:
                 "grad_range": torch.zeros(nl, dtype=torch.float32, device=self.device)}
 
 
+class LossGradGraph:
+    """One ``DosePlan.loss_grad`` captured into a CUDA graph, for loops that evaluate the same
+    field repeatedly (plan optimisation, line searches): a replay launches the library's
+    kernels without the per-call host work.
+
+    The graph reads the weights from ``self.w`` (a device tensor owned by this object); with
+    ``host_w`` (a pinned host tensor of the weights' shape) every replay first uploads it,
+    and with ``host_out`` (a dict of pinned host tensors keyed like the outputs: any of
+    "loss", "grad_w", "grad_range", "dose") every replay ends by downloading those results.
+    ``mask`` and ``presc`` stay referenced; change their contents in place, not the tensors."""
+
+    def __init__(self, plan: "DosePlan", mask, presc, host_w=None, host_out=None):
+        torch = plan.torch
+        self.plan = plan
+        self.mask, self.presc = mask, presc
+        self.w = plan.w.clone()
+        self.out = plan.alloc_outputs()
+        self.host_w, self.host_out = host_w, dict(host_out or {})
+        # first call outside the capture: workspace allocation and schedule lookup
+        plan.loss_grad(mask, presc, w=self.w, outputs=self.out)
+        torch.cuda.synchronize(plan.device)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            if host_w is not None:
+                self.w.copy_(host_w, non_blocking=True)
+            plan.loss_grad(mask, presc, w=self.w, outputs=self.out)
+            for k, t in self.host_out.items():
+                t.copy_(self.out[k], non_blocking=True)
+
+    def replay(self):
+        """Enqueue one evaluation on the current stream; returns the device outputs."""
+        self.graph.replay()
+        return self.out
+
+
 def _autograd_function():
     torch = _lib.require_cuda()
 
