@@ -582,29 +582,46 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
         acc[k] = 0.f;
     }
     const int z0 = seg * kRedZ, z1 = min(nz, z0 + kRedZ);
-    for (int z = z0; z < z1; ++z) {
-        const double c = idd[z];
-        if (c == 0.0) continue;
-        const float cf = (float)c;
-        const float* pz = J.partial + ((size_t)l * nz + z) * per;
-        float pd = 0.f, ps = 0.f;
+    // two slices per iteration, so that both slices' loads are in flight together
+    for (int z = z0; z < z1; z += 2) {
+        float pd[2] = {0.f, 0.f}, ps[2] = {0.f, 0.f};
+        float pv[2][kRedPer], qv[2][kRedPer], cf[2];
 #pragma unroll
-        for (int k = 0; k < kRedPer; ++k) {
-            const int e = tid + k * kRedThreads;
-            if (e < per) {
-                const float p = pz[e];
-                const float q = pz[plane + e] + pz[2 * plane + e];
-                acc[k] = fmaf(cf, p, acc[k]);
-                pd = fmaf(p, wv[k], pd);
-                ps = fmaf(q, wv[k], ps);
+        for (int h = 0; h < 2; ++h) {
+            const double c = z + h < z1 ? idd[z + h] : 0.0;
+            const bool act = c != 0.0;
+            cf[h] = (float)c;
+            const float* pz = J.partial + ((size_t)l * nz + (act ? z + h : z)) * per;
+#pragma unroll
+            for (int k = 0; k < kRedPer; ++k) {
+                const int e = tid + k * kRedThreads;
+                const bool in = act && e < per;
+                pv[h][k] = in ? pz[e] : 0.f;
+                qv[h][k] = in ? pz[plane + e] + pz[2 * plane + e] : 0.f;
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+            for (int k = 0; k < kRedPer; ++k) {
+                acc[k] = fmaf(cf[h], pv[h][k], acc[k]);
+                pd[h] = fmaf(pv[h][k], wv[k], pd[h]);
+                ps[h] = fmaf(qv[h][k], wv[k], ps[h]);
             }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            pd += __shfl_xor_sync(0xffffffffu, pd, o);
-            ps += __shfl_xor_sync(0xffffffffu, ps, o);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                pd[h] += __shfl_xor_sync(0xffffffffu, pd[h], o);
+                ps[h] += __shfl_xor_sync(0xffffffffu, ps[h], o);
+            }
         }
-        if (lane == 0) { sdc[z - z0][warp] = pd; sds[z - z0][warp] = ps; }
+        if (lane == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (z + h < z1) { sdc[z + h - z0][warp] = pd[h]; sds[z + h - z0][warp] = ps[h]; }
+        }
     }
     __syncthreads();
     if (tid < z1 - z0) {
@@ -630,23 +647,25 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     __threadfence();
     const bool bad = *err != 0 || (J.fwd_err != nullptr && *J.fwd_err != 0);
     const float nan = __int_as_float(0x7fc00000);
+    {
+        // segment partials summed in segment order; every entry's load of a segment is
+        // issued together (segments unrolled by 4) so that many loads are in flight
+        float g[kRedPer];
 #pragma unroll
-    for (int k = 0; k < kRedPer; ++k) {
-        const int e = tid + k * kRedThreads;
-        if (e < per) {
-            // four interleaved partial sums (segments s, s+4, ...) combined in a fixed order
-            const float* pe = part + (size_t)l * nseg * per + e;
-            float g0 = 0.f, g1 = 0.f, g2 = 0.f, g3 = 0.f;
-            int sgi = 0;
-            for (; sgi + 4 <= nseg; sgi += 4) {
-                g0 += __ldcg(pe + (size_t)sgi * per);
-                g1 += __ldcg(pe + (size_t)(sgi + 1) * per);
-                g2 += __ldcg(pe + (size_t)(sgi + 2) * per);
-                g3 += __ldcg(pe + (size_t)(sgi + 3) * per);
+        for (int k = 0; k < kRedPer; ++k) g[k] = 0.f;
+        const float* pl = part + (size_t)l * nseg * per;
+#pragma unroll 4
+        for (int sgi = 0; sgi < nseg; ++sgi) {
+#pragma unroll
+            for (int k = 0; k < kRedPer; ++k) {
+                const int e = tid + k * kRedThreads;
+                if (e < per) g[k] += __ldcg(pl + (size_t)sgi * per + e);
             }
-            for (; sgi < nseg; ++sgi) g0 += __ldcg(pe + (size_t)sgi * per);
-            J.grad_w[(size_t)l * per + (size_t)(e % nsy) * nsx + e / nsy] =
-                bad ? nan : (g0 + g1) + (g2 + g3);
+        }
+#pragma unroll
+        for (int k = 0; k < kRedPer; ++k) {
+            const int e = tid + k * kRedThreads;
+            if (e < per) J.grad_w[(size_t)l * per + (size_t)(e % nsy) * nsx + e / nsy] = bad ? nan : g[k];
         }
     }
     if (with_range) {
