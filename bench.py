@@ -46,9 +46,11 @@ def parse():
                     "to tf32x3 (tcgen05, <= 1e-6 of max against FP64)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="clinical", choices=["clinical", "robust", "precision"],
+    ap.add_argument("--workload", default="clinical",
+                    choices=["clinical", "robust", "precision", "optimize"],
                     help="clinical: the headline gradient workload; robust: 4 fields x 25 "
-                    "scenarios batched; precision: forward error vs FP64 per precision mode")
+                    "scenarios batched; precision: forward error vs FP64 per precision mode; "
+                    "optimize: on-device plan-optimisation iterations")
     return ap.parse_args()
 
 
@@ -324,6 +326,72 @@ def robust_bench(args):
     return 0
 
 
+def optimize_bench(args):
+    """Plan optimisation on the device, every iteration one CUDA-graph replay, L2 flushed
+    between iterations (outside the events):
+
+      nominal  projected Adam on the 67,240 spot weights of the 128^3 / 41x41x40 field
+               (masked quadratic loss of the 60 mm target cube)
+      range    the same plus the 40 per-layer range shifts (tables rebuilt every iteration)
+      robust   min-max over 4 fields x 25 scenarios: 100 loss gradients, 4 combinations
+               and 4 Adam updates per iteration"""
+    import torch
+    pb, wl = workload_arrays()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    prec = args.precision or "tf32x3"
+    K, W = args.steps, max(args.warmup, 3)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    prob = pb.model.problem_from_workload(wl)
+    m = torch.as_tensor(wl["mask"], device=dev)
+    p = torch.as_tensor(wl["presc"], device=dev)
+    Adam = pb.optimize.Adam
+    clocks = ClockSampler(0)
+    clocks.start()
+    legs = {}
+
+    def leg(name, opt, steps):
+        opt.step(W)
+        ms = _timed(torch, dev, lambda: opt.step(1), steps, flush)
+        h = opt.history()
+        h = h if h.ndim == 1 else h.sum(0)
+        legs[name] = {"ms_per_iteration": ms, "iterations_per_s": 1e3 / ms, "iterations": steps,
+                      "loss_first": float(h[0]), "loss_last": float(h[-1])}
+
+    n_it = W + K + 1
+    plan = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
+    leg("nominal", pb.optimize.PlanOptimizer(plan, m, p, adam=Adam(lr=0.01), max_iter=n_it), K)
+    plan_r = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
+    leg("range", pb.optimize.PlanOptimizer(plan_r, m, p, adam=Adam(lr=0.01),
+                                           range_adam=Adam(lr=0.01, lo=-0.5, hi=0.5),
+                                           max_iter=n_it), K)
+    del plan, plan_r
+    fields = pb.workloads.robust_fields()
+    sb = pb.robust.ScenarioBatch(pb.robust.robust_problems(fields),
+                                 pb.workloads.robust_scenarios(), precision=prec, device=dev,
+                                 with_grad=True)
+    mr_np, pr_np = pb.workloads.target_loss_arrays(fields[0]["grid"])
+    mr = torch.as_tensor(mr_np, device=dev)
+    pr_ = torch.as_tensor(pr_np, device=dev)
+    kr = max(3, min(K, 20))
+    leg("robust_minmax", pb.optimize.RobustOptimizer(sb, mr, pr_, objective="max",
+                                                      adam=Adam(lr=0.01), max_iter=W + kr + 1),
+        kr)
+    clk = clocks.stop()
+    nom = legs["nominal"]
+    line = {"workload": "optimize", "metric": "plan-optimisation iterations/s (projected Adam "
+            "on 67,240 spot weights, 128^3 / 41x41x40)", "value": nom["iterations_per_s"],
+            "unit": "iterations/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": nom["ms_per_iteration"], "higher_is_better": True, "dtype": prec,
+            "data": "synthetic",
+            "config": {"workload": "128^3 / 41x41x40 masked quadratic loss; robust: 4 fields x "
+                       "25 scenarios", "precision": prec,
+                       "l2": "flushed between iterations (256 MiB write, outside the events)"},
+            "legs": legs, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def precision_bench(args):
     """Forward of the 200x200x256 / 61x61x60 field in every precision mode: time per call
     (L2 flushed between calls) and error against the FP64 oracle on the host."""
@@ -383,6 +451,8 @@ def main():
         return robust_bench(args)
     if args.workload == "precision":
         return precision_bench(args)
+    if args.workload == "optimize":
+        return optimize_bench(args)
     import torch
     import torch.distributed as dist
 

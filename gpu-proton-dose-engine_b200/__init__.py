@@ -16,17 +16,18 @@ Modules
   physics    device depth-LUT builder (FP64) and range-table lookups
   engines    torch_separable, the autograd function, the fused loss gradient
   robust     batched fields x scenarios in one persistent launch, CUDA graphs
+  optimize   on-device plan optimisation (projected Adam, robust mean / min-max), CUDA graphs
   tuning     measured choice of the work-item sizes, cached per geometry
   distributed  depth-slab and job sharding over torch.distributed (one GPU per rank)
   workloads  synthetic workloads of the benchmark shapes (host, NumPy)
 """
 import sys as _sys
 
-from . import workloads, _lib, physics, model, engines, robust, tuning, distributed  # noqa: F401
+from . import workloads, _lib, physics, model, engines, robust, tuning, distributed, optimize  # noqa: F401
 
 __version__ = "0.1.0"
 
 _sys.modules.setdefault("pbdose_b200", _sys.modules[__name__])
 for _name in ("workloads", "_lib", "physics", "model", "engines", "robust", "tuning",
-              "distributed"):
+              "distributed", "optimize"):
     _sys.modules.setdefault("pbdose_b200." + _name, _sys.modules[__name__ + "." + _name])

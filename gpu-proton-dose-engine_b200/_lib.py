@@ -51,6 +51,14 @@ class Job(ctypes.Structure):
                 ("dose", c_void_p)]
 
 
+class AdamParams(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("eps", ctypes.c_float), ("lo", ctypes.c_float), ("hi", ctypes.c_float),
+                ("grad_scale", ctypes.c_float)]
+
+
+OBJ = {"mean": 0, "max": 1}
+
 _SIGS = {
     "pbd_strerror": (c_char_p, [c_int]),
     "pbd_version": (c_int, []),
@@ -79,6 +87,10 @@ _SIGS = {
                                     c_void_p]),
     "pbd_forward_batch_workspace": (c_int, [POINTER(Job), c_int, c_int, POINTER(c_size_t)]),
     "pbd_forward_batch": (c_int, [POINTER(Job), c_int, c_int, c_void_p, c_size_t, c_void_p]),
+    "pbd_adam_step": (c_int, [POINTER(AdamParams), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "pbd_scenario_combine": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p]),
 }
 
 _lib = None

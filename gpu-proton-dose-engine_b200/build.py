@@ -30,6 +30,7 @@ SOURCES = {
     "tc_fwd.cu": [],
     "noalloc.cu": [],
     "adj_tc.cu": [],
+    "optim.cu": [],
 }
 
 

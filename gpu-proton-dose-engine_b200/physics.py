@@ -96,6 +96,47 @@ def build_tables(nz: int, z0: float, dz: float, energies, *, range_shift=None,
     return DepthTables(idd=idd, sigma=sig, didd_dr=didd, dsigma_dr=dsig, fd_step=fd_step)
 
 
+class TableBuilder:
+    """Rebuilds one field's depth tables in place: the outputs and the workspace are
+    allocated once, so ``build`` only enqueues the builder's kernels and can run inside a
+    captured CUDA graph, reading the range shifts from a device float64 vector."""
+
+    def __init__(self, nz: int, z0: float, dz: float, energies, *, fd_step: float = 0.0,
+                 device=None, **spec_kw):
+        torch = _lib.require_cuda()
+        self.torch = torch
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        self.energies = torch.as_tensor(np.asarray(energies, dtype=np.float64),
+                                        device=self.device).contiguous()
+        self.n_layers = int(self.energies.numel())
+        self.spec = lut_spec(nz, z0, dz, fd_step=fd_step, **spec_kw)
+        nbytes = _lib.query("pbd_lut_workspace", ctypes.byref(self.spec), self.n_layers)
+        self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        shape = (self.n_layers, nz)
+        f64 = torch.float64
+        self.tables = DepthTables(
+            idd=torch.empty(shape, dtype=f64, device=self.device),
+            sigma=torch.empty(shape, dtype=f64, device=self.device),
+            didd_dr=torch.empty(shape, dtype=f64, device=self.device) if fd_step > 0 else None,
+            dsigma_dr=torch.empty(shape, dtype=f64, device=self.device) if fd_step > 0 else None,
+            fd_step=fd_step)
+
+    def build(self, range_shift=None) -> DepthTables:
+        """Enqueue the rebuild at CSDA ranges R0_l + range_shift_l (``range_shift``: a device
+        float64 tensor of L entries, or None) on the current stream."""
+        if range_shift is not None and (range_shift.dtype != self.torch.float64
+                                        or range_shift.numel() != self.n_layers
+                                        or not range_shift.is_contiguous()):
+            raise ValueError("range_shift must be a contiguous float64 tensor of L entries")
+        t = self.tables
+        _lib.call("pbd_build_luts", ctypes.byref(self.spec), self.n_layers, _lib.ptr(self.energies),
+                  _lib.ptr(range_shift), _lib.ptr(t.idd), _lib.ptr(t.sigma), _lib.ptr(t.didd_dr),
+                  _lib.ptr(t.dsigma_dr), _lib.ptr(self.ws), self.ws.numel(),
+                  _lib.stream_handle(self.device))
+        return t
+
+
 def _uniform_axis(z):
     z = np.asarray(z, dtype=np.float64)
     if z.ndim != 1 or z.size == 0:

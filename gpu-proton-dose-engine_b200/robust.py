@@ -134,17 +134,29 @@ class ScenarioBatch:
 
     # -- gradients of every job ----------------------------------------------------------
     def alloc_grad_outputs(self):
+        """Per-job gradient outputs.  The dL/dW and loss of one field's scenarios are views
+        of one contiguous block, ``field_grads[f]`` (S, L, nsy, nsx) and
+        ``field_losses[f]`` (S,), which a robust objective combines in one call."""
+        if getattr(self, "grad_outputs", None):
+            return self.grad_outputs
         torch = self.torch
+        n_s = len(self.scenarios)
+        self.field_grads, self.field_losses = [], []
         outs = []
-        for k in range(self.n_jobs):
-            f = self.jobs[k].field
-            outs.append({"grad_dose": torch.empty((f.nz, f.ny, f.nx), dtype=torch.float32,
-                                                  device=self.device),
-                         "loss": torch.zeros((), dtype=torch.float64, device=self.device),
-                         "grad_w": torch.empty((f.n_layers, f.n_sy, f.n_sx), dtype=torch.float32,
-                                               device=self.device),
-                         "grad_range": torch.zeros(f.n_layers, dtype=torch.float32,
-                                                   device=self.device)})
+        for fi in range(len(self.problems)):
+            f = self.jobs[fi * n_s].field
+            gw = torch.empty((n_s, f.n_layers, f.n_sy, f.n_sx), dtype=torch.float32,
+                             device=self.device)
+            ls = torch.zeros(n_s, dtype=torch.float64, device=self.device)
+            self.field_grads.append(gw)
+            self.field_losses.append(ls)
+            for si in range(n_s):
+                outs.append({"grad_dose": torch.empty((f.nz, f.ny, f.nx), dtype=torch.float32,
+                                                      device=self.device),
+                             "loss": ls[si],
+                             "grad_w": gw[si],
+                             "grad_range": torch.zeros(f.n_layers, dtype=torch.float32,
+                                                       device=self.device)})
         self.grad_outputs = outs
         return outs
 

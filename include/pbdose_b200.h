@@ -187,6 +187,38 @@ PBD_API int pbd_forward_batch_workspace(const pbd_job *jobs, int n_jobs, int pre
 PBD_API int pbd_forward_batch(const pbd_job *jobs, int n_jobs, int precision,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- plan-optimisation steps (no counterpart in the reference) ---------------------
+ * Device-resident state, so that an optimisation iteration (tables, loss gradient,
+ * combination, update) can be captured into one CUDA graph and replayed. */
+
+/* Projected Adam (Kingma & Ba 2015, Algorithm 1) in FP32:
+ *   g' = grad_scale * g;  m = b1 m + (1-b1) g';  v = b2 v + (1-b2) g'^2;
+ *   x = clamp(x - lr * (m / (1-b1^t)) / (sqrt(v / (1-b2^t)) + eps), lo, hi)
+ * with t = state[0] + 1.  state: device int[2], zero before the first step; state[0] counts
+ * completed steps (the call increments it), state[1] is scratch and stays 0 between calls.
+ * n == 0 enqueues nothing (x, m, v, grad may then be NULL; the count does not advance).
+ * x64 (may be NULL) receives a float64 copy of x (e.g. the range shifts the LUT builder
+ * reads).  If hist_len > 0, the value at `loss` (a device float64 scalar, the loss of the
+ * gradient being applied) is stored at loss_hist[t-1] for t <= hist_len. */
+typedef struct pbd_adam_params {
+    float lr, beta1, beta2, eps;
+    float lo, hi;          /* projection box; -inf / +inf for none */
+    float grad_scale;      /* multiplies the gradient before the update */
+} pbd_adam_params;
+PBD_API int pbd_adam_step(const pbd_adam_params *p, int n, float *x, float *m, float *v,
+                          const float *grad, int *state, double *x64, const double *loss,
+                          double *loss_hist, int hist_len, void *stream);
+
+/* Robust objective over n_scen scenarios of one field: grads is (n_scen, n), losses
+ * (n_scen) float64.  PBD_OBJ_MEAN: out_grad = (sum_s grads[s]) / n_scen in scenario order,
+ * out_loss = mean loss.  PBD_OBJ_MAX (min-max): the scenario with the largest loss (the
+ * first on ties) gives out_grad and out_loss.  out_loss may be NULL. */
+#define PBD_OBJ_MEAN 0
+#define PBD_OBJ_MAX  1
+PBD_API int pbd_scenario_combine(int mode, int n_scen, int n, const float *grads,
+                                 const double *losses, float *out_grad, double *out_loss,
+                                 void *stream);
+
 #ifdef __cplusplus
 }
 #endif

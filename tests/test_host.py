@@ -77,6 +77,37 @@ def test_entry_points_validate_before_device_work(pb, lib):
     assert lib.pbd_set_schedule(0, 0) == 0
 
 
+def test_optimizer_steps_validate_before_device_work(pb, lib):
+    fake = 0x1000
+    P = pb._lib.AdamParams
+    ok = P(lr=0.01, beta1=0.9, beta2=0.999, eps=1e-8, lo=0.0, hi=float("inf"), grad_scale=1.0)
+    st = ctypes.c_void_p(fake)
+    assert lib.pbd_adam_step(None, 4, fake, fake, fake, fake, st, None, None, None, 0, None) == -1
+    assert lib.pbd_adam_step(ctypes.byref(ok), 4, fake, fake, fake, fake, None, None, None, None,
+                             0, None) == -1
+    assert lib.pbd_adam_step(ctypes.byref(ok), 4, None, fake, fake, fake, st, None, None, None, 0,
+                             None) == -1
+    assert lib.pbd_adam_step(ctypes.byref(ok), -1, fake, fake, fake, fake, st, None, None, None,
+                             0, None) == -2
+    assert lib.pbd_adam_step(ctypes.byref(ok), 4, fake, fake, fake, fake, st, None, None, None,
+                             8, None) == -1                      # history without a loss
+    for bad in (dict(lr=float("nan")), dict(lr=-1.0), dict(beta1=1.0), dict(beta2=-0.1),
+                dict(eps=0.0), dict(lo=1.0, hi=0.0), dict(grad_scale=float("inf"))):
+        kw = dict(lr=0.01, beta1=0.9, beta2=0.999, eps=1e-8, lo=0.0, hi=1.0, grad_scale=1.0)
+        kw.update(bad)
+        assert lib.pbd_adam_step(ctypes.byref(P(**kw)), 4, fake, fake, fake, fake, st, None, None,
+                                 None, 0, None) == -10, bad
+    # n == 0 enqueues nothing and succeeds
+    assert lib.pbd_adam_step(ctypes.byref(ok), 0, None, None, None, None, st, None, None, None, 0,
+                             None) == 0
+    assert lib.pbd_scenario_combine(2, 3, 4, fake, fake, fake, None, None) == -10
+    assert lib.pbd_scenario_combine(0, 0, 4, fake, fake, fake, None, None) == -2
+    assert lib.pbd_scenario_combine(1, 129, 4, fake, fake, fake, None, None) == -2
+    assert lib.pbd_scenario_combine(1, 3, 4, None, fake, fake, None, None) == -1
+    assert lib.pbd_scenario_combine(1, 3, 4, fake, None, fake, None, None) == -1
+    assert lib.pbd_scenario_combine(1, 3, 0, None, fake, None, None, None) == 0
+
+
 def test_batch_limits(pb, lib):
     jobs = (pb._lib.Job * 129)()
     for k in range(129):
