@@ -47,10 +47,10 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="clinical",
-                    choices=["clinical", "robust", "precision", "optimize"],
+                    choices=["clinical", "robust", "precision", "optimize", "gamma"],
                     help="clinical: the headline gradient workload; robust: 4 fields x 25 "
                     "scenarios batched; precision: forward error vs FP64 per precision mode; "
-                    "optimize: on-device plan-optimisation iterations")
+                    "optimize: on-device plan-optimisation iterations; gamma: gamma index")
     return ap.parse_args()
 
 
@@ -392,6 +392,74 @@ def optimize_bench(args):
     return 0
 
 
+def gamma_bench(args):
+    """Gamma index of two doses of the clinical field (128^3, 2 mm; the evaluation has the
+    spot lattice moved 1 mm in x and 1 % more weight) at 3 %/3 mm and 2 %/2 mm, and of two
+    doses of the 200 x 200 x 256 field of 1 mm voxels at 3 %/3 mm (123 search offsets).  One
+    ``GammaPlan.run`` per step (map, mask, statistics and percentiles), L2 flushed between
+    steps; the oracle's float64 NumPy gamma index on the host is the CPU baseline."""
+    import torch
+    pb = importlib.import_module("gpu-proton-dose-engine_b200")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    K, W = args.steps, max(args.warmup, 3)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    legs = {}
+    pairs = {}
+    for cfg in (1, 4):
+        wl = pb.workloads.build_workload(cfg)
+        prob = pb.model.problem_from_workload(wl)
+        plan = pb.engines.DosePlan(prob, tables="device", precision="tf32x3", device=dev)
+        ref = plan.forward()
+        prob.lattice.x0 += 0.1
+        plan2 = pb.engines.DosePlan(prob, tables="device", precision="tf32x3", device=dev)
+        ev = plan2.forward(plan2.w * 1.01)
+        g = wl["grid"]
+        pairs[cfg] = (ref, ev, (g["dz"], g["dy"], g["dx"]))
+    cases = [("clinical_3mm_3pct", 1, 3.0, 3.0), ("clinical_2mm_2pct", 1, 2.0, 2.0),
+             ("fine_1mm_grid_3mm_3pct", 4, 3.0, 3.0)]
+    for name, cfg, dp, dta in cases:
+        ref, ev, sp = pairs[cfg]
+        spec = pb.gamma.gamma_spec(sp, dose_crit_pct=dp, dta_mm=dta)
+        gp = pb.gamma.GammaPlan(ref.shape, spec, device=dev)
+        for _ in range(W):
+            gp.run(ref, ev)
+        ms = _timed(torch, dev, lambda: gp.run(ref, ev), K, flush)
+        st = gp.stats()
+        n_vox = ref.numel()
+        legs[name] = {"ms": ms, "analyses_per_s": 1e3 / ms, "voxels": n_vox,
+                      "voxels_per_s": n_vox * 1e3 / ms, "offsets": st.n_dta_offsets,
+                      "pass_rate": st.pass_rate, "gamma_p95": st.gamma_p95,
+                      "n_eval": st.n_eval}
+    clk = clocks.stop()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import gamma_ref
+        ref, ev, sp = pairs[1]
+        r64, e64 = ref.double().cpu().numpy(), ev.double().cpu().numpy()
+        t0 = time.perf_counter()
+        n = 0
+        while n < 3 and (n == 0 or time.perf_counter() - t0 < args.cpu_budget_s):
+            gamma_ref.gamma_index(r64, e64, spacing=sp)
+            n += 1
+        el = time.perf_counter() - t0
+        cpu = {"value": n / el, "unit": "analyses/s", "cores": 1, "kind": "port",
+               "sample": f"{n} full 128^3 gamma analyses at 3 %/3 mm (NumPy float64)"}
+    head = legs["clinical_3mm_3pct"]
+    line = {"workload": "gamma", "metric": "gamma analyses/s, 128^3 dose pair at 3 %/3 mm",
+            "value": head["analyses_per_s"], "unit": "analyses/s", "n_gpus": 1, "steps": K,
+            "warmup": W, "ms_per_step": head["ms"], "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "gamma index of TF32x3 doses: clinical 128^3 field vs the "
+                       "same with the lattice moved 1 mm and +1 % weight; 200x200x256 1 mm "
+                       "field likewise", "l2": "flushed between steps"},
+            "legs": legs, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def precision_bench(args):
     """Forward of the 200x200x256 / 61x61x60 field in every precision mode: time per call
     (L2 flushed between calls) and error against the FP64 oracle on the host."""
@@ -453,6 +521,8 @@ def main():
         return precision_bench(args)
     if args.workload == "optimize":
         return optimize_bench(args)
+    if args.workload == "gamma":
+        return gamma_bench(args)
     import torch
     import torch.distributed as dist
 

@@ -59,6 +59,24 @@ class AdamParams(ctypes.Structure):
 
 OBJ = {"mean": 0, "max": 1}
 
+
+class GammaSpec(ctypes.Structure):
+    _fields_ = [("dz", c_double), ("dy", c_double), ("dx", c_double),
+                ("dose_crit_pct", c_double), ("dta_mm", c_double), ("threshold_pct", c_double),
+                ("normalization", c_int), ("use_ref_dose", c_int), ("ref_dose", c_double),
+                ("max_vox", c_int)]
+
+
+class GammaStats(ctypes.Structure):
+    _fields_ = [("pass_rate", c_double), ("gamma_mean", c_double), ("gamma_max", c_double),
+                ("gamma_p95", c_double), ("gamma_p99", c_double), ("ref_max", c_double),
+                ("n_eval", ctypes.c_longlong), ("n_pass", ctypes.c_longlong),
+                ("n_dta_offsets", c_int), ("mask_fallback", c_int), ("status", c_int),
+                ("reserved", c_int)]
+
+
+DTYPE = {"float32": 0, "float64": 1}
+
 _SIGS = {
     "pbd_strerror": (c_char_p, [c_int]),
     "pbd_version": (c_int, []),
@@ -91,6 +109,10 @@ _SIGS = {
                               c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "pbd_scenario_combine": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                      c_void_p]),
+    "pbd_gamma_offsets": (c_int, [POINTER(GammaSpec), POINTER(c_int), c_void_p, c_void_p]),
+    "pbd_gamma_workspace": (c_int, [c_int, c_int, c_int, POINTER(c_size_t)]),
+    "pbd_gamma_index": (c_int, [POINTER(GammaSpec), c_int, c_int, c_int, c_void_p, c_void_p, c_int,
+                                c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
 }
 
 _lib = None

@@ -31,6 +31,7 @@ SOURCES = {
     "noalloc.cu": [],
     "adj_tc.cu": [],
     "optim.cu": [],
+    "gamma.cu": [],
 }
 
 

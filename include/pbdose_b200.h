@@ -219,6 +219,51 @@ PBD_API int pbd_scenario_combine(int mode, int n_scen, int n, const float *grads
                                  const double *losses, float *out_grad, double *out_loss,
                                  void *stream);
 
+/* ---- gamma index (replaces gamma.py:41-60 dta_offsets, 81-160 gamma_index and 213-261
+ * gamma_index_torch) -------------------------------------------------------------------------
+ *   gamma(r)^2 = min over integer voxel offsets o, |o| <= DTA (at most max_vox voxels per axis),
+ *                of (|o|/DTA)^2 + ((E[r+o] - R[r]) / dose_crit(r))^2,   E = 0 outside the grid
+ *   dose_crit = pct/100 * ref_max (global) or pct/100 * max(R[r], 1e-12) (local)
+ *   mask = R >= threshold_pct/100 * ref_max, or R > 0 when that mask is empty
+ *   ref_max = max(R), or ref_dose when use_ref_dose.
+ * Computed in float64 with the reference's order of operations: the gamma map, mask, counts,
+ * maximum and the NumPy-'linear' 95th / 99th percentiles equal the reference's float64
+ * results; the mean is a fixed-order sum.  reference / evaluation: (nz, ny, nx) device arrays
+ * of `dtype`; gamma_map (float64) and mask_map (0/1 bytes) may be NULL; `stats` is a DEVICE
+ * pointer, written at the end of the call (status = PBD_ERR_BAD_VALUE when ref_max <= 0 or no
+ * voxel is evaluated, as gamma.py:112-113 raises). */
+#define PBD_GAMMA_GLOBAL 0
+#define PBD_GAMMA_LOCAL  1
+#define PBD_DTYPE_F32 0
+#define PBD_DTYPE_F64 1
+typedef struct pbd_gamma_spec {
+    double dz, dy, dx;          /* voxel spacing, cm */
+    double dose_crit_pct;       /* 3.0 = 3 % */
+    double dta_mm;
+    double threshold_pct;       /* low-dose threshold, % of ref_max */
+    int normalization;          /* PBD_GAMMA_GLOBAL or PBD_GAMMA_LOCAL */
+    int use_ref_dose;           /* 1: ref_max = ref_dose */
+    double ref_dose;
+    int max_vox;                /* search radius cap per axis, 0..6 (the reference uses 6) */
+} pbd_gamma_spec;
+typedef struct pbd_gamma_stats {
+    double pass_rate, gamma_mean, gamma_max, gamma_p95, gamma_p99, ref_max;
+    long long n_eval, n_pass;
+    int n_dta_offsets;
+    int mask_fallback;          /* 1: the statistics used R > 0 */
+    int status;
+    int reserved;
+} pbd_gamma_stats;
+/* Host only: the search offsets of a spec (count, radii z/y/x, and the weights (|o|/DTA)^2
+ * as a 7x7x7 table over (|a|, |b|, |c|), -1 outside the ball); radii / weights may be NULL. */
+PBD_API int pbd_gamma_offsets(const pbd_gamma_spec *spec, int *n_offsets, int *radii,
+                              double *weights);
+PBD_API int pbd_gamma_workspace(int nz, int ny, int nx, size_t *bytes);
+PBD_API int pbd_gamma_index(const pbd_gamma_spec *spec, int nz, int ny, int nx,
+                            const void *reference, const void *evaluation, int dtype,
+                            double *gamma_map, unsigned char *mask_map, pbd_gamma_stats *stats,
+                            void *workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
