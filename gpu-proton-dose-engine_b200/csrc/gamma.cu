@@ -25,7 +25,8 @@
 //                         appended to a key list; per-block partial sums and maxima
 //   (same kernel, fallback pass: runs only when the threshold mask was empty)
 //   gamma_finish_kernel   counts, mean, max, pass rate, percentile ranks (NumPy 'linear')
-//   gamma_hist/scan       radix select of the four order statistics the percentiles need
+//   gamma_select_kernel   radix select of the four order statistics the percentiles need (one
+//                         launch per digit; the last block to arrive picks the digits)
 //   gamma_final_kernel    NumPy's interpolation between the order statistics
 #include <math.h>
 #include <string.h>
@@ -47,13 +48,18 @@ constexpr int kBins = 1 << kDigitBits;
 constexpr int kSelPasses = 6;          // 6 x 11 bits cover the 64-bit keys
 constexpr int kHistThreads = 512;
 constexpr int kFinThreads = 1024;
-// largest staged brick: radius 6 on every axis
-constexpr int kGMaxSmem = (kTX + 12) * (kTY + 12) * (kTZ + 12) * (int)sizeof(double);
+constexpr int kSelPer = 16;            // keys per thread a select pass aims at
+constexpr int kRowBatch = 4;           // staged rows per warp whose loads are issued together
+// largest staged brick (radius 6 on every axis) and offset list (13^3 offsets)
+constexpr int kGMaxOff = 13 * 13 * 13;
+constexpr int kGMaxSmem = (kTX + 12) * (kTY + 12) * (kTZ + 12) * (int)sizeof(double) +
+                          kGMaxOff * (int)(sizeof(double) + sizeof(int));
 
 struct GammaParams {
     int nz, ny, nx;
     int hz, hy, hx;
     int n_entries;                     // distinct (|a|,|b|,|c|) inside the ball
+    int n_off;                         // offsets (entries with their signs)
     int local;
     int use_ref_dose;
     int want_gamma, want_mask;
@@ -63,6 +69,7 @@ struct GammaParams {
     double q[2];                       // 95/100, 99/100
     double w[kGTab];                   // (|o|/DTA)^2, ascending
     unsigned char abc[kGTab][4];       // |a|, |b|, |c| of each entry
+    short start[kGTab];                // first offset of each entry in the expanded list
 };
 
 // Device state in the workspace.
@@ -79,6 +86,8 @@ struct GammaState {
     double vir[2];                     // NumPy virtual indexes of p95, p99 (-1: use max)
     double mean, maxv, pass_rate;
     unsigned long long n_eval, n_pass, n_nan;
+    unsigned int sel_arrive;           // blocks of the current select pass that finished
+    unsigned long long n_cand;         // keys copied to the candidate list
 };
 
 // Order-preserving map of a double to an unsigned key (NaN above +inf).
@@ -105,9 +114,14 @@ template <class T>
 __global__ void __launch_bounds__(kGThreads)
 gamma_refmax_kernel(const T* __restrict__ ref, size_t n, GammaState* st) {
     unsigned long long best = 0ull;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (size_t)gridDim.x * blockDim.x)
-        best = max(best, dkey(ld(ref, i)));
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {          // four loads in flight
+        const double a = ld(ref, i), b = ld(ref, i + stride), c = ld(ref, i + 2 * stride),
+                     d = ld(ref, i + 3 * stride);
+        best = max(max(best, dkey(a)), max(dkey(b), max(dkey(c), dkey(d))));
+    }
+    for (; i < n; i += stride) best = max(best, dkey(ld(ref, i)));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
     if ((threadIdx.x & 31) == 0 && best) atomicMax(&st->ref_key, best);
@@ -118,93 +132,149 @@ __global__ void __launch_bounds__(kGThreads)
 gamma_kernel(const GammaParams P, const T* __restrict__ ref, const T* __restrict__ ev,
              double* __restrict__ gmap, unsigned char* __restrict__ mmap, GammaState* st,
              unsigned long long* __restrict__ keys, double* __restrict__ part_sum,
-             double* __restrict__ part_max) {
+             double* __restrict__ part_max, int gx, int gy, int n_bricks) {
     extern __shared__ double tile[];
     __shared__ double red_s[kGThreads / 32], red_m[kGThreads / 32];
     __shared__ unsigned long long red_c[kGThreads / 32][3];
+    __shared__ unsigned int s_wcnt[kGThreads / 32], s_wpre[kGThreads / 32];
+    __shared__ unsigned long long s_base;
     __shared__ int s_nonfinite;
     const int pass = kFallback ? 1 : 0;
     if (kFallback && __ldcg(&st->cnt[0][0]) != 0ull) return;   // the threshold mask is used
     const double ref_max = P.use_ref_dose ? P.ref_dose : dunkey(__ldcg(&st->ref_key));
     if (ref_max <= 0.0) {                                      // gamma.py:112-113
-        if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0)
-            st->status = PBD_ERR_BAD_VALUE;
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->status = PBD_ERR_BAD_VALUE;
         return;
     }
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * kTZ;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int TX = kTX + 2 * P.hx, TY = kTY + 2 * P.hy, TZ = kTZ + 2 * P.hz;
     const int plane = TX * TY;
-    if (tid == 0) s_nonfinite = 0;
-    __syncthreads();
-    int nonfin = 0;
-    for (int i = tid; i < plane * TZ; i += kGThreads) {
-        const int tz = i / plane, r = i - tz * plane, ty = r / TX, tx = r - ty * TX;
-        const int z = z0 - P.hz + tz, y = y0 - P.hy + ty, x = x0 - P.hx + tx;
-        double v = 0.0;
-        if (z >= 0 && z < P.nz && y >= 0 && y < P.ny && x >= 0 && x < P.nx)
-            v = ld(ev, ((size_t)z * P.ny + y) * P.nx + x);
-        nonfin |= !finite_d(v);
-        tile[i] = v;
+    double* s_w = tile + (size_t)plane * TZ;                    // weight of each offset
+    int* s_off = reinterpret_cast<int*>(s_w + P.n_off);         // its position in the tile
+    // offsets of each (|a|,|b|,|c|) entry with their signs, in ascending weight
+    for (int u = tid; u < P.n_entries; u += kGThreads) {
+        const int ia = P.abc[u][0], ib = P.abc[u][1], ic = P.abc[u][2];
+        int o = P.start[u];
+        for (int sgn = 0; sgn < 8; ++sgn) {
+            if (((sgn & 4) && ia == 0) || ((sgn & 2) && ib == 0) || ((sgn & 1) && ic == 0))
+                continue;
+            const int sa = (sgn & 4) ? -ia : ia, sb = (sgn & 2) ? -ib : ib, sc = (sgn & 1) ? -ic : ic;
+            s_w[o] = P.w[u];
+            s_off[o] = sa * plane + sb * TX + sc;
+            ++o;
+        }
     }
-    if (nonfin) s_nonfinite = 1;
-    __syncthreads();
-    const bool tile_finite = s_nonfinite == 0;
     const double crit_g = __dmul_rn(P.crit_frac, ref_max);     // global dose criterion
     const double thr_dose = __dmul_rn(P.thr_frac, ref_max);
     const bool ok_g = finite_d(crit_g) || P.local;
-    const int tx = tid & 31, ty = tid >> 5;
-    const int x = x0 + tx, y = y0 + ty;
+    const int tx = lane, ty = warp;
     double sum = 0.0, mx = -1.0;                 // gamma >= 0
     unsigned long long c_eval = 0, c_pass = 0, c_nan = 0;
-    const int lane = tid & 31;
-    for (int k = 0; k < kTZ; ++k) {
-        const int z = z0 + k;
-        const bool in = x < P.nx && y < P.ny && z < P.nz;
-        double g = 0.0;
-        bool masked = false;
-        if (in) {
-            const size_t v = ((size_t)z * P.ny + y) * P.nx + x;
-            const double r = ld(ref, v);
-            const double crit = P.local ? __dmul_rn(P.crit_frac, r > 1e-12 || r != r ? r : 1e-12)
-                                        : crit_g;
-            // early exit is exact when no NaN can appear later: finite doses, a finite
-            // non-zero criterion (NaN needs 0/0, inf - inf or inf/inf)
-            const bool fast = tile_finite && finite_d(r) && finite_d(crit) && crit != 0.0 && ok_g;
-            const double* c0 = tile + (size_t)(k + P.hz) * plane + (ty + P.hy) * TX + (tx + P.hx);
-            double best = __longlong_as_double(0x7FF0000000000000ll);    // +inf
-            for (int u = 0; u < P.n_entries; ++u) {
-                const double w = P.w[u];
-                if (fast && w >= best) break;    // w + d^2 >= w >= best for this and later
-                const int ia = P.abc[u][0], ib = P.abc[u][1], ic = P.abc[u][2];
-                for (int s = 0; s < 8; ++s) {
-                    const int sa = (s & 4) ? -ia : ia, sb = (s & 2) ? -ib : ib,
-                              sc = (s & 1) ? -ic : ic;
-                    if (((s & 4) && ia == 0) || ((s & 2) && ib == 0) || ((s & 1) && ic == 0))
-                        continue;
-                    const double e = c0[sa * plane + sb * TX + sc];
-                    const double dd = __ddiv_rn(__dsub_rn(e, r), crit);
-                    best = nmin(best, __dadd_rn(w, __dmul_rn(dd, dd)));
+    // bricks of 32 x 8 x 4 voxels, statically strided over the persistent blocks
+    for (int brick = blockIdx.x; brick < n_bricks; brick += gridDim.x) {
+        const int bx = brick % gx, rest = brick / gx, by = rest % gy, bz = rest / gy;
+        const int x0 = bx * kTX, y0 = by * kTY, z0 = bz * kTZ;
+        const int x = x0 + tx, y = y0 + ty;
+        // this thread's reference doses, loaded before the staging barrier
+        double rv[kTZ];
+#pragma unroll
+        for (int k = 0; k < kTZ; ++k) {
+            const int z = z0 + k;
+            rv[k] = (x < P.nx && y < P.ny && z < P.nz)
+                        ? ld(ref, ((size_t)z * P.ny + y) * P.nx + x) : 0.0;
+        }
+        __syncthreads();                         // the previous brick is done with the tile
+        if (tid == 0) s_nonfinite = 0;
+        __syncthreads();
+        // the evaluated dose of the brick and its halo: each warp takes rows of TX voxels,
+        // kRowBatch rows' loads issued before their stores
+        int nonfin = 0;
+        const int n_rows = TY * TZ;
+        for (int row0 = warp; row0 < n_rows; row0 += kRowBatch * (kGThreads / 32)) {
+            for (int t0 = 0; t0 < TX; t0 += 32) {
+                double v[kRowBatch];
+#pragma unroll
+                for (int q = 0; q < kRowBatch; ++q) {
+                    const int row = row0 + q * (kGThreads / 32);
+                    const int tz = row / TY, tyy = row - tz * TY;
+                    const int z = z0 - P.hz + tz, yy = y0 - P.hy + tyy, xx = x0 - P.hx + t0 + lane;
+                    const bool ok = row < n_rows && t0 + lane < TX && z >= 0 && z < P.nz &&
+                                    yy >= 0 && yy < P.ny && xx >= 0 && xx < P.nx;
+                    v[q] = ok ? ld(ev, ((size_t)z * P.ny + yy) * P.nx + xx) : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < kRowBatch; ++q) {
+                    const int row = row0 + q * (kGThreads / 32);
+                    if (row < n_rows && t0 + lane < TX) {
+                        nonfin |= !finite_d(v[q]);
+                        tile[row * TX + t0 + lane] = v[q];
+                    }
                 }
             }
-            g = __dsqrt_rn(best);
-            masked = kFallback ? (r > 0.0) : (r >= thr_dose);
-            if (!kFallback && P.want_gamma) gmap[v] = g;
-            if (P.want_mask) mmap[v] = masked ? 1 : 0;
         }
-        // masked voxels: counts, partial sum / max, and the key list for the percentiles
-        if (masked) {
-            ++c_eval;
-            c_pass += g <= 1.0;
-            if (g != g) ++c_nan;
-            else { sum = __dadd_rn(sum, g); mx = g > mx ? g : mx; }
+        if (nonfin) s_nonfinite = 1;
+        __syncthreads();
+        const bool tile_finite = s_nonfinite == 0;
+        double gk[kTZ];
+        unsigned int bal[kTZ];
+        unsigned int wcnt = 0;
+#pragma unroll
+        for (int k = 0; k < kTZ; ++k) {
+            const int z = z0 + k;
+            const bool in = x < P.nx && y < P.ny && z < P.nz;
+            double g = 0.0;
+            bool masked = false;
+            if (in) {
+                const size_t v = ((size_t)z * P.ny + y) * P.nx + x;
+                const double r = rv[k];
+                masked = kFallback ? (r > 0.0) : (r >= thr_dose);
+                // without a gamma map only masked voxels need their gamma
+                if (masked || (!kFallback && P.want_gamma)) {
+                    const double crit =
+                        P.local ? __dmul_rn(P.crit_frac, r > 1e-12 || r != r ? r : 1e-12) : crit_g;
+                    // early exit is exact when no NaN can appear later: finite doses, a finite
+                    // non-zero criterion (NaN needs 0/0, inf - inf or inf/inf)
+                    const bool fast =
+                        tile_finite && finite_d(r) && finite_d(crit) && crit != 0.0 && ok_g;
+                    const double* c0 =
+                        tile + (size_t)(k + P.hz) * plane + (ty + P.hy) * TX + (tx + P.hx);
+                    double best = __longlong_as_double(0x7FF0000000000000ll);    // +inf
+                    for (int j = 0; j < P.n_off; ++j) {
+                        const double w = s_w[j];
+                        if (fast && w >= best) break;    // w + d^2 >= w >= best, here and later
+                        const double dd = __ddiv_rn(__dsub_rn(c0[s_off[j]], r), crit);
+                        best = nmin(best, __dadd_rn(w, __dmul_rn(dd, dd)));
+                    }
+                    g = __dsqrt_rn(best);
+                    if (!kFallback && P.want_gamma) gmap[v] = g;
+                }
+                if (P.want_mask) mmap[v] = masked ? 1 : 0;
+            }
+            if (masked) {
+                ++c_eval;
+                c_pass += g <= 1.0;
+                if (g != g) ++c_nan;
+                else { sum = __dadd_rn(sum, g); mx = g > mx ? g : mx; }
+            }
+            gk[k] = g;
+            bal[k] = __ballot_sync(0xffffffffu, masked);
+            wcnt += __popc(bal[k]);
         }
-        const unsigned int bal = __ballot_sync(0xffffffffu, masked);
-        if (bal) {
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(&st->cnt[pass][3], (unsigned long long)__popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (masked) keys[base + __popc(bal & ((1u << lane) - 1u))] = dkey(g);
+        // masked voxels' keys for the percentiles: one atomic per brick
+        if (lane == 0) s_wcnt[warp] = wcnt;
+        __syncthreads();
+        if (tid == 0) {
+            unsigned int tot = 0;
+            for (int w = 0; w < kGThreads / 32; ++w) { s_wpre[w] = tot; tot += s_wcnt[w]; }
+            s_base = tot ? atomicAdd(&st->cnt[pass][3], (unsigned long long)tot) : 0ull;
+        }
+        __syncthreads();
+        unsigned long long pos = s_base + s_wpre[warp];
+        const unsigned int below = (1u << lane) - 1u;
+#pragma unroll
+        for (int k = 0; k < kTZ; ++k) {
+            if (bal[k] & (1u << lane)) keys[pos + __popc(bal[k] & below)] = dkey(gk[k]);
+            pos += __popc(bal[k]);
         }
     }
     // block reduction in a fixed order
@@ -217,7 +287,6 @@ gamma_kernel(const GammaParams P, const T* __restrict__ ref, const T* __restrict
         c_pass += __shfl_xor_sync(0xffffffffu, c_pass, o);
         c_nan += __shfl_xor_sync(0xffffffffu, c_nan, o);
     }
-    const int warp = tid >> 5;
     if (lane == 0) {
         red_s[warp] = sum; red_m[warp] = mx;
         red_c[warp][0] = c_eval; red_c[warp][1] = c_pass; red_c[warp][2] = c_nan;
@@ -231,9 +300,8 @@ gamma_kernel(const GammaParams P, const T* __restrict__ ref, const T* __restrict
             m = red_m[w] > m ? red_m[w] : m;
             a += red_c[w][0]; b += red_c[w][1]; c += red_c[w][2];
         }
-        const size_t bid = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        part_sum[bid] = s;
-        part_max[bid] = m;
+        part_sum[blockIdx.x] = s;
+        part_max[blockIdx.x] = m;
         if (a) atomicAdd(&st->cnt[pass][0], a);
         if (b) atomicAdd(&st->cnt[pass][1], b);
         if (c) atomicAdd(&st->cnt[pass][2], c);
@@ -243,10 +311,11 @@ gamma_kernel(const GammaParams P, const T* __restrict__ ref, const T* __restrict
 // Statistics of the chosen mask and the ranks of the order statistics (one block).
 __global__ void __launch_bounds__(kFinThreads)
 gamma_finish_kernel(const GammaParams P, GammaState* st, const double* __restrict__ part_sum,
-                    const double* __restrict__ part_max, int n_blocks) {
+                    const double* __restrict__ part_max, int grid0, int grid1) {
     __shared__ double s_sum[kFinThreads / 32], s_max[kFinThreads / 32];
     if (st->status != 0) return;
     const int pass = st->cnt[0][0] != 0ull ? 0 : 1;
+    const int n_blocks = pass ? grid1 : grid0;
     double s = 0.0, m = -1.0;
     // fixed order: thread t sums blocks t, t + T, ... then the warps, then the block
     for (int b = threadIdx.x; b < n_blocks; b += kFinThreads) {
@@ -290,67 +359,141 @@ gamma_finish_kernel(const GammaParams P, GammaState* st, const double* __restric
     for (int j = 0; j < 4; ++j) { st->prefix[j] = 0ull; st->rem[j] = st->rank[j]; }
 }
 
-// One radix-select pass: histogram of key bits [shift, top) of the keys whose bits above
-// `top` equal each target's prefix (digits of 11 bits from the top, the last one 9 bits).
+// One radix-select pass over key bits [shift, top) (digits of 11 bits from the top, the last
+// one 9 bits).  The blocks histogram the keys whose bits above `top` equal a target's prefix
+// (targets with equal prefixes share a histogram; runs of equal digits are counted in
+// registers before one shared-memory atomic), add their histograms to the global one, and
+// the last block to arrive picks each target's digit from the totals, updates its prefix and
+// remaining rank, and clears the histogram and the arrival counter for the next pass.
+// mode 0 reads every masked key; mode 1 also copies the keys that match any target's
+// prefix into a candidate list; mode 2 reads only the candidates.  The grid is trimmed to
+// about kSelPer keys per thread.
 __global__ void __launch_bounds__(kHistThreads)
-gamma_hist_kernel(const GammaState* st, const unsigned long long* __restrict__ keys, int shift,
-                  int top, unsigned int* __restrict__ hist) {
+gamma_select_kernel(GammaState* st, const unsigned long long* __restrict__ keys,
+                    unsigned long long* __restrict__ cand, int shift, int top, int mode,
+                    unsigned int* __restrict__ hist) {
     __shared__ unsigned int h[4][kBins];
+    __shared__ int s_last;
     if (st->status != 0) return;
-    for (int i = threadIdx.x; i < 4 * kBins; i += kHistThreads) (&h[0][0])[i] = 0u;
-    __syncthreads();
-    const unsigned long long n = st->n_eval;
+    const unsigned long long n = mode == 2 ? st->n_cand : st->n_eval;
+    const unsigned long long* src = mode == 2 ? cand : keys;
+    const unsigned long long want = (n + (unsigned long long)kHistThreads * kSelPer - 1) /
+                                    ((unsigned long long)kHistThreads * kSelPer);
+    const unsigned int active = (unsigned int)(want < gridDim.x ? (want ? want : 1) : gridDim.x);
+    if (blockIdx.x >= active) return;
     const unsigned long long himask = top >= 64 ? 0ull : ~((1ull << top) - 1ull);
     const unsigned int dmask = (1u << (top - shift)) - 1u;
     unsigned long long pre[4];
+    int grp[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) pre[j] = st->prefix[j];
-    for (unsigned long long i = (unsigned long long)blockIdx.x * kHistThreads + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * kHistThreads) {
-        const unsigned long long k = __ldg(keys + i);
-        const unsigned int d = (unsigned int)(k >> shift) & dmask;
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if ((k & himask) == pre[j]) atomicAdd(&h[j][d], 1u);
+    for (int j = 0; j < 4; ++j) {
+        pre[j] = st->prefix[j];
+        grp[j] = j;
+        for (int q = 0; q < j; ++q)
+            if (grp[j] == j && pre[q] == pre[j]) grp[j] = grp[q];
     }
+    for (int j = 0; j < 4; ++j)
+        if (grp[j] == j)
+            for (int i = threadIdx.x; i < kBins; i += kHistThreads) h[j][i] = 0u;
     __syncthreads();
-    for (int i = threadIdx.x; i < 4 * kBins; i += kHistThreads) {
-        const unsigned int c = (&h[0][0])[i];
-        if (c) atomicAdd(hist + i, c);
-    }
-}
-
-// Pick each target's digit from its histogram (one warp per target), then clear the histogram.
-__global__ void __launch_bounds__(128)
-gamma_scan_kernel(GammaState* st, int shift, unsigned int* __restrict__ hist) {
-    if (st->status != 0) return;
-    const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned int* hj = hist + j * kBins;
-    constexpr int per = kBins / 32;
-    unsigned long long loc = 0;
-    for (int i = 0; i < per; ++i) loc += hj[lane * per + i];
-    unsigned long long inc = loc;
+    const int lane = threadIdx.x & 31;
+    unsigned int rd[4] = {0u, 0u, 0u, 0u}, rc[4] = {0u, 0u, 0u, 0u};
+    const unsigned long long stride = (unsigned long long)active * kHistThreads;
+    // warp-uniform trip count (the candidate append is warp-collective); four keys per
+    // thread loaded before they are counted
+    for (unsigned long long b0 = (unsigned long long)blockIdx.x * kHistThreads + (threadIdx.x & ~31);
+         b0 < n; b0 += 4 * stride) {
+      unsigned long long kk[4];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
-    }
-    const unsigned long long rem = st->rem[j];
-    const unsigned int hit = __ballot_sync(0xffffffffu, inc > rem);
-    const int src = hit ? __ffs(hit) - 1 : 31;
-    if (lane == src) {
-        unsigned long long before = inc - loc;
-        int d = lane * per;
-        for (int i = 0; i < per; ++i) {
-            const unsigned int c = hj[lane * per + i];
-            if (before + c > rem) { d = lane * per + i; break; }
-            before += c;
+      for (int q = 0; q < 4; ++q) {
+        const unsigned long long i = b0 + q * stride + lane;
+        kk[q] = i < n ? __ldg(src + i) : 0ull;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const unsigned long long b = b0 + q * stride;
+        if (b >= n) break;                                   // warp-uniform
+        const bool valid = b + lane < n;
+        const unsigned long long k = kk[q];
+        const unsigned int d = (unsigned int)(k >> shift) & dmask;
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (grp[j] != j || !valid || (k & himask) != pre[j]) continue;
+            any = true;
+            if (rc[j] && rd[j] == d) { ++rc[j]; continue; }
+            if (rc[j]) atomicAdd(&h[j][rd[j]], rc[j]);
+            rd[j] = d;
+            rc[j] = 1u;
         }
-        st->rem[j] = rem - before;
-        st->prefix[j] |= (unsigned long long)d << shift;
+        if (mode == 1) {
+            const unsigned int bal = __ballot_sync(0xffffffffu, any);
+            if (bal) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(&st->n_cand, (unsigned long long)__popc(bal));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (any) cand[base + __popc(bal & ((1u << lane) - 1u))] = k;
+            }
+        }
+      }
     }
-    __syncwarp();
-    for (int i = lane; i < kBins; i += 32) hj[i] = 0u;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (rc[j]) atomicAdd(&h[j][rd[j]], rc[j]);
+    __syncthreads();
+    for (int j = 0; j < 4; ++j)
+        if (grp[j] == j)
+            for (int i = threadIdx.x; i < kBins; i += kHistThreads) {
+                const unsigned int c = h[j][i];
+                if (c) atomicAdd(hist + j * kBins + i, c);
+            }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&st->sel_arrive, 1u) == active - 1u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int j = 0; j < 4; ++j)
+        if (grp[j] == j) {
+            unsigned int c[kBins / kHistThreads];
+#pragma unroll
+            for (int q = 0; q < kBins / kHistThreads; ++q)
+                c[q] = __ldcg(hist + j * kBins + threadIdx.x + q * kHistThreads);
+#pragma unroll
+            for (int q = 0; q < kBins / kHistThreads; ++q) {
+                h[j][threadIdx.x + q * kHistThreads] = c[q];
+                hist[j * kBins + threadIdx.x + q * kHistThreads] = 0u;
+            }
+        }
+    __syncthreads();
+    const int j = threadIdx.x >> 5;
+    if (j < 4) {
+        const unsigned int* hj = h[grp[j]];
+        constexpr int per = kBins / 32;
+        unsigned long long loc = 0;
+        for (int q = 0; q < per; ++q) loc += hj[lane * per + q];
+        unsigned long long inc = loc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const unsigned long long rem = st->rem[j];
+        const unsigned int hit = __ballot_sync(0xffffffffu, inc > rem);
+        const int srcl = hit ? __ffs(hit) - 1 : 31;
+        if (lane == srcl) {
+            unsigned long long before = inc - loc;
+            int dsel = lane * per + per - 1;
+            for (int q = 0; q < per; ++q) {
+                const unsigned int c = hj[lane * per + q];
+                if (before + c > rem) { dsel = lane * per + q; break; }
+                before += c;
+            }
+            st->rem[j] = rem - before;
+            st->prefix[j] |= (unsigned long long)dsel << shift;
+        }
+    }
+    if (threadIdx.x == 0) st->sel_arrive = 0u;
 }
 
 // NumPy's _lerp between the order statistics; statistics out.
@@ -461,6 +604,7 @@ int validate(const pbd_gamma_spec* s, int nz, int ny, int nx) {
 struct GammaWs {
     GammaState* st;
     unsigned long long* keys;
+    unsigned long long* cand;
     double* psum;
     double* pmax;
     unsigned int* hist;
@@ -477,6 +621,7 @@ int carve(void* base, int nz, int ny, int nx, GammaWs& w, size_t* bytes) {
     w.psum = c.take<double>(w.n_blocks);
     w.pmax = c.take<double>(w.n_blocks);
     w.keys = c.take<unsigned long long>(n);
+    w.cand = c.take<unsigned long long>(n);
     *bytes = c.used;
     return PBD_OK;
 }
@@ -497,7 +642,8 @@ int launch_gamma(const GammaParams& P, const T* ref, const T* ev, double* gmap,
         ++launches;
     }
     const size_t smem = (size_t)(kTX + 2 * P.hx) * (kTY + 2 * P.hy) * (kTZ + 2 * P.hz) *
-                        sizeof(double);
+                            sizeof(double) +
+                        (size_t)P.n_off * (sizeof(double) + sizeof(int));
     static bool attr_set = false;               // one per input type
     if (!attr_set) {
         PBD_TRY(cuda_rc(cudaFuncSetAttribute(gamma_kernel<T, false>,
@@ -508,27 +654,33 @@ int launch_gamma(const GammaParams& P, const T* ref, const T* ev, double* gmap,
                                              kGMaxSmem)));
         attr_set = true;
     }
-    const dim3 grid((P.nx + kTX - 1) / kTX, (P.ny + kTY - 1) / kTY, (P.nz + kTZ - 1) / kTZ);
-    gamma_kernel<T, false><<<grid, kGThreads, smem, s>>>(P, ref, ev, gmap, mmap, w.st, w.keys,
-                                                         w.psum, w.pmax);
+    const int gx = (P.nx + kTX - 1) / kTX, gy = (P.ny + kTY - 1) / kTY;
+    const int n_bricks = w.n_blocks;
+    int occ = 0;
+    PBD_TRY(cuda_rc(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gamma_kernel<T, false>,
+                                                                  kGThreads, smem)));
+    const int grid0 = std::max(1, std::min(n_bricks, std::max(occ, 1) * num_sms()));
+    const int grid1 = std::max(1, std::min(n_bricks, num_sms()));   // fallback: usually idle
+    gamma_kernel<T, false><<<grid0, kGThreads, smem, s>>>(P, ref, ev, gmap, mmap, w.st, w.keys,
+                                                          w.psum, w.pmax, gx, gy, n_bricks);
     PBD_LAUNCH_CHECK();
-    gamma_kernel<T, true><<<grid, kGThreads, smem, s>>>(P, ref, ev, gmap, mmap, w.st, w.keys,
-                                                        w.psum, w.pmax);
+    gamma_kernel<T, true><<<grid1, kGThreads, smem, s>>>(P, ref, ev, gmap, mmap, w.st, w.keys,
+                                                         w.psum, w.pmax, gx, gy, n_bricks);
     PBD_LAUNCH_CHECK();
-    gamma_finish_kernel<<<1, kFinThreads, 0, s>>>(P, w.st, w.psum, w.pmax, w.n_blocks);
+    gamma_finish_kernel<<<1, kFinThreads, 0, s>>>(P, w.st, w.psum, w.pmax, grid0, grid1);
     PBD_LAUNCH_CHECK();
     const int hblocks = num_sms() * 2;
     for (int p = 0; p < kSelPasses; ++p) {
         const int top = 64 - kDigitBits * p;                       // 64, 53, 42, 31, 20, 9
         const int shift = top > kDigitBits ? top - kDigitBits : 0;
-        gamma_hist_kernel<<<hblocks, kHistThreads, 0, s>>>(w.st, w.keys, shift, top, w.hist);
-        PBD_LAUNCH_CHECK();
-        gamma_scan_kernel<<<1, 128, 0, s>>>(w.st, shift, w.hist);
+        const int mode = p < 2 ? 0 : (p == 2 ? 1 : 2);
+        gamma_select_kernel<<<hblocks, kHistThreads, 0, s>>>(w.st, w.keys, w.cand, shift, top,
+                                                             mode, w.hist);
         PBD_LAUNCH_CHECK();
     }
     gamma_final_kernel<<<1, 1, 0, s>>>(P, w.st, out, n_offsets);
     PBD_LAUNCH_CHECK();
-    count_launch(launches + 4 + 2 * kSelPasses);
+    count_launch(launches + 4 + kSelPasses);
     return PBD_OK;
 }
 
@@ -587,10 +739,14 @@ int pbd_gamma_index(const pbd_gamma_spec* spec, int nz, int ny, int nx, const vo
     P.thr_frac = spec->threshold_pct / 100.0;                      // gamma.py:126
     P.q[0] = 95.0 / 100.0;
     P.q[1] = 99.0 / 100.0;
+    int o = 0;
     for (int i = 0; i < t.n_entries; ++i) {
         P.w[i] = t.w[i];
         for (int a = 0; a < 3; ++a) P.abc[i][a] = t.abc[i][a];
+        P.start[i] = (short)o;
+        o += (t.abc[i][0] ? 2 : 1) * (t.abc[i][1] ? 2 : 1) * (t.abc[i][2] ? 2 : 1);
     }
+    P.n_off = o;
     cudaStream_t s = (cudaStream_t)stream;
     if (dtype == PBD_DTYPE_F32)
         return launch_gamma<float>(P, (const float*)reference, (const float*)evaluation,
