@@ -267,24 +267,74 @@ __global__ void layer_setup_kernel(pbd_lut_spec spec, LutDims dm, const double* 
     }
 }
 
-// Range-straggling convolution (see the file comment).
-__global__ void conv_kernel(LutDims dm, const LayerScal* scal, const double* binned,
-                            const double* ker, double* smooth) {
+// Range-straggling convolution (see the file comment): smooth[i] = sum_m bin[m] kr[|i - m|]
+// over |i - m| <= K, bins outside [0, n) being zero, each output summed in ascending m with
+// FMA.  A thread owns kConvB consecutive outputs i0 .. i0 + B - 1 and walks the steps
+// s = m - i0 + K = 0 .. 2K + B - 1: at each step one bin (shared by its B outputs) and one
+// kernel value kr[|K - s|] (the same for every thread of the block) are read from shared
+// memory, and the kernel value is kept in a ring of B registers whose slot is the step
+// modulo B -- output b needs the value loaded b steps earlier -- so the unrolled body needs
+// no register moves.  Steps run in chunks of kConvChunk whose bins and kernel values are
+// staged in shared memory; B is odd so that the threads' strided bin reads do not collide
+// in the banks.
+constexpr int kConvB = 9;
+constexpr int kConvThreads = 128;
+constexpr int kConvSeg = kConvB * kConvThreads;          // outputs per block
+constexpr int kConvChunk = 112 * kConvB;                 // steps per staged chunk
+constexpr int kConvSmem = (kConvSeg + kConvChunk + kConvChunk) * (int)sizeof(double);
+
+__global__ void __launch_bounds__(kConvThreads)
+conv_kernel(LutDims dm, const LayerScal* scal, const double* binned, const double* ker,
+            double* smooth) {
+    extern __shared__ double csm[];
+    double* sbin = csm;                                   // kConvSeg + kConvChunk bins
+    double* skw = csm + kConvSeg + kConvChunk;            // kConvChunk kernel values
     const int lv = blockIdx.x;
     const int n = dm.n_idd;
-    const int i = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int s0 = blockIdx.y * kConvSeg;
     const double* bin = binned + (size_t)lv * n;
+    double* out = smooth + (size_t)lv * n;
     const LayerScal sc = scal[lv];
     if (sc.sig_r <= 0.0) {
-        smooth[(size_t)lv * n + i] = bin[i];
+        for (int i = s0 + threadIdx.x; i < min(n, s0 + kConvSeg); i += kConvThreads)
+            out[i] = bin[i];
         return;
     }
     const double* kr = ker + (size_t)lv * n;
-    const int lo = max(0, i - sc.conv_k), hi = min(n - 1, i + sc.conv_k);
-    double acc = 0.0;
-    for (int m = lo; m <= hi; ++m) acc += bin[m] * kr[abs(i - m)];
-    smooth[(size_t)lv * n + i] = acc;
+    const int K = sc.conv_k;
+    const int n_steps = 2 * K + kConvB;
+    const int i0 = s0 + threadIdx.x * kConvB;             // this thread's first output
+    double acc[kConvB], ring[kConvB];
+#pragma unroll
+    for (int b = 0; b < kConvB; ++b) { acc[b] = 0.0; ring[b] = 0.0; }
+    for (int c0 = 0; c0 < n_steps; c0 += kConvChunk) {
+        // bins m = s0 - K + c0 + j, j < kConvSeg + kConvChunk; kernel kr[|K - c0 - j|], j < chunk
+        __syncthreads();
+        for (int j = threadIdx.x; j < kConvSeg + kConvChunk; j += kConvThreads) {
+            const int m = s0 - K + c0 + j;
+            sbin[j] = (m >= 0 && m < n) ? bin[m] : 0.0;
+        }
+        for (int j = threadIdx.x; j < kConvChunk; j += kConvThreads) {
+            const int t = K - c0 - j;
+            const int a = t < 0 ? -t : t;
+            skw[j] = a <= K ? kr[a] : 0.0;
+        }
+        __syncthreads();
+        const double* sb = sbin + threadIdx.x * kConvB;   // bin of step c0 + j is sb[j]
+        for (int j = 0; j < kConvChunk; j += kConvB) {
+#pragma unroll
+            for (int q = 0; q < kConvB; ++q) {
+                ring[q] = skw[j + q];                     // kr[|K - s|], s = c0 + j + q
+                const double bv = sb[j + q];
+#pragma unroll
+                for (int b = 0; b < kConvB; ++b)
+                    acc[b] = __fma_rn(bv, ring[(q - b + kConvB) % kConvB], acc[b]);
+            }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kConvB; ++b)
+        if (i0 + b < n) out[i0 + b] = acc[b];
 }
 
 // Fermi-Eyges direct scattering integral B(zf_i) = sum_{j<i} (zf_i - zf_j)^2 T_j h_j,
@@ -404,6 +454,28 @@ int validate_spec(const pbd_lut_spec* s, int n_layers) {
     return PBD_OK;
 }
 
+// The range table is a constant of the physics: the first call on a device builds it and
+// waits for it (once per process and device), so that later calls on any stream find it
+// ready.  Inside a stream capture the build is recorded into the graph instead and the
+// device is not marked.
+bool g_range_built[64];
+
+int ensure_range_table(cudaStream_t st) {
+    int dev = 0;
+    PBD_TRY(cuda_rc(cudaGetDevice(&dev)));
+    if (dev >= 0 && dev < 64 && g_range_built[dev]) return PBD_OK;
+    range_table_kernel<<<1, 1024, 0, st>>>();
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PBD_TRY(cuda_rc(cudaStreamIsCapturing(st, &cs)));
+    if (cs == cudaStreamCaptureStatusNone && dev >= 0 && dev < 64) {
+        PBD_TRY(cuda_rc(cudaStreamSynchronize(st)));
+        g_range_built[dev] = true;
+    }
+    return PBD_OK;
+}
+
 struct LutWs {
     LayerScal* scal;
     double *binned, *ker, *smooth, *t_fe, *b_fe, *zf_fe, *hf_fe;
@@ -458,15 +530,14 @@ int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const
     carve_lut(c, w, n_layers, dm.nvar, dm.n_idd, dm.n_fe);
     const int lvn = n_layers * dm.nvar;
 
-    range_table_kernel<<<1, 1024, 0, st>>>();
-    PBD_LAUNCH_CHECK();
+    PBD_TRY(ensure_range_table(st));
     fe_grid_kernel<<<(dm.n_fe + 255) / 256, 256, 0, st>>>(dm, w.zf_fe, w.hf_fe);
     PBD_LAUNCH_CHECK();
     layer_setup_kernel<<<lvn, 256, 0, st>>>(*s, dm, energies, shift, w.scal, w.binned, w.ker,
                                             w.t_fe);
     PBD_LAUNCH_CHECK();
-    conv_kernel<<<dim3(lvn, (dm.n_idd + 127) / 128), 128, 0, st>>>(dm, w.scal, w.binned, w.ker,
-                                                                   w.smooth);
+    conv_kernel<<<dim3(lvn, (dm.n_idd + kConvSeg - 1) / kConvSeg), kConvThreads, kConvSmem, st>>>(
+        dm, w.scal, w.binned, w.ker, w.smooth);
     PBD_LAUNCH_CHECK();
     fe_b_kernel<<<dim3(lvn, (dm.n_fe + 127) / 128), 128, 0, st>>>(dm, w.zf_fe, w.hf_fe, w.t_fe,
                                                                   w.b_fe);
@@ -474,19 +545,18 @@ int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const
     lut_output_kernel<<<n_layers, 128, 0, st>>>(*s, dm, w.scal, w.smooth, w.zf_fe, w.b_fe,
                                                  fl.single_depth, idd, sigma, didd, dsig);
     PBD_LAUNCH_CHECK();
-    count_launch(6);
+    count_launch(5);
     return PBD_OK;
 }
 
 int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st) {
     if (!e || !r) return PBD_ERR_NULL_ARG;
     if (n < 0) return PBD_ERR_BAD_DIM;
-    range_table_kernel<<<1, 1024, 0, st>>>();
-    PBD_LAUNCH_CHECK();
+    PBD_TRY(ensure_range_table(st));
     if (n == 0) return PBD_OK;
     csda_kernel<<<(n + 255) / 256, 256, 0, st>>>(e, r, n, inverse);
     PBD_LAUNCH_CHECK();
-    count_launch(2);
+    count_launch(1);
     return PBD_OK;
 }
 
