@@ -261,7 +261,8 @@ def robust_bench(args):
     Three legs, each timed with L2 flushed between steps: a loop of one plain FP32
     ``pbd_forward`` per job (the per-scenario baseline), the batched forward of every job
     in one persistent launch replayed from a CUDA graph, and the loss gradient of every
-    job (``pbd_loss_grad`` per job) replayed from a CUDA graph."""
+    job (``pbd_loss_grad_batch``: one forward and one adjoint launch for all jobs) replayed
+    from a CUDA graph."""
     import torch
     pb = importlib.import_module("gpu-proton-dose-engine_b200")
     dev = torch.device("cuda", 0)
@@ -317,7 +318,7 @@ def robust_bench(args):
                        "layers) x 25 scenarios, 128^3 voxels of 2 mm", "jobs": n,
                        "precision": prec, "l2": "flushed between steps"},
             "legs_ms": {"fp32_loop_per_job_forward": t_loop, "batched_forward_graph": t_batch,
-                        "per_job_loss_grad_graph": t_grad},
+                        "batched_loss_grad_graph": t_grad},
             "speedup_batched_vs_fp32_loop": t_loop / t_batch,
             "grad_evals_per_s": n * 1e3 / t_grad,
             "gpu_launches_per_replay": {"batched_forward": per_batch, "loss_grad": per_grad},

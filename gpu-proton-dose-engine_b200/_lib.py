@@ -57,6 +57,13 @@ class AdamParams(ctypes.Structure):
                 ("grad_scale", ctypes.c_float)]
 
 
+class GradJob(ctypes.Structure):
+    _fields_ = [("field", Field), ("w", c_void_p), ("idd", c_void_p), ("sigma", c_void_p),
+                ("didd_dr", c_void_p), ("dsigma_dr", c_void_p), ("mask", c_void_p),
+                ("presc", c_void_p), ("dose", c_void_p), ("grad_dose", c_void_p),
+                ("loss", c_void_p), ("grad_w", c_void_p), ("grad_range", c_void_p)]
+
+
 OBJ = {"mean": 0, "max": 1}
 
 
@@ -105,6 +112,8 @@ _SIGS = {
                                     c_void_p]),
     "pbd_forward_batch_workspace": (c_int, [POINTER(Job), c_int, c_int, POINTER(c_size_t)]),
     "pbd_forward_batch": (c_int, [POINTER(Job), c_int, c_int, c_void_p, c_size_t, c_void_p]),
+    "pbd_loss_grad_batch_workspace": (c_int, [POINTER(GradJob), c_int, c_int, POINTER(c_size_t)]),
+    "pbd_loss_grad_batch": (c_int, [POINTER(GradJob), c_int, c_int, c_void_p, c_size_t, c_void_p]),
     "pbd_adam_step": (c_int, [POINTER(AdamParams), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "pbd_scenario_combine": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -559,8 +559,9 @@ constexpr int kRedPer = 16;        // entries per thread: nsy * nsx <= 64 * 64 =
 
 __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     const JobDev* __restrict__ jobs, int with_range, int finalize_loss, const int* __restrict__ err,
-    int* layer_count) {
+    int* layer_counts, int layer_stride) {
     const JobDev& J = jobs[blockIdx.z];
+    int* layer_count = layer_counts + (size_t)blockIdx.z * layer_stride;   // this job's counters
     const int seg = blockIdx.x, l = blockIdx.y;
     if (l >= J.nl) return;
     const int nz = J.nz, nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;
@@ -740,6 +741,10 @@ int tc_adjoint_dims(int precision, const pbd_field* f, int* N1) {
     return PBD_OK;
 }
 
+size_t tc_adjoint_counter_ints(int n_jobs, int max_layers) {
+    return 2u + (size_t)n_jobs * (size_t)max_layers;
+}
+
 size_t tc_adjoint_slot_elems(const pbd_field* f) {
     const size_t per = (size_t)f->n_sy * f->n_sx;
     const size_t nseg = ((size_t)f->nz + kRedZ - 1) / kRedZ;
@@ -770,15 +775,14 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     const long long units = (long long)nzm * cm * n_jobs;
     if (units > (1LL << 30)) return PBD_ERR_UNSUPPORTED;
     P.n_units = (int)units;
-    if (n_jobs != 1) return PBD_ERR_UNSUPPORTED;   // per-layer arrival counters of one job
-    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, (2 + (size_t)max_l) * sizeof(int), s)));
+    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, tc_adjoint_counter_ints(n_jobs, max_l) * sizeof(int), s)));
     int rc = PBD_OK;
     if (precision == PBD_PREC_BF16) rc = launch_mode<PBD_PREC_BF16>(P, s);
     else rc = launch_mode<PBD_PREC_BF16X3>(P, s);
     PBD_TRY(rc);
     (void)max_per;
     adj_tc_reduce_kernel<<<dim3((nzm + kRedZ - 1) / kRedZ, max_l, n_jobs), kRedThreads, 0, s>>>(
-        jobs_dev, with_range, finalize_loss, counter + 1, counter + 2);
+        jobs_dev, with_range, finalize_loss, counter + 1, counter + 2, max_l);
     PBD_LAUNCH_CHECK();
     count_launch(2);
     return PBD_OK;

@@ -66,6 +66,65 @@ __global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_bas
     dst[k] = J;
 }
 
+// Batched loss gradient: per-job descriptors installed in groups of kGradInstall (kernel
+// parameter size) into the forward and adjoint views.
+struct GradLite {
+    int nx, ny, nz, nsx, nsy, nl;
+    int max_chunks_f, max_chunks_a, direct, n_loss_part;
+    double ox, oy, dx, dy, sx0, sy0, dsx, dsy;
+    const float* w;
+    const double *idd, *sigma, *didd, *dsig;
+    const float *mask, *presc;
+    float *dose, *grad_dose;
+    double* loss;
+    float *grad_w, *grad_range;
+    size_t fpart_off, arrive_off, loss_off, slot_off, dcs_off;
+};
+constexpr int kGradInstall = 64;
+struct GradTable {
+    int n, base;
+    GradLite j[kGradInstall];
+};
+static_assert(sizeof(GradTable) < 32000, "kernel parameter limit");
+
+struct GradBufs {
+    JobDev *fwd, *adj;
+    float* fpart;
+    int* farr;
+    double* lpart;
+    float *apart, *dcs, *dsgs;
+    const int* fwd_err;
+};
+
+__global__ void install_grad_kernel(GradTable t, GradBufs b) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= t.n) return;
+    const GradLite& a = t.j[k];
+    JobDev J;
+    memset(&J, 0, sizeof(J));
+    J.nx = a.nx; J.ny = a.ny; J.nz = a.nz; J.nsx = a.nsx; J.nsy = a.nsy; J.nl = a.nl;
+    J.ntx = (a.nx + kTile - 1) / kTile;
+    J.nty = (a.ny + kTile - 1) / kTile;
+    J.ox = a.ox; J.oy = a.oy; J.dx = a.dx; J.dy = a.dy;
+    J.sx0 = a.sx0; J.sy0 = a.sy0; J.dsx = a.dsx; J.dsy = a.dsy;
+    J.w = a.w; J.idd = a.idd; J.sigma = a.sigma; J.didd_dr = a.didd; J.dsig_dr = a.dsig;
+    J.dose = a.dose; J.mask = a.mask; J.presc = a.presc; J.grad_dose = a.grad_dose;
+    J.loss = a.loss; J.grad_w = a.grad_w; J.grad_range = a.grad_range;
+    J.n_loss_part = a.n_loss_part;
+    J.loss_part = b.lpart + a.loss_off;
+    JobDev F = J, A = J;
+    F.max_chunks = a.max_chunks_f;
+    F.partial = a.direct ? a.dose : b.fpart + a.fpart_off;
+    F.arrive = b.farr + a.arrive_off;
+    A.max_chunks = a.max_chunks_a;
+    A.partial = b.apart + a.slot_off;
+    A.dc = b.dcs + a.dcs_off;
+    A.dsg = b.dsgs + a.dcs_off;
+    A.fwd_err = b.fwd_err;
+    b.fwd[t.base + k] = F;
+    b.adj[t.base + k] = A;
+}
+
 int g_sms[64] = {0};
 std::mutex g_sms_mu;
 
@@ -160,7 +219,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
             w.adj_tc = 1;
             w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : 8;
             pe = tc_adjoint_slot_elems(f);
-            w.acnt = c.take<int>(2 + (size_t)f->n_layers);
+            w.acnt = c.take<int>(tc_adjoint_counter_ints(1, f->n_layers));
         } else {
             PBD_TRY(adj_plan_sizes(f, w.a_chunk, &pe, &w.a_items));
             w.aitems = c.take<AdjItem>(w.a_items);
@@ -469,6 +528,75 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     return run_adjoint(ws, precision, &A, with_range, 1, s);
 }
 
+// ---- batched loss gradient ------------------------------------------------------------
+constexpr int kBatchAdjChunk = 8;   // layers per tensor-core adjoint unit (the single-job default)
+
+struct GradPlan {
+    int chunk, direct, with_range, max_l;
+    size_t arr, fpart, lpart, apart, dcs;
+};
+
+static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, GradPlan* gp) {
+    if (!jobs) return PBD_ERR_NULL_ARG;
+    if (n_jobs <= 0) return PBD_ERR_BAD_DIM;
+    if (n_jobs > PBD_MAX_JOBS) return PBD_ERR_TOO_MANY;
+    PBD_TRY(check_precision(precision));
+    if (precision == PBD_PREC_FP32) return PBD_ERR_UNSUPPORTED;
+    int max_l = 0, chunk = kMaxChunkCost;
+    gp->with_range = jobs[0].grad_range != nullptr;
+    for (int k = 0; k < n_jobs; ++k) {
+        const pbd_field* f = &jobs[k].field;
+        PBD_TRY(host_validate_field(f));
+        PBD_TRY(check_field_precision(f, precision));
+        PBD_TRY(adjoint_supported(f));
+        int n1 = 0;
+        PBD_TRY(tc_adjoint_dims(precision, f, &n1));
+        if ((jobs[k].grad_range != nullptr) != (gp->with_range != 0)) return PBD_ERR_BAD_VALUE;
+        max_l = max_l > f->n_layers ? max_l : f->n_layers;
+        const int ch = choose_fwd_chunk(f, precision);
+        chunk = ch < chunk ? ch : chunk;
+    }
+    gp->max_l = max_l;
+    gp->direct = (max_l <= kMaxChunkCost && g_fwd_chunk == 0) ? 1 : 0;
+    gp->chunk = gp->direct ? max_l : chunk;
+    gp->arr = gp->fpart = gp->lpart = gp->apart = gp->dcs = 0;
+    for (int k = 0; k < n_jobs; ++k) {
+        const pbd_field& f = jobs[k].field;
+        const size_t tiles = (size_t)((f.nx + kTile - 1) / kTile) * ((f.ny + kTile - 1) / kTile);
+        size_t pe = 0;
+        int it = 0;
+        PBD_TRY(fwd_plan_sizes(&f, gp->chunk, &pe, &it));
+        gp->arr += (size_t)f.nz * tiles * kTcFwdWarps;
+        gp->fpart += gp->direct ? 0 : pe;
+        gp->lpart += (size_t)f.nz * tiles * kTcFwdWarps;
+        gp->apart += tc_adjoint_slot_elems(&f);
+        gp->dcs += (size_t)f.n_layers * f.nz;
+    }
+    return PBD_OK;
+}
+
+struct GradCarve {
+    JobDev *fwd, *adj;
+    int *fcnt, *acnt;
+    float* fpart;
+    double* lpart;
+    float *apart, *dcs, *dsgs;
+};
+
+static size_t carve_grad(void* base, int n_jobs, const GradPlan& gp, GradCarve& g) {
+    Carve c(base);
+    g.fwd = c.take<JobDev>(n_jobs);
+    g.adj = c.take<JobDev>(n_jobs);
+    g.fcnt = c.take<int>(2 + gp.arr);
+    g.acnt = c.take<int>(tc_adjoint_counter_ints(n_jobs, gp.max_l));
+    g.fpart = c.take<float>(gp.fpart);
+    g.lpart = c.take<double>(gp.lpart);
+    g.apart = c.take<float>(gp.apart);
+    g.dcs = c.take<float>(gp.dcs);
+    g.dsgs = c.take<float>(gp.dcs);
+    return c.used + 256;
+}
+
 // Planning of a batched launch (host).  When every job has at most kMaxChunkCost layers,
 // one work item covers all layers of a (job, slice, tile) and writes the output slice
 // directly ("direct" mode: no partial sums, no partial buffer; the many jobs keep the
@@ -578,6 +706,83 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     count_launch(1);
     return launch_forward(jd, host_view, n_jobs, items, item_base, counter, 2 + arr_off, bp.chunk,
                           0, precision, 1, s);
+}
+
+int pbd_loss_grad_batch_workspace(const pbd_grad_job* jobs, int n_jobs, int precision,
+                                  size_t* bytes) {
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    GradPlan gp;
+    PBD_TRY(plan_grad_batch(jobs, n_jobs, precision, &gp));
+    GradCarve g;
+    *bytes = carve_grad(nullptr, n_jobs, gp, g);
+    return PBD_OK;
+}
+
+int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+    GradPlan gp;
+    PBD_TRY(plan_grad_batch(jobs, n_jobs, precision, &gp));
+    for (int k = 0; k < n_jobs; ++k) {
+        const pbd_grad_job& j = jobs[k];
+        if (!j.w || !j.idd || !j.sigma || !j.mask || !j.presc || !j.dose || !j.grad_dose ||
+            !j.loss || !j.grad_w)
+            return PBD_ERR_NULL_ARG;
+        if (gp.with_range && (!j.didd_dr || !j.dsigma_dr)) return PBD_ERR_NULL_ARG;
+    }
+    GradCarve g;
+    const size_t need = carve_grad(nullptr, n_jobs, gp, g);
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    carve_grad(workspace, n_jobs, gp, g);
+    cudaStream_t s = (cudaStream_t)stream;
+    GradBufs b{g.fwd, g.adj, g.fpart, g.fcnt + 2, g.lpart, g.apart, g.dcs, g.dsgs, g.fcnt + 1};
+    JobDev fview[PBD_MAX_JOBS], aview[PBD_MAX_JOBS];
+    size_t arr = 0, fpart = 0, lpart = 0, apart = 0, dcs = 0;
+    GradTable t;
+    for (int base = 0; base < n_jobs; base += kGradInstall) {
+        memset(&t, 0, sizeof(t));
+        t.base = base;
+        t.n = n_jobs - base < kGradInstall ? n_jobs - base : kGradInstall;
+        for (int q = 0; q < t.n; ++q) {
+            const int k = base + q;
+            const pbd_grad_job& j = jobs[k];
+            const pbd_field* f = &j.field;
+            const size_t tiles =
+                (size_t)((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile);
+            size_t pe = 0;
+            int it = 0;
+            PBD_TRY(fwd_plan_sizes(f, gp.chunk, &pe, &it));
+            GradLite& a = t.j[q];
+            a.nx = f->nx; a.ny = f->ny; a.nz = f->nz; a.nsx = f->n_sx; a.nsy = f->n_sy;
+            a.nl = f->n_layers;
+            a.max_chunks_f = gp.direct ? 1 : (f->n_layers + gp.chunk - 1) / gp.chunk;
+            a.max_chunks_a = (f->n_layers + kBatchAdjChunk - 1) / kBatchAdjChunk;
+            a.direct = gp.direct;
+            a.n_loss_part = (int)((size_t)f->nz * tiles * kTcFwdWarps);
+            a.ox = f->ox; a.oy = f->oy; a.dx = f->dx; a.dy = f->dy;
+            a.sx0 = f->x0; a.sy0 = f->y0; a.dsx = f->dx_spot; a.dsy = f->dy_spot;
+            a.w = j.w; a.idd = j.idd; a.sigma = j.sigma; a.didd = j.didd_dr; a.dsig = j.dsigma_dr;
+            a.mask = j.mask; a.presc = j.presc; a.dose = j.dose; a.grad_dose = j.grad_dose;
+            a.loss = j.loss; a.grad_w = j.grad_w; a.grad_range = j.grad_range;
+            a.fpart_off = fpart; a.arrive_off = arr; a.loss_off = lpart; a.slot_off = apart;
+            a.dcs_off = dcs;
+            fill_job(f, &fview[k]);
+            fview[k].max_chunks = a.max_chunks_f;
+            aview[k] = fview[k];
+            aview[k].max_chunks = a.max_chunks_a;
+            arr += (size_t)f->nz * tiles * kTcFwdWarps;
+            fpart += gp.direct ? 0 : pe;
+            lpart += (size_t)a.n_loss_part;
+            apart += tc_adjoint_slot_elems(f);
+            dcs += (size_t)f->n_layers * f->nz;
+        }
+        install_grad_kernel<<<(t.n + 63) / 64, 64, 0, s>>>(t, b);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    }
+    PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr, gp.chunk, 1,
+                           precision, 0, s));
+    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, kBatchAdjChunk,
+                             gp.with_range, 1, s);
 }
 
 }  // extern "C"

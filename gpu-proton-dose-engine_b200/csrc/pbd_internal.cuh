@@ -125,9 +125,12 @@ int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_job
 // adjoint (tcgen05) -- adj_tc.cu.  Units (slice, chunk of `chunk` active layers) are
 // pulled z-major; `partial` holds three (layer, slice) slot planes of nsy * nsx floats and
 // the reduction's segment partials (tc_adjoint_slot_elems); counter[0] = unit counter,
-// counter[1] = error word, counter[2 .. 2 + nl) = per-layer arrival counters (one job).
+// counter[1] = error word, then per job max_layers per-layer arrival counters.
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
 size_t tc_adjoint_slot_elems(const pbd_field* f);
+// Ints of the adjoint's counter block: unit counter, error word, then per job one arrival
+// counter per layer (max_layers of them).
+size_t tc_adjoint_counter_ints(int n_jobs, int max_layers);
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
                       int* counter, int chunk, int with_range, int finalize_loss, cudaStream_t s);
 

@@ -160,12 +160,19 @@ class ScenarioBatch:
         self.grad_outputs = outs
         return outs
 
-    def loss_grad_all(self, mask, presc):
-        """Forward, masked quadratic loss and adjoint of every (field, scenario) job, one
-        ``pbd_loss_grad`` call per job on the current stream with a shared workspace.
-        ``mask`` / ``presc``: one (nz, ny, nx) pair for all jobs (same grid)."""
+    def loss_grad_all(self, mask, presc, batched=None):
+        """Forward, masked quadratic loss and adjoint of every (field, scenario) job on the
+        current stream.  ``mask`` / ``presc``: one (nz, ny, nx) pair for all jobs (same grid).
+
+        ``batched`` (default: for the tensor-core precisions): every job's forward in one
+        persistent launch and every adjoint in another (``pbd_loss_grad_batch``); otherwise
+        one ``pbd_loss_grad`` call per job with a shared workspace."""
         if not getattr(self, "grad_outputs", None):
             self.alloc_grad_outputs()
+        if batched is None:
+            batched = self.precision != _lib.PREC["fp32"]
+        if batched:
+            return self._loss_grad_batched(mask, presc)
         need = max(_lib.query("pbd_loss_grad_workspace", ctypes.byref(self.jobs[k].field),
                               self.precision) for k in range(self.n_jobs))
         ws = self._ws("grad", need)
@@ -178,6 +185,29 @@ class ScenarioBatch:
                       _lib.ptr(t.didd_dr), _lib.ptr(t.dsigma_dr), _lib.ptr(mask), _lib.ptr(presc),
                       j.dose, _lib.ptr(o["grad_dose"]), _lib.ptr(o["loss"]), _lib.ptr(o["grad_w"]),
                       _lib.ptr(o["grad_range"]), self.precision, _lib.ptr(ws), ws.numel(), st)
+        return self.grad_outputs
+
+    def _loss_grad_batched(self, mask, presc):
+        key = (_lib.ptr(mask), _lib.ptr(presc))
+        if getattr(self, "_gjobs_key", None) != key:
+            gj = (_lib.GradJob * self.n_jobs)()
+            for k in range(self.n_jobs):
+                j, t, o = self.jobs[k], self.tables[k], self.grad_outputs[k]
+                if t.didd_dr is None:
+                    raise RuntimeError("build the batch with with_grad=True for gradients")
+                gj[k] = _lib.GradJob(field=j.field, w=j.w, idd=j.idd, sigma=j.sigma,
+                                     didd_dr=_lib.ptr(t.didd_dr), dsigma_dr=_lib.ptr(t.dsigma_dr),
+                                     mask=_lib.ptr(mask), presc=_lib.ptr(presc), dose=j.dose,
+                                     grad_dose=_lib.ptr(o["grad_dose"]), loss=_lib.ptr(o["loss"]),
+                                     grad_w=_lib.ptr(o["grad_w"]),
+                                     grad_range=_lib.ptr(o["grad_range"]))
+            self._gjobs, self._gjobs_key = gj, key
+            self._gjobs_refs = (mask, presc)
+        need = _lib.query("pbd_loss_grad_batch_workspace", self._gjobs, self.n_jobs,
+                          self.precision)
+        ws = self._ws("grad_batch", need)
+        _lib.call("pbd_loss_grad_batch", self._gjobs, self.n_jobs, self.precision, _lib.ptr(ws),
+                  ws.numel(), _lib.stream_handle(self.device))
         return self.grad_outputs
 
     def capture_loss_grad(self, mask, presc):

@@ -187,6 +187,26 @@ PBD_API int pbd_forward_batch_workspace(const pbd_job *jobs, int n_jobs, int pre
 PBD_API int pbd_forward_batch(const pbd_job *jobs, int n_jobs, int precision,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- batched loss gradient: several fields / scenarios in one forward and one adjoint ----
+ * No counterpart in the reference.  Each job has its own field, tables, loss arrays and
+ * outputs, with the meaning they have in pbd_loss_grad; all jobs' forwards (with the fused
+ * loss) run in one persistent launch and all adjoints in another.  Tensor-core precisions
+ * only (PBD_ERR_UNSUPPORTED for PBD_PREC_FP32); grad_range (with didd_dr, dsigma_dr) on every
+ * job or on none.  jobs: HOST array of n_jobs <= PBD_MAX_JOBS descriptors. */
+typedef struct pbd_grad_job {
+    pbd_field field;
+    const float *w;
+    const double *idd, *sigma, *didd_dr, *dsigma_dr;
+    const float *mask, *presc;
+    float *dose, *grad_dose;
+    double *loss;
+    float *grad_w, *grad_range;
+} pbd_grad_job;
+PBD_API int pbd_loss_grad_batch_workspace(const pbd_grad_job *jobs, int n_jobs, int precision,
+                                          size_t *bytes);
+PBD_API int pbd_loss_grad_batch(const pbd_grad_job *jobs, int n_jobs, int precision,
+                                void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- plan-optimisation steps (no counterpart in the reference) ---------------------
  * Device-resident state, so that an optimisation iteration (tables, loss gradient,
  * combination, update) can be captured into one CUDA graph and replayed. */

@@ -106,6 +106,55 @@ def test_batch_gradients_vs_oracle_and_graph_replay(pb):
             assert torch.equal(o0[key], o1[key]), key
 
 
+def test_batched_loss_grad_vs_per_job_and_oracle(pb):
+    """pbd_loss_grad_batch (all forwards in one launch, all adjoints in another) on two
+    fields x three scenarios -- the 70-layer field takes the chunked forward -- against the
+    per-job tensor-core calls and the float64 oracle; graph replay equals the eager call.
+    Tolerances: loss 1e-6 relative, grad_w / grad_range 1e-4 of max (split-BF16 adjoint)."""
+    import torch
+    fields = _fields(pb)
+    probs = [p for _, _, p in fields]
+    mask, presc = pb.workloads.target_loss_arrays(fields[0][0]["grid"], half=1.0, shell=1.0,
+                                                  depth=5.0)
+    m = torch.as_tensor(mask, device="cuda")
+    p = torch.as_tensor(presc * 100.0, device="cuda")
+    b = pb.robust.ScenarioBatch(probs, SCEN, precision="tf32x3", with_grad=True)
+    per = [{k: v.clone() for k, v in o.items()} for o in b.loss_grad_all(m, p, batched=False)]
+    outs = b.loss_grad_all(m, p, batched=True)
+    torch.cuda.synchronize()
+    bat = [{k: v.clone() for k, v in o.items()} for o in outs]
+    g = probs[0].grid
+    for k in range(b.n_jobs):
+        wl, en, prob = fields[k // len(SCEN)]
+        sx, sy, sz, sc = SCEN[k % len(SCEN)]
+        o, q = bat[k], per[k]
+        assert abs(float(o["loss"]) - float(q["loss"])) <= 1e-6 * abs(float(q["loss"])), k
+        assert rel(o["grad_w"].cpu().numpy(), q["grad_w"].cpu().numpy()) < 1e-4, k
+        assert rel(o["grad_range"].cpu().numpy(), q["grad_range"].cpu().numpy()) < 1e-4, k
+        t = b.tables[k]
+        wt = torch.tensor(wl["weights"].astype(np.float64), requires_grad=True)
+        it = torch.tensor(t.idd.cpu().numpy(), requires_grad=True)
+        st = torch.tensor(t.sigma.cpu().numpy(), requires_grad=True)
+        d = er.separable_torch(g.x, g.y, prob.lattice.spot_x + sx, prob.lattice.spot_y + sy,
+                               wt, it, st)
+        loss = er.masked_quadratic_loss(d, torch.as_tensor(mask, dtype=torch.float64),
+                                        torch.as_tensor(presc * 100.0, dtype=torch.float64))
+        loss.backward()
+        gr = ((it.grad * t.didd_dr.cpu().double()).sum(1)
+              + (st.grad * t.dsigma_dr.cpu().double()).sum(1)).numpy()
+        print(f"job {k}: loss rel {abs(float(o['loss']) - float(loss)) / float(loss):.2e}, "
+              f"grad_w {rel(o['grad_w'].cpu().numpy(), wt.grad.numpy()):.2e}")
+        assert abs(float(o["loss"]) - float(loss)) <= 1e-6 * abs(float(loss)), k
+        assert rel(o["grad_w"].cpu().numpy(), wt.grad.numpy()) < 1e-4, k
+        assert rel(o["grad_range"].cpu().numpy(), gr) < 1e-4, k
+    b.capture_loss_grad(m, p)
+    b.replay_loss_grad()
+    torch.cuda.synchronize()
+    for o0, o1 in zip(bat, b.grad_outputs):
+        for key in ("loss", "grad_w", "grad_range", "grad_dose"):
+            assert torch.equal(o0[key], o1[key]), key
+
+
 def test_batch_without_grad_tables_refuses_gradients(pb):
     import torch
     _, _, prob = _fields(pb)[0]

@@ -108,6 +108,21 @@ def test_optimizer_steps_validate_before_device_work(pb, lib):
     assert lib.pbd_scenario_combine(1, 3, 0, None, fake, None, None, None) == 0
 
 
+def test_batched_loss_grad_validation(pb, lib):
+    jobs = (pb._lib.GradJob * 129)()
+    for k in range(129):
+        jobs[k].field = field(pb)
+    sz = ctypes.c_size_t(0)
+    assert lib.pbd_loss_grad_batch_workspace(jobs, 129, 1, ctypes.byref(sz)) == -9
+    assert lib.pbd_loss_grad_batch_workspace(jobs, 0, 1, ctypes.byref(sz)) == -2
+    assert lib.pbd_loss_grad_batch_workspace(jobs, 4, 0, ctypes.byref(sz)) == -5   # fp32
+    assert lib.pbd_loss_grad_batch_workspace(jobs, 4, 1, ctypes.byref(sz)) == 0 and sz.value > 0
+    jobs[2].grad_range = 0x1000                       # range gradient on some jobs only
+    assert lib.pbd_loss_grad_batch_workspace(jobs, 4, 1, ctypes.byref(sz)) == -10
+    jobs[2].grad_range = None
+    assert lib.pbd_loss_grad_batch(jobs, 4, 1, ctypes.c_void_p(0x1000), sz.value, None) == -1
+
+
 def test_batch_limits(pb, lib):
     jobs = (pb._lib.Job * 129)()
     for k in range(129):
