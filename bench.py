@@ -47,10 +47,11 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="clinical",
-                    choices=["clinical", "robust", "precision", "optimize", "gamma"],
+                    choices=["clinical", "robust", "precision", "optimize", "gamma", "luts"],
                     help="clinical: the headline gradient workload; robust: 4 fields x 25 "
                     "scenarios batched; precision: forward error vs FP64 per precision mode; "
-                    "optimize: on-device plan-optimisation iterations; gamma: gamma index")
+                    "optimize: on-device plan-optimisation iterations; gamma: gamma index; "
+                    "luts: depth-table builds")
     return ap.parse_args()
 
 
@@ -469,6 +470,61 @@ def gamma_bench(args):
     return 0
 
 
+def luts_bench(args):
+    """Depth tables of the clinical field (40 layers, 128 depths of 2 mm) built on the device
+    by one ``pbd_build_luts`` call -- the per-layer host loop of the reference's model.py
+    moved to the device -- replayed from a CUDA graph, L2 flushed between steps: the nominal
+    tables alone, and with the +-5 um range variants that give dIDD/dR and dsigma/dR.  The
+    CPU baseline is the oracle's NumPy restatement of the reference's loop (one host core)."""
+    import torch
+    pb, wl = workload_arrays()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    K, W = args.steps, max(args.warmup, 3)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    g = wl["grid"]
+    prob = pb.model.problem_from_workload(wl)
+    en = prob.lattice.energies
+    legs = {}
+    clocks = ClockSampler(0)
+    clocks.start()
+    for name, fd in (("nominal", 0.0), ("with_range_derivatives", 0.005)):
+        tb = pb.physics.TableBuilder(g["nz"], g["oz"], g["dz"], en, fd_step=fd, device=dev)
+        tb.build()
+        torch.cuda.synchronize(dev)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            tb.build()
+        for _ in range(W):
+            graph.replay()
+        ms = _timed(torch, dev, graph.replay, K, flush)
+        legs[name] = {"ms": ms, "builds_per_s": 1e3 / ms}
+    clk = clocks.stop()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import physics_ref as pr
+        z = g["oz"] + np.arange(g["nz"]) * g["dz"]
+        e_np = np.asarray(en, dtype=np.float64)
+        t0 = time.perf_counter()
+        n = 0
+        while n < 3 and (n == 0 or time.perf_counter() - t0 < args.cpu_budget_s):
+            pr.layer_luts(z, e_np)
+            n += 1
+        el = time.perf_counter() - t0
+        cpu = {"value": n / el, "unit": "builds/s", "cores": 1, "kind": "port",
+               "sample": f"{n} nominal 40-layer builds (NumPy float64)"}
+    head = legs["nominal"]
+    line = {"workload": "luts", "metric": "depth-table builds/s, 40 layers x 128 depths",
+            "value": head["builds_per_s"], "unit": "builds/s", "n_gpus": 1, "steps": K,
+            "warmup": W, "ms_per_step": head["ms"], "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "clinical field tables (IDD, sigma), "
+                                            "40 layers, 60-160 mm ranges, 128 depths of 2 mm",
+                                            "l2": "flushed between steps"},
+            "legs": legs, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def precision_bench(args):
     """Forward of the 200x200x256 / 61x61x60 field in every precision mode: time per call
     (L2 flushed between calls) and error against the FP64 oracle on the host."""
@@ -532,6 +588,8 @@ def main():
         return optimize_bench(args)
     if args.workload == "gamma":
         return gamma_bench(args)
+    if args.workload == "luts":
+        return luts_bench(args)
     import torch
     import torch.distributed as dist
 
