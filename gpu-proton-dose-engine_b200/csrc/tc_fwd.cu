@@ -437,6 +437,15 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
     // per-thread distance table: float4 groups [g][tid]; y part first, then x part
     float4* tab = reinterpret_cast<float4*>(smem + L.tab);
 
+    // this thread's B1 chunks (row j, K group) -- fixed for the launch, so the divisions by
+    // N1 are done once here rather than in every step
+    int wrg[kWReg];                                 // row | group << 16, or -1
+#pragma unroll
+    for (int r = 0; r < kWReg; ++r) {
+        const int e = tid + r * kMath;
+        wrg[r] = e < nb1 ? (e % N1) | ((e / N1) << 16) : -1;
+    }
+
     uint32_t ph1 = 0, ph2 = 0;
     bool ok = true;
     float dsum[64];
@@ -566,12 +575,11 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             const float* wl = cur.w;
 #pragma unroll
             for (int r = 0; r < kWReg; ++r) {
-                const int e = tid + r * kMath;
-                const int row = e % N1, g = e / N1;
+                const int row = wrg[r] & 0xFFFF, g = wrg[r] >> 16;
 #pragma unroll
                 for (int q = 0; q < EPC; ++q) {
                     const int i = g * EPC + q;
-                    wv[r][q] = (e < nb1 && row < nsy && i < nsx) ? __ldg(wl + (size_t)row * nsx + i) : 0.f;
+                    wv[r][q] = (wrg[r] >= 0 && row < nsy && i < nsx) ? __ldg(wl + (size_t)row * nsx + i) : 0.f;
                 }
             }
         }
@@ -685,9 +693,8 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         // ---- G: B1 = W (N1 rows j, K1 = i) from the registers ----
 #pragma unroll
         for (int r = 0; r < kWReg; ++r) {
-            const int e = tid + r * kMath;
-            if (e < nb1) {
-                const int row = e % N1, g = e / N1;
+            if (wrg[r] >= 0) {
+                const int row = wrg[r] & 0xFFFF, g = wrg[r] >> 16;
                 uint4 hi, lo;
                 split_chunk<MODE>(wv[r], hi, lo);
                 const uint32_t off = (uint32_t)g * plane_n1 + (uint32_t)row * 16u;
