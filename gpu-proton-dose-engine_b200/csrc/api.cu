@@ -217,7 +217,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
         if (tc_adjoint_dims(precision, f, &n1) == PBD_OK) {
             // tensor-core adjoint: (slice, layer-chunk) units, three slots per (layer, slice)
             w.adj_tc = 1;
-            w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : 8;
+            w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : kTcAdjChunk;
             pe = tc_adjoint_slot_elems(f);
             w.acnt = c.take<int>(tc_adjoint_counter_ints(1, f->n_layers));
         } else {
@@ -529,7 +529,9 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
 }
 
 // ---- batched loss gradient ------------------------------------------------------------
-constexpr int kBatchAdjChunk = 8;   // layers per tensor-core adjoint unit (the single-job default)
+// layers per tensor-core adjoint unit of a batch: many jobs balance the grid by themselves,
+// so the batch keeps larger units than one job (8 measured 2 % faster than 4 on 100 jobs)
+constexpr int kBatchAdjChunk = 8;
 
 struct GradPlan {
     int chunk, direct, with_range, max_l;

@@ -272,9 +272,10 @@ int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_job
 int fwd_chunk_layers(const pbd_field* f, int precision) {
     // FP32: ~4 layers per item keeps items small next to the ~2 CTAs per SM.  Tensor cores:
     // the pipeline runs across unit boundaries, so larger units only save partial slices
-    // (16 measured best on the 128^3 / 41 x 41 x 40 field; the autotuner refines it).
+    // (24 measured best, with 4-layer adjoint units, on the 128^3 / 41 x 41 x 40 field;
+    // the autotuner refines it per geometry).
     (void)f;
-    return precision == PBD_PREC_FP32 ? 4 : 16;
+    return precision == PBD_PREC_FP32 ? 4 : 24;
 }
 
 int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items) {

@@ -54,6 +54,8 @@ constexpr int kSpotChunk = 64;      // spots per lattice chunk in the FP32 forwa
 constexpr int kAdjMaxSpots = 64;    // adjoint lattice limit per axis
 constexpr int kMaxChunkCost = 64;   // largest layers-per-item / z-per-item
 constexpr int kLossBlocks = 296;    // fixed grid of the loss reduction (deterministic order)
+constexpr int kTcAdjChunk = 4;      // default active layers per tensor-core adjoint unit
+                                    // (4 measured best on the 128^3 / 41 x 41 x 40 field)
 constexpr int kTcFwdWarps = 8;      // math warps of the tensor-core forward: each owns 32 rows x
                                     // 64 columns of a tile, its own arrival counter and loss partial
 

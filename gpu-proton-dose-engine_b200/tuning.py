@@ -19,8 +19,8 @@ import threading
 
 from . import _lib
 
-CANDIDATES_FWD = (4, 8, 16, 32)
-CANDIDATES_ADJ = (4, 8, 16)
+CANDIDATES_FWD = (8, 16, 24, 32)
+CANDIDATES_ADJ = (2, 4, 8, 16)
 _lock = threading.Lock()
 
 
