@@ -737,6 +737,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
     carve_grad(workspace, n_jobs, gp, g);
     cudaStream_t s = (cudaStream_t)stream;
     GradBufs b{g.fwd, g.adj, g.fpart, g.fcnt + 2, g.lpart, g.apart, g.dcs, g.dsgs, g.fcnt + 1};
+    const int a_chunk = g_adj_chunk > 0 ? g_adj_chunk : kBatchAdjChunk;
     JobDev fview[PBD_MAX_JOBS], aview[PBD_MAX_JOBS];
     size_t arr = 0, fpart = 0, lpart = 0, apart = 0, dcs = 0;
     GradTable t;
@@ -757,7 +758,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
             a.nx = f->nx; a.ny = f->ny; a.nz = f->nz; a.nsx = f->n_sx; a.nsy = f->n_sy;
             a.nl = f->n_layers;
             a.max_chunks_f = gp.direct ? 1 : (f->n_layers + gp.chunk - 1) / gp.chunk;
-            a.max_chunks_a = (f->n_layers + kBatchAdjChunk - 1) / kBatchAdjChunk;
+            a.max_chunks_a = (f->n_layers + a_chunk - 1) / a_chunk;
             a.direct = gp.direct;
             a.n_loss_part = (int)((size_t)f->nz * tiles * kTcFwdWarps);
             a.ox = f->ox; a.oy = f->oy; a.dx = f->dx; a.dy = f->dy;
@@ -783,8 +784,8 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
     }
     PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr, gp.chunk, 1,
                            precision, 0, s));
-    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, kBatchAdjChunk,
-                             gp.with_range, 1, s);
+    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, a_chunk, gp.with_range, 1,
+                             s);
 }
 
 }  // extern "C"

@@ -68,14 +68,15 @@ class ScenarioBatch:
                 self.doses.append(d)
                 k += 1
         self.n_jobs = n_jobs
-        nbytes = _lib.query("pbd_forward_batch_workspace", self.jobs, n_jobs, self.precision)
-        self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
         self.graph = None
 
     def run(self):
-        """Enqueue the batched forward on the current stream."""
-        _lib.call("pbd_forward_batch", self.jobs, self.n_jobs, self.precision, _lib.ptr(self.ws),
-                  self.ws.numel(), _lib.stream_handle(self.device))
+        """Enqueue the batched forward on the current stream (the workspace follows the
+        schedule in force, see ``tuning.schedule``)."""
+        need = _lib.query("pbd_forward_batch_workspace", self.jobs, self.n_jobs, self.precision)
+        ws = self._ws("fwd_batch", need)
+        _lib.call("pbd_forward_batch", self.jobs, self.n_jobs, self.precision, _lib.ptr(ws),
+                  ws.numel(), _lib.stream_handle(self.device))
         return self.doses
 
     def capture(self):
