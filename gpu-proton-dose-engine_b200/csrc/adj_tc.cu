@@ -4,7 +4,7 @@
 // Same mathematics as adj_simt.cu.  With G = dL/dD[z] and unnormalised Gaussians of width
 // s = sigma_l(z), for every active (layer l, slice z):
 //
-//   stage 1   Y[m, x] = sum_y A[m, y] G[y, x]        A = [Gy | Gy']^T, m < 64: j, m >= 64: j'
+//   stage 1   Y[m, x] = sum_y A[m, y] G[y, x]        A = [Gy | Gy']^T, m = 2 j: j, m = 2 j + 1: j'
 //             M = 128 (m), N = 128 (x), K = 128 (y); A generated into TMEM, G^T in smem
 //   stage 2   Q[m, n] = sum_x Y[m, x] B[n, x]        B = [Gx | Gx'], n < N1: i, n >= N1: i'
 //             M = 128 (m), N = 2 N1 (n), K = 128 (x); Y split back into TMEM, B in smem
@@ -26,10 +26,13 @@
 //  * Math warps, per pair n (buffer b = n & 1), without block barriers:
 //      at a unit's first pair: G^T of the slice, split, into smem (the previous unit's last
 //          stage 1 is complete: it was waited for before this pair)
-//      G   A = [Gy | Gy']^T -> TMEM A[b] (tcgen05.st); arrive on ops1
+//      G   A = [Gy | Gy']^T -> TMEM A[b] (tcgen05.st); arrive on ops1.  Rows j and j' of a
+//          spot are adjacent lanes of one warp: each lane evaluates the exponentials of half
+//          the row's columns and the pair swaps them (one shuffle per value), so every
+//          exponential of Gy serves Gy' too
 //      DR  pair n-1's Q from TMEM: Q / (2 pi s^2) into three (layer, slice) slots --
-//          P = Q[j, i], A = Q[j, i'], B = Q[j', i] -- stored transposed ([i][j]) so that a
-//          warp's 32 lanes write 128 contiguous bytes
+//          P = Q[j, i], A = Q[j, i'], B = Q[j', i] -- stored transposed ([i][j]) so that the
+//          even (j) or odd (j') lanes of a warp write 64 contiguous bytes
 //      B   [Gx | Gx'] -> smem (read by stage 2 only, whose previous use DR waited for);
 //          each Gaussian value and its derivative come from one exp
 //      E1  Y of pair n from TMEM, split, back into TMEM A[b]; arrive on ops2
@@ -276,8 +279,8 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
     const int sp = warp & 3, half = warp >> 2;
     const uint32_t lane_base = (uint32_t)(32 * sp) << 16;
     const int m = 32 * sp + lane;          // TMEM lane: row m of A, Y, Q
-    const int jrow = m & 63;
-    const bool deriv = m >= 64;
+    const int jrow = m >> 1;               // rows 2 j (Gy) and 2 j + 1 (Gy') of spot row j
+    const bool deriv = (m & 1) != 0;
     const int N1 = P.N1, R2 = 2 * N1;
     const uint32_t planeR2 = (uint32_t)R2 * 16u;
 
@@ -327,24 +330,39 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         }
 
         // ---- G: A = [Gy | Gy']^T -> TMEM A[b] (row m, y columns [64 half, +64)) ----
+        // The j lane evaluates the exponentials of columns c < 32 of the two rows, the j'
+        // lane those of columns 32 + c; a shuffle swaps them.  Each column's value is the
+        // same FP32 computation as evaluating it in place.
         {
             const float dyf = (float)J.dy;
             const bool valid = jrow < nsy;
+            const float cself = deriv ? 32.f : 0.f;   // first column of this lane's exponentials
             uint32_t hi[2][16], lo[2][16];
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                float v2[2];
+            for (int kp = 0; kp < 16; ++kp) {
+                float vl[2], vh[2];                     // columns 2 kp + t and 32 + 2 kp + t
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
-                    const float d = fmaf((float)(2 * q + t), dyf, ybase), dd = d * d;
-                    const float e = ex2_approx(-dd * a2);
-                    v2[t] = valid ? (deriv ? e * fmaf(dd, inv_s3, -inv_s) : e) : 0.f;
+                    const float c = (float)(2 * kp + t);
+                    const float ds = fmaf(cself + c, dyf, ybase);
+                    const float own = ex2_approx(-(ds * ds) * a2);
+                    const float oth = __shfl_xor_sync(0xffffffffu, own, 1);
+                    const float el = deriv ? oth : own, eh = deriv ? own : oth;
+                    const float dl = fmaf(c, dyf, ybase), ddl = dl * dl;
+                    const float dh = fmaf(32.f + c, dyf, ybase), ddh = dh * dh;
+                    vl[t] = valid ? (deriv ? el * fmaf(ddl, inv_s3, -inv_s) : el) : 0.f;
+                    vh[t] = valid ? (deriv ? eh * fmaf(ddh, inv_s3, -inv_s) : eh) : 0.f;
                 }
-                const uint32_t ha = bf16_bits(v2[0]), hb = bf16_bits(v2[1]);
-                hi[q >> 4][q & 15] = ha | (hb << 16);
-                if (NARR == 2)
-                    lo[q >> 4][q & 15] = bf16_bits(v2[0] - __uint_as_float(ha << 16)) |
-                                         (bf16_bits(v2[1] - __uint_as_float(hb << 16)) << 16);
+                const uint32_t la = bf16_bits(vl[0]), lb = bf16_bits(vl[1]);
+                const uint32_t ha = bf16_bits(vh[0]), hb = bf16_bits(vh[1]);
+                hi[0][kp] = la | (lb << 16);
+                hi[1][kp] = ha | (hb << 16);
+                if (NARR == 2) {
+                    lo[0][kp] = bf16_bits(vl[0] - __uint_as_float(la << 16)) |
+                                (bf16_bits(vl[1] - __uint_as_float(lb << 16)) << 16);
+                    lo[1][kp] = bf16_bits(vh[0] - __uint_as_float(ha << 16)) |
+                                (bf16_bits(vh[1] - __uint_as_float(hb << 16)) << 16);
+                }
             }
             const uint32_t col = kColA + (uint32_t)b * 128u + (uint32_t)(32 * half);
             tc::tmem_st16(tb + lane_base + col, hi[0]);
@@ -369,14 +387,14 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             const JobDev& Jp = P.jobs[prev.job];
             const int pnsx = Jp.nsx, pnsy = Jp.nsy;
             const size_t per = (size_t)pnsy * pnsx;
-            // which slot this warp's quarter of Q feeds (warp-uniform): (j, i) -> P,
+            // which slot this lane's row of the warp's half of Q feeds: (j, i) -> P,
             // (j, i') -> A, (j', i) -> B; the (j', i') quarter is not needed.  tcgen05.ld is
             // warp-collective, so the whole warp loads and only the lanes of real rows store.
             const int which = deriv ? (half == 0 ? 2 : -1) : half;
-            if (which >= 0) {
-                float* slot_base = Jp.partial + (size_t)which * Jp.nl * Jp.nz * per +
+            {
+                float* slot_base = Jp.partial + (size_t)(which >= 0 ? which : 0) * Jp.nl * Jp.nz * per +
                                    ((size_t)prev.l * Jp.nz + prev.z) * per;
-                const bool row_ok = jrow < pnsy;
+                const bool row_ok = which >= 0 && jrow < pnsy;
                 for (int c0 = 0; c0 < N1; c0 += 16) {
                     uint32_t r[16];
                     tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(half * N1 + c0), r);
@@ -469,14 +487,14 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             const JobDev& Jp = P.jobs[prev.job];
             const int pnsx = Jp.nsx, pnsy = Jp.nsy;
             const size_t per = (size_t)pnsy * pnsx;
-            // which slot this warp's quarter of Q feeds (warp-uniform): (j, i) -> P,
+            // which slot this lane's row of the warp's half of Q feeds: (j, i) -> P,
             // (j, i') -> A, (j', i) -> B; the (j', i') quarter is not needed.  tcgen05.ld is
             // warp-collective, so the whole warp loads and only the lanes of real rows store.
             const int which = deriv ? (half == 0 ? 2 : -1) : half;
-            if (which >= 0) {
-                float* slot_base = Jp.partial + (size_t)which * Jp.nl * Jp.nz * per +
+            {
+                float* slot_base = Jp.partial + (size_t)(which >= 0 ? which : 0) * Jp.nl * Jp.nz * per +
                                    ((size_t)prev.l * Jp.nz + prev.z) * per;
-                const bool row_ok = jrow < pnsy;
+                const bool row_ok = which >= 0 && jrow < pnsy;
                 for (int c0 = 0; c0 < N1; c0 += 16) {
                     uint32_t r[16];
                     tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(half * N1 + c0), r);
