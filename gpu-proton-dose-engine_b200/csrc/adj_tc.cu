@@ -30,9 +30,10 @@
 //          spot are adjacent lanes of one warp: each lane evaluates the exponentials of half
 //          the row's columns and the pair swaps them (one shuffle per value), so every
 //          exponential of Gy serves Gy' too
-//      DR  pair n-1's Q from TMEM: Q / (2 pi s^2) into three (layer, slice) slots --
-//          P = Q[j, i], A = Q[j, i'], B = Q[j', i] -- stored transposed ([i][j]) so that the
-//          even (j) or odd (j') lanes of a warp write 64 contiguous bytes
+//      DR  pair n-1's Q from TMEM: Q / (2 pi s^2) into two (layer, slice) slots --
+//          P = Q[j, i] and S = Q[j, i'] + Q[j', i] (the j' lane's value moved to the j lane
+//          by shuffle) -- stored transposed ([i][j]) so that the j lanes of a warp write 64
+//          contiguous bytes
 //      B   [Gx | Gx'] -> smem (read by stage 2 only, whose previous use DR waited for);
 //          each Gaussian value and its derivative come from one exp
 //      E1  Y of pair n from TMEM, split, back into TMEM A[b]; arrive on ops2
@@ -378,7 +379,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(ops1);
 
-        // ---- DR: Q of the previous pair -> the three slots ----
+        // ---- DR: Q of the previous pair -> the two slots ----
         if (have_prev) {
             ok = ok && wait_bar(mma2, ph2);
             if (ok) ph2 ^= 1;
@@ -387,23 +388,29 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             const JobDev& Jp = P.jobs[prev.job];
             const int pnsx = Jp.nsx, pnsy = Jp.nsy;
             const size_t per = (size_t)pnsy * pnsx;
-            // which slot this lane's row of the warp's half of Q feeds: (j, i) -> P,
-            // (j, i') -> A, (j', i) -> B; the (j', i') quarter is not needed.  tcgen05.ld is
-            // warp-collective, so the whole warp loads and only the lanes of real rows store.
-            const int which = deriv ? (half == 0 ? 2 : -1) : half;
+            // Two slots per (layer, slice): P = Q[j, i] and S = Q[j, i'] + Q[j', i] (each term
+            // scaled first).  The warps of a lane quadrant split the i columns in chunks of 16;
+            // a warp loads its chunk of the i and the i' columns (tcgen05.ld is warp-collective),
+            // the j' lane hands Q[j', i] to its j lane by shuffle, and the j lanes store.
             {
-                float* slot_base = Jp.partial + (size_t)(which >= 0 ? which : 0) * Jp.nl * Jp.nz * per +
-                                   ((size_t)prev.l * Jp.nz + prev.z) * per;
-                const bool row_ok = which >= 0 && jrow < pnsy;
-                for (int c0 = 0; c0 < N1; c0 += 16) {
-                    uint32_t r[16];
-                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(half * N1 + c0), r);
+                float* slot_p = Jp.partial + ((size_t)prev.l * Jp.nz + prev.z) * per;
+                float* slot_s = slot_p + (size_t)Jp.nl * Jp.nz * per;
+                const bool row_ok = !deriv && jrow < pnsy;
+                for (int c0 = 16 * half; c0 < N1; c0 += 32) {
+                    uint32_t ri[16], rd[16];
+                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)c0, ri);
+                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(N1 + c0), rd);
                     tc::tmem_wait_ld();
 #pragma unroll
                     for (int q = 0; q < 16; ++q) {
                         const int i = c0 + q;
-                        if (row_ok && i < pnsx)
-                            slot_base[(size_t)i * pnsy + jrow] = prev.nrm * __uint_as_float(r[q]);
+                        const float vi = prev.nrm * __uint_as_float(ri[q]);   // Q[j, i] or Q[j', i]
+                        const float vd = prev.nrm * __uint_as_float(rd[q]);   // Q[j, i']
+                        const float b = __shfl_xor_sync(0xffffffffu, vi, 1);  // j lane: Q[j', i]
+                        if (row_ok && i < pnsx) {
+                            slot_p[(size_t)i * pnsy + jrow] = vi;
+                            slot_s[(size_t)i * pnsy + jrow] = vd + b;
+                        }
                     }
                 }
             }
@@ -487,23 +494,29 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             const JobDev& Jp = P.jobs[prev.job];
             const int pnsx = Jp.nsx, pnsy = Jp.nsy;
             const size_t per = (size_t)pnsy * pnsx;
-            // which slot this lane's row of the warp's half of Q feeds: (j, i) -> P,
-            // (j, i') -> A, (j', i) -> B; the (j', i') quarter is not needed.  tcgen05.ld is
-            // warp-collective, so the whole warp loads and only the lanes of real rows store.
-            const int which = deriv ? (half == 0 ? 2 : -1) : half;
+            // Two slots per (layer, slice): P = Q[j, i] and S = Q[j, i'] + Q[j', i] (each term
+            // scaled first).  The warps of a lane quadrant split the i columns in chunks of 16;
+            // a warp loads its chunk of the i and the i' columns (tcgen05.ld is warp-collective),
+            // the j' lane hands Q[j', i] to its j lane by shuffle, and the j lanes store.
             {
-                float* slot_base = Jp.partial + (size_t)(which >= 0 ? which : 0) * Jp.nl * Jp.nz * per +
-                                   ((size_t)prev.l * Jp.nz + prev.z) * per;
-                const bool row_ok = which >= 0 && jrow < pnsy;
-                for (int c0 = 0; c0 < N1; c0 += 16) {
-                    uint32_t r[16];
-                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(half * N1 + c0), r);
+                float* slot_p = Jp.partial + ((size_t)prev.l * Jp.nz + prev.z) * per;
+                float* slot_s = slot_p + (size_t)Jp.nl * Jp.nz * per;
+                const bool row_ok = !deriv && jrow < pnsy;
+                for (int c0 = 16 * half; c0 < N1; c0 += 32) {
+                    uint32_t ri[16], rd[16];
+                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)c0, ri);
+                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(N1 + c0), rd);
                     tc::tmem_wait_ld();
 #pragma unroll
                     for (int q = 0; q < 16; ++q) {
                         const int i = c0 + q;
-                        if (row_ok && i < pnsx)
-                            slot_base[(size_t)i * pnsy + jrow] = prev.nrm * __uint_as_float(r[q]);
+                        const float vi = prev.nrm * __uint_as_float(ri[q]);   // Q[j, i] or Q[j', i]
+                        const float vd = prev.nrm * __uint_as_float(rd[q]);   // Q[j, i']
+                        const float b = __shfl_xor_sync(0xffffffffu, vi, 1);  // j lane: Q[j', i]
+                        if (row_ok && i < pnsx) {
+                            slot_p[(size_t)i * pnsy + jrow] = vi;
+                            slot_s[(size_t)i * pnsy + jrow] = vd + b;
+                        }
                     }
                 }
             }
@@ -567,7 +580,7 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
 // slots.  Block (segment of kRedZ slices, layer l, job): its threads hold W_l (transposed to
 // the slots' [i][j] order) in registers and walk the segment's active slices in order,
 // accumulating IDD * P slot into a partial dL/dW and forming <P slot, W> (dL/dIDD) and
-// IDD <A + B slot, W> (dL/dsigma) per slice (warp shuffles, then the warps in order).  The
+// IDD <S slot, W> (dL/dsigma) per slice (warp shuffles, then the warps in order).  The
 // block that completes a layer's last segment (per-layer arrival counter) sums the segment
 // partials in segment order into dL/dW and forms dL/dR_l in FP64; the one completing layer
 // 0 also sums the loss partials.  Every sum is in a fixed order: deterministic.
@@ -586,7 +599,7 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     const int nseg = (nz + kRedZ - 1) / kRedZ;
     if (seg >= nseg) return;
     const size_t plane = (size_t)J.nl * nz * per;
-    float* part = J.partial + 3 * plane;           // (nl, nseg, per) segment partials
+    float* part = J.partial + 2 * plane;           // (nl, nseg, per) segment partials
     const double* idd = J.idd + (size_t)l * nz;
     const float* wl = J.w + (size_t)l * per;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -616,7 +629,7 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
                 const int e = tid + k * kRedThreads;
                 const bool in = act && e < per;
                 pv[h][k] = in ? pz[e] : 0.f;
-                qv[h][k] = in ? pz[plane + e] + pz[2 * plane + e] : 0.f;
+                qv[h][k] = in ? pz[plane + e] : 0.f;
             }
         }
 #pragma unroll
@@ -766,7 +779,7 @@ size_t tc_adjoint_counter_ints(int n_jobs, int max_layers) {
 size_t tc_adjoint_slot_elems(const pbd_field* f) {
     const size_t per = (size_t)f->n_sy * f->n_sx;
     const size_t nseg = ((size_t)f->nz + kRedZ - 1) / kRedZ;
-    return 3u * (size_t)f->n_layers * f->nz * per + (size_t)f->n_layers * nseg * per;
+    return 2u * (size_t)f->n_layers * f->nz * per + (size_t)f->n_layers * nseg * per;
 }
 
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,

@@ -215,7 +215,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
         size_t pe = 0;
         int n1 = 0;
         if (tc_adjoint_dims(precision, f, &n1) == PBD_OK) {
-            // tensor-core adjoint: (slice, layer-chunk) units, three slots per (layer, slice)
+            // tensor-core adjoint: (slice, layer-chunk) units, two slots per (layer, slice)
             w.adj_tc = 1;
             w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : kTcAdjChunk;
             pe = tc_adjoint_slot_elems(f);

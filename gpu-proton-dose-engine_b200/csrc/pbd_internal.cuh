@@ -125,7 +125,7 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
 
 // adjoint (tcgen05) -- adj_tc.cu.  Units (slice, chunk of `chunk` active layers) are
-// pulled z-major; `partial` holds three (layer, slice) slot planes of nsy * nsx floats and
+// pulled z-major; `partial` holds two (layer, slice) slot planes of nsy * nsx floats and
 // the reduction's segment partials (tc_adjoint_slot_elems); counter[0] = unit counter,
 // counter[1] = error word, then per job max_layers per-layer arrival counters.
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
