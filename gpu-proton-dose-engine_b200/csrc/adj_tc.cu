@@ -554,6 +554,10 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
+    // Launched as a programmatic dependent of the forward: everything above overlaps the
+    // forward's last CTAs; nothing below runs before the forward has completed (no-op when
+    // there is no such predecessor).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     if (warp >= kMathWarps) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
@@ -591,6 +595,8 @@ constexpr int kRedPer = 16;        // entries per thread: nsy * nsx <= 64 * 64 =
 __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     const JobDev* __restrict__ jobs, int with_range, int finalize_loss, const int* __restrict__ err,
     int* layer_counts, int layer_stride) {
+    // a programmatic dependent of the adjoint kernel: wait for its slots (no-op otherwise)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const JobDev& J = jobs[blockIdx.z];
     int* layer_count = layer_counts + (size_t)blockIdx.z * layer_stride;   // this job's counters
     const int seg = blockIdx.x, l = blockIdx.y;
@@ -757,8 +763,7 @@ int launch_mode(const Params& P0, cudaStream_t s) {
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
     const int grid = std::max(1, std::min(P.n_units, num_sms()));
     prof_mark(kProfAdj, 0, s);
-    adj_tc_kernel<MODE><<<grid, kThreads, smem, s>>>(P);
-    PBD_LAUNCH_CHECK();
+    PBD_TRY(launch_dependent(adj_tc_kernel<MODE>, dim3(grid), dim3(kThreads), smem, s, P));
     prof_mark(kProfAdj, 1, s);
     return PBD_OK;
 }
@@ -783,7 +788,8 @@ size_t tc_adjoint_slot_elems(const pbd_field* f) {
 }
 
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      int* counter, int chunk, int with_range, int finalize_loss, cudaStream_t s) {
+                      int* counter, int chunk, int with_range, int finalize_loss,
+                      int counters_zeroed, cudaStream_t s) {
     Params P{};
     P.jobs = jobs_dev;
     P.n_jobs = n_jobs;
@@ -806,15 +812,17 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     const long long units = (long long)nzm * cm * n_jobs;
     if (units > (1LL << 30)) return PBD_ERR_UNSUPPORTED;
     P.n_units = (int)units;
-    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, tc_adjoint_counter_ints(n_jobs, max_l) * sizeof(int), s)));
+    if (!counters_zeroed)
+        PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0,
+                                        tc_adjoint_counter_ints(n_jobs, max_l) * sizeof(int), s)));
     int rc = PBD_OK;
     if (precision == PBD_PREC_BF16) rc = launch_mode<PBD_PREC_BF16>(P, s);
     else rc = launch_mode<PBD_PREC_BF16X3>(P, s);
     PBD_TRY(rc);
     (void)max_per;
-    adj_tc_reduce_kernel<<<dim3((nzm + kRedZ - 1) / kRedZ, max_l, n_jobs), kRedThreads, 0, s>>>(
-        jobs_dev, with_range, finalize_loss, counter + 1, counter + 2, max_l);
-    PBD_LAUNCH_CHECK();
+    PBD_TRY(launch_dependent(adj_tc_reduce_kernel, dim3((nzm + kRedZ - 1) / kRedZ, max_l, n_jobs),
+                             dim3(kRedThreads), 0, s, (const JobDev*)jobs_dev, with_range,
+                             finalize_loss, (const int*)(counter + 1), counter + 2, max_l));
     count_launch(2);
     return PBD_OK;
 }

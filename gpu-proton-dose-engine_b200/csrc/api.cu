@@ -417,10 +417,10 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
 }
 
 static int run_adjoint(const Ws& ws, int precision, const JobDev* A, int with_range,
-                       int finalize_loss, cudaStream_t s) {
+                       int finalize_loss, int counters_zeroed, cudaStream_t s) {
     if (ws.adj_tc)
         return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, ws.acnt, ws.a_chunk, with_range,
-                                 finalize_loss, s);
+                                 finalize_loss, counters_zeroed, s);
     return launch_adjoint(ws.jobs + 1, A, 1, static_cast<AdjItem*>(ws.aitems), ws.a_items,
                           ws.counters + 2, ws.a_chunk, with_range, finalize_loss, s);
 }
@@ -474,7 +474,7 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return run_adjoint(ws, precision, &A, with_range, 0, s);
+    return run_adjoint(ws, precision, &A, with_range, 0, 0, s);
 }
 
 int pbd_loss_grad_workspace(const pbd_field* f, int precision, size_t* bytes) {
@@ -520,12 +520,17 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     fill_adj_view(f, ws, A);
     A.fwd_err = ws.counters + 1;
     p.j[1] = A;
+    // the adjoint's counters are cleared before the forward, so that forward -> adjoint ->
+    // reduce run back to back (programmatic dependent launches)
+    if (ws.adj_tc)
+        PBD_TRY(cuda_rc(cudaMemsetAsync(ws.acnt, 0,
+                                        tc_adjoint_counter_ints(1, f->n_layers) * sizeof(int), s)));
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
                            ws.f_chunk, 1, precision, 0, s));
-    return run_adjoint(ws, precision, &A, with_range, 1, s);
+    return run_adjoint(ws, precision, &A, with_range, 1, ws.adj_tc, s);
 }
 
 // ---- batched loss gradient ------------------------------------------------------------
@@ -737,6 +742,8 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
     carve_grad(workspace, n_jobs, gp, g);
     cudaStream_t s = (cudaStream_t)stream;
     GradBufs b{g.fwd, g.adj, g.fpart, g.fcnt + 2, g.lpart, g.apart, g.dcs, g.dsgs, g.fcnt + 1};
+    PBD_TRY(cuda_rc(cudaMemsetAsync(g.acnt, 0,
+                                    tc_adjoint_counter_ints(n_jobs, gp.max_l) * sizeof(int), s)));
     const int a_chunk = g_adj_chunk > 0 ? g_adj_chunk : kBatchAdjChunk;
     JobDev fview[PBD_MAX_JOBS], aview[PBD_MAX_JOBS];
     size_t arr = 0, fpart = 0, lpart = 0, apart = 0, dcs = 0;
@@ -784,7 +791,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
     }
     PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr, gp.chunk, 1,
                            precision, 0, s));
-    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, a_chunk, gp.with_range, 1,
+    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, a_chunk, gp.with_range, 1, 1,
                              s);
 }
 

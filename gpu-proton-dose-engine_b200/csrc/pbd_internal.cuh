@@ -78,6 +78,25 @@ inline int cuda_rc(cudaError_t e) { return e == cudaSuccess ? PBD_OK : PBD_ERR_C
         if (pbd_e_ != cudaSuccess) return PBD_ERR_CUDA;          \
     } while (0)
 
+// Launch `kernel` as a programmatic dependent of the previous kernel on `s`: its CTAs may
+// start (and run their prologue) while the previous kernel's last CTAs finish; the kernel
+// itself executes griddepcontrol.wait before touching that kernel's results.
+template <class... KArgs, class... Args>
+int launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                     cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cuda_rc(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+}
+
 // Bump allocator over the caller's workspace.  With base == nullptr it only sizes.
 struct Carve {
     char* base;
@@ -133,8 +152,11 @@ size_t tc_adjoint_slot_elems(const pbd_field* f);
 // Ints of the adjoint's counter block: unit counter, error word, then per job one arrival
 // counter per layer (max_layers of them).
 size_t tc_adjoint_counter_ints(int n_jobs, int max_layers);
+// counters_zeroed: the caller cleared the counter block earlier on the stream (so that no
+// memset sits between the forward and this launch, which runs as its programmatic dependent).
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      int* counter, int chunk, int with_range, int finalize_loss, cudaStream_t s);
+                      int* counter, int chunk, int with_range, int finalize_loss,
+                      int counters_zeroed, cudaStream_t s);
 
 // forward (tcgen05) -- tc_fwd.cu.  Work units (slice, layer chunk, tile) are enumerated
 // z-major; counter[0] = unit counter, counter[1] = error word; every job's `arrive` array
