@@ -47,11 +47,12 @@ def parse():
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="clinical",
-                    choices=["clinical", "robust", "precision", "optimize", "gamma", "luts"],
+                    choices=["clinical", "robust", "precision", "optimize", "gamma", "luts",
+                             "hetero"],
                     help="clinical: the headline gradient workload; robust: 4 fields x 25 "
                     "scenarios batched; precision: forward error vs FP64 per precision mode; "
                     "optimize: on-device plan-optimisation iterations; gamma: gamma index; "
-                    "luts: depth-table builds")
+                    "luts: depth-table builds; hetero: dose in a slab phantom (WED)")
     return ap.parse_args()
 
 
@@ -525,6 +526,78 @@ def luts_bench(args):
     return 0
 
 
+def hetero_bench(args):
+    """The clinical field (128^3, 41x41x40) in a slab phantom -- bone (1.6) from 3 to 5 cm,
+    lung (0.25) from 7 to 10 cm on one side: the WED ray trace and the heterogeneous forward
+    (per-layer lateral maps in one batched tensor-core launch, then the depth doses at the
+    WED), each replayed from a CUDA graph, L2 flushed between steps; the homogeneous forward
+    of the same field beside them.  CPU baseline: the oracle's float64 heterogeneous dose."""
+    import torch
+    pb, wl = workload_arrays()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    prec = args.precision or "tf32x3"
+    K, W = args.steps, max(args.warmup, 3)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    prob = pb.model.problem_from_workload(wl)
+    g = prob.grid
+    zc = g.oz + np.arange(g.nz) * g.dz
+    rho_np = np.ones((g.nz, g.ny, g.nx), dtype=np.float32)
+    rho_np[(zc >= 3.0) & (zc < 5.0)] = 1.6
+    rho_np[(zc >= 7.0) & (zc < 10.0), :, : g.nx // 2] = 0.25
+    rho = torch.as_tensor(rho_np, device=dev)
+    wed = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float64, device=dev)
+    plan = pb.hetero.WedPlan(prob, precision=prec, device=dev)
+    homog = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
+    out = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device=dev)
+    out_h = torch.empty_like(out)
+    clocks = ClockSampler(0)
+    clocks.start()
+
+    def trace():
+        wed.copy_(pb.hetero.wed_raytrace(rho, g, device=dev))
+
+    legs = {}
+    for name, fn in (("wed_raytrace", lambda: pb.hetero.wed_raytrace(rho, g, device=dev)),
+                     ("heterogeneous_forward", lambda: plan.forward(wed, out=out)),
+                     ("homogeneous_forward", lambda: homog.forward(out=out_h))):
+        trace()
+        fn()
+        torch.cuda.synchronize(dev)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            fn()
+        for _ in range(W):
+            graph.replay()
+        legs[name] = {"ms": _timed(torch, dev, graph.replay, K, flush)}
+    clk = clocks.stop()
+    trace()
+    plan.forward(wed, out=out)
+    torch.cuda.synchronize(dev)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import hetero_ref, physics_ref as pr
+        t0 = time.perf_counter()
+        wr = hetero_ref.wed_ref(rho_np, g.oz, g.dz)
+        sig = pr.layer_luts(zc, prob.lattice.energies)[1]
+        ref = hetero_ref.dose_ref(g.x, g.y, prob.lattice.spot_x, prob.lattice.spot_y,
+                                  prob.lattice.ensure_weights(), prob.lattice.energies, sig, wr)
+        el = time.perf_counter() - t0
+        d = out.double().cpu().numpy()
+        legs["max_rel_err_vs_fp64"] = float(np.max(np.abs(d - ref)) / np.max(np.abs(ref)))
+        cpu = {"value": 1.0 / el, "unit": "doses/s", "cores": 16, "kind": "port",
+               "sample": "1 heterogeneous 128^3 dose (NumPy / torch float64, incl. the tables)"}
+    head = legs["heterogeneous_forward"]
+    line = {"workload": "hetero", "metric": "heterogeneous-medium doses/s, 128^3 / 41x41x40",
+            "value": 1e3 / head["ms"], "unit": "doses/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": head["ms"], "higher_is_better": True, "dtype": prec,
+            "data": "synthetic", "config": {"workload": "clinical field, bone and lung slabs",
+                                            "l2": "flushed between steps"},
+            "legs": legs, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def precision_bench(args):
     """Forward of the 200x200x256 / 61x61x60 field in every precision mode: time per call
     (L2 flushed between calls) and error against the FP64 oracle on the host."""
@@ -590,6 +663,8 @@ def main():
         return gamma_bench(args)
     if args.workload == "luts":
         return luts_bench(args)
+    if args.workload == "hetero":
+        return hetero_bench(args)
     import torch
     import torch.distributed as dist
 

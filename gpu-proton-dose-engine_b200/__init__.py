@@ -18,17 +18,18 @@ Modules
   robust     batched fields x scenarios in one persistent launch, CUDA graphs
   optimize   on-device plan optimisation (projected Adam, robust mean / min-max), CUDA graphs
   gamma      gamma index (the reference's gamma.py) in one device call, float64 semantics
+  hetero     water-equivalent depth ray trace and the dose in heterogeneous media
   tuning     measured choice of the work-item sizes, cached per geometry
   distributed  depth-slab and job sharding over torch.distributed (one GPU per rank)
   workloads  synthetic workloads of the benchmark shapes (host, NumPy)
 """
 import sys as _sys
 
-from . import workloads, _lib, physics, model, engines, robust, tuning, distributed, optimize, gamma  # noqa: F401,E501
+from . import workloads, _lib, physics, model, engines, robust, tuning, distributed, optimize, gamma, hetero  # noqa: F401,E501
 
 __version__ = "0.1.0"
 
 _sys.modules.setdefault("pbdose_b200", _sys.modules[__name__])
 for _name in ("workloads", "_lib", "physics", "model", "engines", "robust", "tuning",
-              "distributed", "optimize", "gamma"):
+              "distributed", "optimize", "gamma", "hetero"):
     _sys.modules.setdefault("pbdose_b200." + _name, _sys.modules[__name__ + "." + _name])

@@ -114,6 +114,12 @@ _SIGS = {
     "pbd_forward_batch": (c_int, [POINTER(Job), c_int, c_int, c_void_p, c_size_t, c_void_p]),
     "pbd_loss_grad_batch_workspace": (c_int, [POINTER(GradJob), c_int, c_int, POINTER(c_size_t)]),
     "pbd_loss_grad_batch": (c_int, [POINTER(GradJob), c_int, c_int, c_void_p, c_size_t, c_void_p]),
+    "pbd_wed_raytrace": (c_int, [c_int, c_int, c_int, c_double, c_double, c_void_p, c_void_p,
+                                 c_void_p]),
+    "pbd_forward_wed_workspace": (c_int, [POINTER(Field), POINTER(LutSpec), c_int,
+                                          POINTER(c_size_t)]),
+    "pbd_forward_wed": (c_int, [POINTER(Field), POINTER(LutSpec), c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
     "pbd_adam_step": (c_int, [POINTER(AdamParams), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "pbd_scenario_combine": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

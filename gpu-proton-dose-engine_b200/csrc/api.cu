@@ -290,6 +290,54 @@ int fill_job(const pbd_field* f, JobDev* J) {
     return PBD_OK;
 }
 
+// ---- heterogeneous media helpers ------------------------------------------------------
+// Jobs of one forward launch of the per-layer lateral maps: one single-layer job per layer,
+// depth dose 1 where the layer reaches the slice at all (`act`, (L, nz)), else 0.
+static void wed_jobs(const pbd_field* f, int l0, int n, const float* w, const double* sigma,
+                     const double* act, float* lateral, pbd_job* jobs) {
+    const size_t nvox = (size_t)f->nz * f->ny * f->nx;
+    for (int q = 0; q < n; ++q) {
+        const int l = l0 + q;
+        pbd_job& j = jobs[q];
+        j.field = *f;
+        j.field.n_layers = 1;
+        j.w = w ? w + (size_t)l * f->n_sy * f->n_sx : nullptr;
+        j.idd = act ? act + (size_t)l * f->nz : nullptr;
+        j.sigma = sigma ? sigma + (size_t)l * f->nz : nullptr;
+        j.dose = lateral ? lateral + (size_t)l * nvox : nullptr;
+    }
+}
+
+struct WedCarve {
+    double* act;
+    float* lateral;
+    void* curves;
+    size_t curves_bytes;
+    void* batch;
+    size_t batch_bytes;
+};
+
+static int carve_wed(const pbd_field* f, const pbd_lut_spec* spec, int precision, void* base,
+                     WedCarve& w, size_t* used) {
+    const int L = f->n_layers;
+    const size_t nvox = (size_t)f->nz * f->ny * f->nx;
+    pbd_job jobs[PBD_MAX_JOBS];
+    const int nb = L < PBD_MAX_JOBS ? L : PBD_MAX_JOBS;
+    wed_jobs(f, 0, nb, nullptr, nullptr, nullptr, nullptr, jobs);
+    size_t bb = 0, cb = 0;
+    PBD_TRY(pbd_forward_batch_workspace(jobs, nb, precision, &bb));
+    PBD_TRY(lut_curve_workspace(spec, L, &cb));
+    Carve c(base);
+    w.act = c.take<double>((size_t)L * f->nz);
+    w.lateral = c.take<float>((size_t)L * nvox);
+    w.curves = c.take<char>(cb);
+    w.curves_bytes = cb;
+    w.batch = c.take<char>(bb);
+    w.batch_bytes = bb;
+    *used = c.used + 256;
+    return PBD_OK;
+}
+
 }  // namespace pbd
 
 using namespace pbd;
@@ -713,6 +761,47 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     count_launch(1);
     return launch_forward(jd, host_view, n_jobs, items, item_base, counter, 2 + arr_off, bp.chunk,
                           0, precision, 1, s);
+}
+
+// ---- heterogeneous media ------------------------------------------------------------
+int pbd_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
+                     void* stream) {
+    return lut_wed_raytrace(nz, ny, nx, oz, dz, rho, wed, (cudaStream_t)stream);
+}
+
+int pbd_forward_wed_workspace(const pbd_field* f, const pbd_lut_spec* spec, int precision,
+                              size_t* bytes) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    if (!spec || !bytes) return PBD_ERR_NULL_ARG;
+    WedCarve w;
+    return carve_wed(f, spec, precision, nullptr, w, bytes);
+}
+
+int pbd_forward_wed(const pbd_field* f, const pbd_lut_spec* spec, const double* energies,
+                    const double* range_shift, const float* w, const double* sigma,
+                    const double* wed, float* dose, int precision, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    if (!spec || !energies || !w || !sigma || !wed || !dose) return PBD_ERR_NULL_ARG;
+    WedCarve wc;
+    size_t need = 0;
+    PBD_TRY(carve_wed(f, spec, precision, nullptr, wc, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_wed(f, spec, precision, workspace, wc, &need));
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nslice = (size_t)f->ny * f->nx;
+    PBD_TRY(lut_wed_prepare(spec, f->n_layers, energies, range_shift, wed, f->nz, nslice, wc.act,
+                            wc.curves, wc.curves_bytes, s));
+    pbd_job jobs[PBD_MAX_JOBS];
+    for (int l0 = 0; l0 < f->n_layers; l0 += PBD_MAX_JOBS) {
+        const int n = f->n_layers - l0 < PBD_MAX_JOBS ? f->n_layers - l0 : PBD_MAX_JOBS;
+        wed_jobs(f, l0, n, w, sigma, wc.act, wc.lateral, jobs);
+        PBD_TRY(pbd_forward_batch(jobs, n, precision, wc.batch, wc.batch_bytes, stream));
+    }
+    return lut_wed_combine(spec, f->n_layers, wc.lateral, wed, (size_t)f->nz * nslice, dose,
+                           wc.curves, wc.curves_bytes, s);
 }
 
 int pbd_loss_grad_batch_workspace(const pbd_grad_job* jobs, int n_jobs, int precision,

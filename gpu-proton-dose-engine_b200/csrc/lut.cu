@@ -21,6 +21,8 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <algorithm>
+
 #include "pbd_internal.cuh"
 
 namespace pbd {
@@ -123,6 +125,31 @@ __device__ double interp_lin(double x, double a, double b, int n, const double* 
     double x0 = lin(a, b, n, lo);
     if (x0 == x) return fp[lo];
     double x1 = lin(a, b, n, lo + 1);
+    double slope = (fp[lo + 1] - fp[lo]) / (x1 - x0);
+    return slope * (x - x0) + fp[lo];
+}
+
+// numpy.linspace(a, b, n)[k] with its step (b - a) / (n - 1) passed in: the same value as lin().
+__device__ __forceinline__ double lin_s(double a, double b, int n, int k, double step) {
+    if (k == n - 1) return b;
+    return (double)k * step + a;
+}
+
+// interp_lin with the interval estimated from x * (1 / step) and corrected against the grid
+// points themselves: the same interval, hence the same result, as the binary search.  step =
+// (b - a) / (n - 1) and inv ~ 1 / step come from the caller.
+__device__ double interp_lin_direct(double x, double a, double b, int n, const double* fp,
+                                    double left, double right, double step, double inv) {
+    if (x < a) return left;
+    if (x > b) return right;
+    if (x == b) return fp[n - 1];
+    int lo = (int)((x - a) * inv);
+    lo = lo < 0 ? 0 : (lo > n - 2 ? n - 2 : lo);
+    while (lo > 0 && lin_s(a, b, n, lo, step) > x) --lo;
+    while (lo < n - 2 && lin_s(a, b, n, lo + 1, step) <= x) ++lo;
+    double x0 = lin_s(a, b, n, lo, step);
+    if (x0 == x) return fp[lo];
+    double x1 = lin_s(a, b, n, lo + 1, step);
     double slope = (fp[lo + 1] - fp[lo]) / (x1 - x0);
     return slope * (x - x0) + fp[lo];
 }
@@ -405,6 +432,80 @@ __global__ void lut_output_kernel(pbd_lut_spec spec, LutDims dm, const LayerScal
     }
 }
 
+// Heterogeneous media: dose = sum_l IDD_l(WED) * lateral_l per voxel, IDD_l the layer's
+// smoothed depth curve evaluated at the voxel's water-equivalent depth with the same
+// interpolation as the tables (lut_output_kernel).  Accumulated in FP64, in layer order.
+constexpr int kWedLayers = 256;   // layers whose curve scalars are staged in shared memory
+
+__global__ void wed_combine_kernel(LutDims dm, const LayerScal* scal, const double* smooth,
+                                   const float* lateral, const double* wed, size_t nvox,
+                                   int n_layers, float* dose) {
+    __shared__ double zmax[kWedLayers], stp[kWedLayers], istp[kWedLayers];
+    for (int l = threadIdx.x; l < n_layers && l < kWedLayers; l += blockDim.x) {
+        zmax[l] = scal[l].zmax;
+        stp[l] = (scal[l].zmax - 0.0) / (double)(dm.n_idd - 1);
+        istp[l] = 1.0 / stp[l];
+    }
+    __syncthreads();
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (size_t)gridDim.x * blockDim.x) {
+        const double d = wed[v];
+        double acc = 0.0;
+        for (int l = 0; l < n_layers; ++l) {
+            const double zm = l < kWedLayers ? zmax[l] : scal[l].zmax;
+            const double st = l < kWedLayers ? stp[l] : (zm - 0.0) / (double)(dm.n_idd - 1);
+            const double is = l < kWedLayers ? istp[l] : 1.0 / st;
+            const double idd = interp_lin_direct(d, 0.0, zm, dm.n_idd, smooth + (size_t)l * dm.n_idd,
+                                                 0.0, 0.0, st, is);
+            // a (layer, slice) the activity table marked inactive has IDD 0 at every voxel;
+            // its lateral map is not read
+            if (idd == 0.0) continue;
+            acc += idd * (double)lateral[(size_t)l * nvox + v];
+        }
+        dose[v] = (float)acc;
+    }
+}
+
+// Per (layer, slice) activity of the heterogeneous dose: 1 when some voxel of the slice has a
+// WED inside the layer's depth curve (<= zmax), else 0 (the layer adds nothing there).  One
+// block per slice: the slice's smallest WED, then one entry per layer.
+__global__ void wed_activity_kernel(const LayerScal* scal, const double* wed, size_t nslice,
+                                   int nz, int n_layers, double* act) {
+    __shared__ double red[256];
+    const int z = blockIdx.x;
+    double m = __longlong_as_double(0x7FF0000000000000ll);   // +inf
+    for (size_t v = threadIdx.x; v < nslice; v += blockDim.x) m = fmin(m, wed[(size_t)z * nslice + v]);
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = fmin(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    for (int l = threadIdx.x; l < n_layers; l += blockDim.x)
+        act[(size_t)l * nz + z] = red[0] <= scal[l].zmax ? 1.0 : 0.0;
+}
+
+// Water-equivalent depth at the voxel centres z_k = oz + k dz along +z (the beam axis):
+// the sum of rho * path length from depth 0 (physics.py:421-423 per voxel path), voxel i
+// filling [z_i - dz/2, z_i + dz/2] with rho_i, water above the first voxel, path lengths
+// clipped at depth 0.  One thread per (y, x) column, FP64, in depth order.
+__global__ void wed_raytrace_kernel(int nz, size_t ncol, double oz, double dz, const float* rho,
+                                    double* wed) {
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncol;
+         c += (size_t)gridDim.x * blockDim.x) {
+        const double top0 = oz - 0.5 * dz;
+        double acc = top0 > 0.0 ? top0 : 0.0;          // water above the first voxel
+        for (int k = 0; k < nz; ++k) {
+            const double zc = oz + (double)k * dz;
+            const double lo = fmax(zc - 0.5 * dz, 0.0), mid = fmax(zc, 0.0);
+            const double hi = fmax(zc + 0.5 * dz, 0.0);
+            const double r = (double)rho[(size_t)k * ncol + c];
+            wed[(size_t)k * ncol + c] = acc + r * (mid - lo);
+            acc += r * (hi - lo);
+        }
+    }
+}
+
 // Depth list of the Fermi-Eyges integral (host): its first and last points and size.
 struct FeList {
     int n_list;
@@ -546,6 +647,86 @@ int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const
                                                  fl.single_depth, idd, sigma, didd, dsig);
     PBD_LAUNCH_CHECK();
     count_launch(5);
+    return PBD_OK;
+}
+
+int lut_curve_workspace(const pbd_lut_spec* s, int n_layers, size_t* bytes) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!bytes) return PBD_ERR_NULL_ARG;
+    FeList fl = fe_list(s);
+    Carve c(nullptr);
+    LutWs w;
+    *bytes = carve_lut(c, w, n_layers, 1, s->idd_n_fine, fl.n_fine) + 256;
+    return PBD_OK;
+}
+
+static int wed_dims(const pbd_lut_spec* s, int n_layers, void* ws, LutDims& dm, LutWs& w) {
+    FeList fl = fe_list(s);
+    dm.n_layers = n_layers;
+    dm.nvar = 1;
+    dm.nz = s->nz;
+    dm.n_idd = s->idd_n_fine;
+    dm.n_fe = fl.n_fine;
+    dm.fe_lo = fl.lo;
+    dm.fe_hi = fl.hi;
+    dm.fd_step = 0.0;
+    Carve c(ws);
+    carve_lut(c, w, n_layers, 1, dm.n_idd, dm.n_fe);
+    return PBD_OK;
+}
+
+int lut_wed_prepare(const pbd_lut_spec* s, int n_layers, const double* energies,
+                    const double* shift, const double* wed, int nz, size_t nslice, double* act,
+                    void* ws, size_t ws_bytes, cudaStream_t st) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!energies || !wed || !act) return PBD_ERR_NULL_ARG;
+    size_t need = 0;
+    PBD_TRY(lut_curve_workspace(s, n_layers, &need));
+    if (!ws || ws_bytes < need) return PBD_ERR_WORKSPACE;
+    LutDims dm;
+    LutWs w;
+    PBD_TRY(wed_dims(s, n_layers, ws, dm, w));
+    PBD_TRY(ensure_range_table(st));
+    layer_setup_kernel<<<n_layers, 256, 0, st>>>(*s, dm, energies, shift, w.scal, w.binned, w.ker,
+                                                 w.t_fe);
+    PBD_LAUNCH_CHECK();
+    conv_kernel<<<dim3(n_layers, (dm.n_idd + kConvSeg - 1) / kConvSeg), kConvThreads, kConvSmem, st>>>(
+        dm, w.scal, w.binned, w.ker, w.smooth);
+    PBD_LAUNCH_CHECK();
+    wed_activity_kernel<<<nz, 256, 0, st>>>(w.scal, wed, nslice, nz, n_layers, act);
+    PBD_LAUNCH_CHECK();
+    count_launch(3);
+    return PBD_OK;
+}
+
+int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, const double* wed,
+                    size_t nvox, float* dose, void* ws, size_t ws_bytes, cudaStream_t st) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!lateral || !wed || !dose) return PBD_ERR_NULL_ARG;
+    size_t need = 0;
+    PBD_TRY(lut_curve_workspace(s, n_layers, &need));
+    if (!ws || ws_bytes < need) return PBD_ERR_WORKSPACE;
+    LutDims dm;
+    LutWs w;
+    PBD_TRY(wed_dims(s, n_layers, ws, dm, w));
+    const int blocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 8);
+    wed_combine_kernel<<<std::max(blocks, 1), 256, 0, st>>>(dm, w.scal, w.smooth, lateral, wed, nvox,
+                                                            n_layers, dose);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    return PBD_OK;
+}
+
+int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
+                     cudaStream_t st) {
+    if (!rho || !wed) return PBD_ERR_NULL_ARG;
+    if (nz <= 0 || ny <= 0 || nx <= 0) return PBD_ERR_BAD_DIM;
+    if (!isfinite(oz) || !(dz > 0.0) || !isfinite(dz)) return PBD_ERR_BAD_VALUE;
+    const size_t ncol = (size_t)ny * nx;
+    const int blocks = (int)std::min<size_t>((ncol + 255) / 256, (size_t)num_sms() * 8);
+    wed_raytrace_kernel<<<std::max(blocks, 1), 256, 0, st>>>(nz, ncol, oz, dz, rho, wed);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
     return PBD_OK;
 }
 

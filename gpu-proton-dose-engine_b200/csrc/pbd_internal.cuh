@@ -181,5 +181,17 @@ int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const
               double* idd, double* sigma, double* didd, double* dsig, void* ws, size_t ws_bytes,
               cudaStream_t st);
 int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st);
+// Heterogeneous media (lut.cu): workspace of the per-layer depth curves; prepare builds the
+// curves and the (layer, slice) activity table act (L, nz); combine forms dose = sum_l
+// IDD_l(WED) * lateral_l with lateral (n_layers, nvox) from the curves prepare left in ws;
+// the WED ray trace along +z.
+int lut_curve_workspace(const pbd_lut_spec* s, int n_layers, size_t* bytes);
+int lut_wed_prepare(const pbd_lut_spec* s, int n_layers, const double* energies,
+                    const double* shift, const double* wed, int nz, size_t nslice, double* act,
+                    void* ws, size_t ws_bytes, cudaStream_t st);
+int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, const double* wed,
+                    size_t nvox, float* dose, void* ws, size_t ws_bytes, cudaStream_t st);
+int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
+                     cudaStream_t st);
 
 }  // namespace pbd

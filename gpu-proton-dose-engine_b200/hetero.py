@@ -1,0 +1,97 @@
+"""Heterogeneous media: water-equivalent depth (WED) and the dose that uses it.
+
+The reference treats water only: ``physics.wed_from_density_path`` (physics.py:421-423) is a
+stub, WED = sum of rho * L along one path, and its README lists heterogeneous media as not
+implemented.  Here, on the device:
+
+* ``wed_raytrace(rho, grid)`` -- WED at every voxel centre along the beam axis (+z) through a
+  relative stopping-power map: the reference's sum of rho * L over the path from depth 0 to
+  the voxel centre, voxel k filling [z_k - dz/2, z_k + dz/2], water above the first voxel
+  (``pbd_wed_raytrace``).  rho = 1 gives WED = depth.
+* ``WedPlan(problem).forward(wed)`` -- the dose with each layer's depth dose evaluated at the
+  voxel's WED instead of its geometric depth: the same smoothed depth curve and interpolation
+  as the depth tables (physics.py:328-387), the lateral widths of water at the geometric
+  depth (a broad-beam ray-casting approximation; the lateral scattering in the material is
+  not modelled) (``pbd_forward_wed``).  In water it reproduces the homogeneous dose.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from . import physics as ph
+
+
+def wed_from_density_path(densities, lengths) -> float:
+    """WED = sum rho_i L_i (the reference's helper, physics.py:421-423), host NumPy."""
+    return float(np.sum(np.asarray(densities) * np.asarray(lengths)))
+
+
+def wed_raytrace(rho, grid, device=None):
+    """WED (cm, float64 device tensor (nz, ny, nx)) of a relative stopping-power map
+    ``rho`` (nz, ny, nx) on ``grid`` (a DoseGrid or a dict with nz, ny, nx, oz, dz)."""
+    torch = _lib.require_cuda()
+    dev = torch.device(device or "cuda")
+    g = grid if isinstance(grid, dict) else {k: getattr(grid, k) for k in ("nz", "ny", "nx", "oz", "dz")}
+    r = rho.to(dev, torch.float32).contiguous() if torch.is_tensor(rho) else \
+        torch.as_tensor(np.ascontiguousarray(rho, dtype=np.float32), device=dev)
+    shape = (int(g["nz"]), int(g["ny"]), int(g["nx"]))
+    if tuple(r.shape) != shape:
+        raise ValueError(f"rho has shape {tuple(r.shape)}, the grid {shape}")
+    wed = torch.empty(shape, dtype=torch.float64, device=dev)
+    _lib.call("pbd_wed_raytrace", shape[0], shape[1], shape[2], float(g["oz"]), float(g["dz"]),
+              _lib.ptr(r), _lib.ptr(wed), _lib.stream_handle(dev))
+    return wed
+
+
+class WedPlan:
+    """One field in a heterogeneous medium: the lateral widths of water at the geometric
+    depths (built once on the device) and the workspace of ``pbd_forward_wed``."""
+
+    def __init__(self, problem, *, precision: str = "tf32x3", device=None,
+                 idd_model: ph.IDDModel = ph.DEFAULT_IDD, sigma_x0: float = 0.30):
+        torch = _lib.require_cuda()
+        self.torch = torch
+        self.device = torch.device(device or "cuda")
+        self.problem = problem
+        g, L = problem.grid, problem.lattice
+        if L.energies is None:
+            raise ValueError("the heterogeneous dose needs lattice.energies")
+        self.field = problem.field_descriptor()
+        self.precision = _lib.precision_code(precision)
+        self.spec = ph.lut_spec(g.nz, g.oz, g.dz, idd_model=idd_model, sigma_x0=sigma_x0)
+        self.energies = torch.as_tensor(np.asarray(L.energies, dtype=np.float64), device=self.device)
+        self.sigma = ph.build_tables(g.nz, g.oz, g.dz, L.energies, idd_model=idd_model,
+                                     sigma_x0=sigma_x0, device=self.device).sigma
+        self.w = torch.as_tensor(np.ascontiguousarray(L.ensure_weights(), dtype=np.float32),
+                                 device=self.device)
+        nbytes = _lib.query("pbd_forward_wed_workspace", ctypes.byref(self.field),
+                            ctypes.byref(self.spec), self.precision)
+        self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        self.shape = (g.nz, g.ny, g.nx)
+
+    def forward(self, wed, w=None, out=None):
+        """Dose (float32 device tensor (nz, ny, nx)) for the WED map ``wed`` (float64 device
+        tensor of the grid's shape, e.g. from ``wed_raytrace``), on the current stream."""
+        torch = self.torch
+        if tuple(wed.shape) != self.shape or wed.dtype != torch.float64:
+            raise ValueError("wed must be a float64 tensor of the grid's shape")
+        wt = self.w if w is None else torch.as_tensor(w, dtype=torch.float32,
+                                                      device=self.device).contiguous()
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        wd = wed.to(self.device).contiguous()
+        _lib.call("pbd_forward_wed", ctypes.byref(self.field), ctypes.byref(self.spec),
+                  _lib.ptr(self.energies), None, _lib.ptr(wt), _lib.ptr(self.sigma), _lib.ptr(wd),
+                  _lib.ptr(out), self.precision, _lib.ptr(self.ws), self.ws.numel(),
+                  _lib.stream_handle(self.device))
+        return out
+
+
+def dose_heterogeneous(problem, rho, *, precision: str = "tf32x3", device=None):
+    """(dose, wed) of ``problem`` in the relative stopping-power map ``rho``."""
+    wed = wed_raytrace(rho, problem.grid, device=device)
+    plan = WedPlan(problem, precision=precision, device=device)
+    return plan.forward(wed), wed

@@ -207,6 +207,28 @@ PBD_API int pbd_loss_grad_batch_workspace(const pbd_grad_job *jobs, int n_jobs, 
 PBD_API int pbd_loss_grad_batch(const pbd_grad_job *jobs, int n_jobs, int precision,
                                 void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- heterogeneous media: water-equivalent depth (WED) -----------------------------
+ * The reference has a stub, physics.wed_from_density_path (physics.py:421-423: WED = sum of
+ * rho * L), and lists heterogeneous media as not implemented.
+ * pbd_wed_raytrace: WED at every voxel centre z_k = oz + k dz along the beam axis (+z),
+ * through the relative stopping-power map rho (nz, ny, nx, float32): the sum of rho * path
+ * length from depth 0, voxel k filling [z_k - dz/2, z_k + dz/2], water above the first voxel,
+ * lengths clipped at depth 0; wed (nz, ny, nx) float64.  rho = 1 gives WED = max(z, 0).
+ * pbd_forward_wed: the dose with every layer's depth dose evaluated at the voxel's WED
+ * instead of its depth -- the same curve and interpolation as the depth tables --
+ *   D[z,y,x] = sum_l IDD_l(WED[z,y,x]) * sum_{j,i} Gy_l(z)[y,j] W_l[j,i] Gx_l(z)[x,i]
+ * with the lateral widths sigma (L, nz) of water at the geometric depth (the tables of
+ * pbd_build_luts).  spec / energies / range_shift: as for pbd_build_luts (the depth curves
+ * are rebuilt per call).  The per-layer lateral maps go through the batched forward. */
+PBD_API int pbd_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float *rho,
+                             double *wed, void *stream);
+PBD_API int pbd_forward_wed_workspace(const pbd_field *f, const pbd_lut_spec *spec, int precision,
+                                      size_t *bytes);
+PBD_API int pbd_forward_wed(const pbd_field *f, const pbd_lut_spec *spec, const double *energies,
+                            const double *range_shift, const float *w, const double *sigma,
+                            const double *wed, float *dose, int precision, void *workspace,
+                            size_t workspace_bytes, void *stream);
+
 /* ---- plan-optimisation steps (no counterpart in the reference) ---------------------
  * Device-resident state, so that an optimisation iteration (tables, loss gradient,
  * combination, update) can be captured into one CUDA graph and replayed. */

@@ -1,0 +1,55 @@
+"""CPU restatement of the water-equivalent depth and the heterogeneous dose (TEST
+INFRASTRUCTURE ONLY).
+
+Oracle for ``pbd_wed_raytrace`` and ``pbd_forward_wed``.  Only ``tests/`` may import it.
+
+* ``wed_path``  the (densities, lengths) of the path from depth 0 to voxel k of a column:
+  water above the first voxel, voxels i < k in full, half of voxel k, each voxel filling
+  [z_i - dz/2, z_i + dz/2], lengths clipped at depth 0.  Its WED is the reference's
+  ``wed_from_density_path`` (physics.py:421-423): ``np.sum(densities * lengths)``.
+* ``wed_ref``   the same per voxel for a whole map, cumulated along z (float64).
+* ``dose_ref``  sum over layers of IDD_l(WED) (``physics_ref.idd_fluence`` evaluated at the
+  WED) times the layer's separable lateral dose with unit depth dose (``engine_ref``).
+Pinned: ``wed_path`` + the reference's helper reproduce tests/golden/hetero.npz, made by the
+reference itself.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import engine_ref as er
+from . import physics_ref as pr
+
+
+def wed_path(rho_col, oz, dz, k):
+    z = oz + np.arange(k + 1) * dz
+    dens = [1.0]
+    lens = [max(0.0, z[0] - 0.5 * dz)]
+    for i in range(k):
+        dens.append(float(rho_col[i]))
+        lens.append(max(0.0, z[i] + 0.5 * dz) - max(0.0, z[i] - 0.5 * dz))
+    dens.append(float(rho_col[k]))
+    lens.append(max(0.0, z[k]) - max(0.0, z[k] - 0.5 * dz))
+    return np.array(dens), np.array(lens)
+
+
+def wed_ref(rho, oz, dz):
+    rho = np.asarray(rho, dtype=np.float64)
+    nz = rho.shape[0]
+    z = oz + np.arange(nz) * dz
+    lo = np.maximum(z - 0.5 * dz, 0.0)
+    mid = np.maximum(z, 0.0)
+    hi = np.maximum(z + 0.5 * dz, 0.0)
+    full = rho * (hi - lo)[:, None, None]
+    before = np.concatenate([np.zeros((1,) + rho.shape[1:]), np.cumsum(full, axis=0)[:-1]])
+    return max(0.0, z[0] - 0.5 * dz) + before + rho * (mid - lo)[:, None, None]
+
+
+def dose_ref(xv, yv, xs, ys, w, energies, sigma, wed):
+    w = np.asarray(w, dtype=np.float64)
+    nz = sigma.shape[1]
+    d = np.zeros(wed.shape)
+    for l, e in enumerate(energies):
+        lat = er.separable_f64(xv, yv, xs, ys, w[l:l + 1], np.ones((1, nz)), sigma[l:l + 1])
+        d += pr.idd_fluence(wed.ravel(), e).reshape(wed.shape) * lat
+    return d

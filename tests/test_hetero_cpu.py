@@ -1,0 +1,55 @@
+"""Heterogeneous media, host side (no GPU): the oracle's WED against fixtures made with the
+reference's own wed_from_density_path (bit for bit per voxel path, 1e-13 cumulated), the
+package's host copy of that helper, and argument validation of the C ABI."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden, load_pkg
+from oracle import hetero_ref as hr
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_oracle_wed_matches_reference_fixture(case):
+    z = golden("hetero.npz")
+    rho, want = z[f"rho{case}"].astype(np.float64), z[f"wed{case}"]
+    oz, dz = z[f"grid{case}"]
+    for y in range(rho.shape[1]):
+        for x in range(rho.shape[2]):
+            for k in range(rho.shape[0]):
+                dens, lens = hr.wed_path(rho[:, y, x], oz, dz, k)
+                assert float(np.sum(dens * lens)) == want[k, y, x]
+    got = hr.wed_ref(rho, oz, dz)
+    assert np.max(np.abs(got - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+def test_package_helper_equals_reference_definition():
+    pb = load_pkg()
+    d, l = [1.0, 1.6, 0.25], [0.1, 0.2, 0.1]
+    assert pb.hetero.wed_from_density_path(d, l) == float(np.sum(np.asarray(d) * np.asarray(l)))
+
+
+def test_wed_entry_points_validate_before_device_work():
+    pb = load_pkg()
+    if not os.path.exists(pb._lib.LIB_PATH):
+        pytest.skip("library not built")
+    lib = pb._lib.load()
+    fake = ctypes.c_void_p(0x1000)
+    assert lib.pbd_wed_raytrace(4, 4, 4, 0.0, 0.2, None, fake, None) == -1
+    assert lib.pbd_wed_raytrace(0, 4, 4, 0.0, 0.2, fake, fake, None) == -2
+    assert lib.pbd_wed_raytrace(4, 4, 4, 0.0, 0.0, fake, fake, None) == -10
+    assert lib.pbd_wed_raytrace(4, 4, 4, float("nan"), 0.2, fake, fake, None) == -10
+    f = pb._lib.Field(nx=32, ny=32, nz=64, dx=0.2, dy=0.2, dz=0.2, ox=-3.1, oy=-3.1, oz=0.0,
+                      n_sx=11, n_sy=11, n_layers=8, dx_spot=0.5, dy_spot=0.5, x0=0.0, y0=0.0)
+    spec = pb.physics.lut_spec(64, 0.0, 0.2)
+    sz = ctypes.c_size_t(0)
+    assert lib.pbd_forward_wed_workspace(ctypes.byref(f), ctypes.byref(spec), 1,
+                                         ctypes.byref(sz)) == 0 and sz.value > 0
+    assert lib.pbd_forward_wed_workspace(ctypes.byref(f), None, 1, ctypes.byref(sz)) == -1
+    args = [ctypes.byref(f), ctypes.byref(spec), fake, None, fake, fake, fake, fake, 1]
+    assert lib.pbd_forward_wed(*args, None, 0, None) == -7
+    bad = list(args)
+    bad[6] = None                                   # no WED map
+    assert lib.pbd_forward_wed(*bad, fake, sz.value, None) == -1
