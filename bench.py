@@ -15,6 +15,7 @@ on the data path; the job time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import importlib
 import json
 import os
@@ -529,9 +530,11 @@ def luts_bench(args):
 def hetero_bench(args):
     """The clinical field (128^3, 41x41x40) in a slab phantom -- bone (1.6) from 3 to 5 cm,
     lung (0.25) from 7 to 10 cm on one side: the WED ray trace and the heterogeneous forward
-    (per-layer lateral maps in one batched tensor-core launch, then the depth doses at the
-    WED), each replayed from a CUDA graph, L2 flushed between steps; the homogeneous forward
-    of the same field beside them.  CPU baseline: the oracle's float64 heterogeneous dose."""
+    (activity table, per-layer lateral maps in one batched tensor-core launch, then the depth
+    doses at the WED) from the plan's depth curves, built once per plan like the homogeneous
+    plan's tables and timed as their own leg (wed_curves), each replayed from a CUDA graph, L2
+    flushed between steps; the homogeneous forward of the same field beside them.  CPU
+    baseline: the oracle's float64 heterogeneous dose."""
     import torch
     pb, wl = workload_arrays()
     dev = torch.device("cuda", 0)
@@ -557,8 +560,14 @@ def hetero_bench(args):
     def trace():
         wed.copy_(pb.hetero.wed_raytrace(rho, g, device=dev))
 
+    def curves():
+        pb._lib.call("pbd_build_wed_curves", ctypes.byref(plan.spec), len(prob.lattice.energies),
+                     pb._lib.ptr(plan.energies), None, pb._lib.ptr(plan.curves),
+                     plan.curves.numel(), pb._lib.stream_handle(dev))
+
     legs = {}
     for name, fn in (("wed_raytrace", lambda: pb.hetero.wed_raytrace(rho, g, device=dev)),
+                     ("wed_curves", curves),
                      ("heterogeneous_forward", lambda: plan.forward(wed, out=out)),
                      ("homogeneous_forward", lambda: homog.forward(out=out_h))):
         trace()

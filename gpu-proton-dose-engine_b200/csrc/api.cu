@@ -293,9 +293,15 @@ int fill_job(const pbd_field* f, JobDev* J) {
 // ---- heterogeneous media helpers ------------------------------------------------------
 // Jobs of one forward launch of the per-layer lateral maps: one single-layer job per layer,
 // depth dose 1 where the layer reaches the slice at all (`act`, (L, nz)), else 0.
+// Row stride (floats) of the per-layer lateral maps: the voxel count rounded up to 64 floats,
+// so every row starts on a 256-byte boundary for the combine's bulk copies.
+static size_t wed_lateral_stride(const pbd_field* f) {
+    return align_up((size_t)f->nz * f->ny * f->nx, 64);
+}
+
 static void wed_jobs(const pbd_field* f, int l0, int n, const float* w, const double* sigma,
                      const double* act, float* lateral, pbd_job* jobs) {
-    const size_t nvox = (size_t)f->nz * f->ny * f->nx;
+    const size_t lstride = wed_lateral_stride(f);
     for (int q = 0; q < n; ++q) {
         const int l = l0 + q;
         pbd_job& j = jobs[q];
@@ -304,13 +310,14 @@ static void wed_jobs(const pbd_field* f, int l0, int n, const float* w, const do
         j.w = w ? w + (size_t)l * f->n_sy * f->n_sx : nullptr;
         j.idd = act ? act + (size_t)l * f->nz : nullptr;
         j.sigma = sigma ? sigma + (size_t)l * f->nz : nullptr;
-        j.dose = lateral ? lateral + (size_t)l * nvox : nullptr;
+        j.dose = lateral ? lateral + (size_t)l * lstride : nullptr;
     }
 }
 
 struct WedCarve {
     double* act;
-    float* lateral;
+    int* err;            // the combine's error word
+    float* lateral;      // (L, wed_lateral_stride) per-layer lateral maps
     void* curves;
     size_t curves_bytes;
     void* batch;
@@ -320,7 +327,6 @@ struct WedCarve {
 static int carve_wed(const pbd_field* f, const pbd_lut_spec* spec, int precision, void* base,
                      WedCarve& w, size_t* used) {
     const int L = f->n_layers;
-    const size_t nvox = (size_t)f->nz * f->ny * f->nx;
     pbd_job jobs[PBD_MAX_JOBS];
     const int nb = L < PBD_MAX_JOBS ? L : PBD_MAX_JOBS;
     wed_jobs(f, 0, nb, nullptr, nullptr, nullptr, nullptr, jobs);
@@ -329,7 +335,8 @@ static int carve_wed(const pbd_field* f, const pbd_lut_spec* spec, int precision
     PBD_TRY(lut_curve_workspace(spec, L, &cb));
     Carve c(base);
     w.act = c.take<double>((size_t)L * f->nz);
-    w.lateral = c.take<float>((size_t)L * nvox);
+    w.err = c.take<int>(1);
+    w.lateral = c.take<float>((size_t)L * wed_lateral_stride(f));
     w.curves = c.take<char>(cb);
     w.curves_bytes = cb;
     w.batch = c.take<char>(bb);
@@ -778,30 +785,71 @@ int pbd_forward_wed_workspace(const pbd_field* f, const pbd_lut_spec* spec, int 
     return carve_wed(f, spec, precision, nullptr, w, bytes);
 }
 
-int pbd_forward_wed(const pbd_field* f, const pbd_lut_spec* spec, const double* energies,
-                    const double* range_shift, const float* w, const double* sigma,
-                    const double* wed, float* dose, int precision, void* workspace,
-                    size_t workspace_bytes, void* stream) {
-    PBD_TRY(host_validate_field(f));
-    PBD_TRY(check_field_precision(f, precision));
-    if (!spec || !energies || !w || !sigma || !wed || !dose) return PBD_ERR_NULL_ARG;
-    WedCarve wc;
-    size_t need = 0;
-    PBD_TRY(carve_wed(f, spec, precision, nullptr, wc, &need));
-    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
-    PBD_TRY(carve_wed(f, spec, precision, workspace, wc, &need));
+int pbd_wed_curves_workspace(const pbd_lut_spec* spec, int n_layers, size_t* bytes) {
+    if (!spec || !bytes) return PBD_ERR_NULL_ARG;
+    return lut_curve_workspace(spec, n_layers, bytes);
+}
+
+int pbd_build_wed_curves(const pbd_lut_spec* spec, int n_layers, const double* energies,
+                         const double* range_shift, void* curves, size_t curves_bytes,
+                         void* stream) {
+    if (!spec || !energies || !curves) return PBD_ERR_NULL_ARG;
+    return lut_wed_curves(spec, n_layers, energies, range_shift, curves, curves_bytes,
+                          (cudaStream_t)stream);
+}
+
+// Activity table, the per-layer lateral maps through the batched forward, then the combine.
+static int forward_wed_body(const pbd_field* f, const pbd_lut_spec* spec, const void* curves,
+                            size_t curves_bytes, const float* w, const double* sigma,
+                            const double* wed, float* dose, int precision, const WedCarve& wc,
+                            void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nslice = (size_t)f->ny * f->nx;
-    PBD_TRY(lut_wed_prepare(spec, f->n_layers, energies, range_shift, wed, f->nz, nslice, wc.act,
-                            wc.curves, wc.curves_bytes, s));
+    PBD_TRY(lut_wed_activity(spec, f->n_layers, curves, curves_bytes, wed, f->nz, nslice, wc.act,
+                             s));
     pbd_job jobs[PBD_MAX_JOBS];
     for (int l0 = 0; l0 < f->n_layers; l0 += PBD_MAX_JOBS) {
         const int n = f->n_layers - l0 < PBD_MAX_JOBS ? f->n_layers - l0 : PBD_MAX_JOBS;
         wed_jobs(f, l0, n, w, sigma, wc.act, wc.lateral, jobs);
         PBD_TRY(pbd_forward_batch(jobs, n, precision, wc.batch, wc.batch_bytes, stream));
     }
-    return lut_wed_combine(spec, f->n_layers, wc.lateral, wed, (size_t)f->nz * nslice, dose,
-                           wc.curves, wc.curves_bytes, s);
+    PBD_TRY(cuda_rc(cudaMemsetAsync(wc.err, 0, sizeof(int), s)));
+    return lut_wed_combine(spec, f->n_layers, wc.lateral, wed_lateral_stride(f), wed,
+                           (size_t)f->nz * nslice, dose, wc.err, curves, curves_bytes, s);
+}
+
+static int wed_setup(const pbd_field* f, const pbd_lut_spec* spec, int precision, void* workspace,
+                     size_t workspace_bytes, WedCarve& wc) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    size_t need = 0;
+    PBD_TRY(carve_wed(f, spec, precision, nullptr, wc, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    return carve_wed(f, spec, precision, workspace, wc, &need);
+}
+
+int pbd_forward_wed(const pbd_field* f, const pbd_lut_spec* spec, const double* energies,
+                    const double* range_shift, const float* w, const double* sigma,
+                    const double* wed, float* dose, int precision, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+    if (!f || !spec || !energies || !w || !sigma || !wed || !dose) return PBD_ERR_NULL_ARG;
+    WedCarve wc;
+    PBD_TRY(wed_setup(f, spec, precision, workspace, workspace_bytes, wc));
+    PBD_TRY(lut_wed_curves(spec, f->n_layers, energies, range_shift, wc.curves, wc.curves_bytes,
+                           (cudaStream_t)stream));
+    return forward_wed_body(f, spec, wc.curves, wc.curves_bytes, w, sigma, wed, dose, precision,
+                            wc, stream);
+}
+
+int pbd_forward_wed_curves(const pbd_field* f, const pbd_lut_spec* spec, const void* curves,
+                           size_t curves_bytes, const float* w, const double* sigma,
+                           const double* wed, float* dose, int precision, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+    if (!f || !spec || !curves || !w || !sigma || !wed || !dose) return PBD_ERR_NULL_ARG;
+    WedCarve wc;
+    PBD_TRY(wed_setup(f, spec, precision, workspace, workspace_bytes, wc));
+    return forward_wed_body(f, spec, curves, curves_bytes, w, sigma, wed, dose, precision, wc,
+                            stream);
 }
 
 int pbd_loss_grad_batch_workspace(const pbd_grad_job* jobs, int n_jobs, int precision,

@@ -622,7 +622,7 @@ int carve(void* base, int nz, int ny, int nx, GammaWs& w, size_t* bytes) {
     w.pmax = c.take<double>(w.n_blocks);
     w.keys = c.take<unsigned long long>(n);
     w.cand = c.take<unsigned long long>(n);
-    *bytes = c.used;
+    *bytes = c.used + 256;       // slack for an unaligned workspace base
     return PBD_OK;
 }
 

@@ -24,6 +24,7 @@
 #include <algorithm>
 
 #include "pbd_internal.cuh"
+#include "tc_common.cuh"
 
 namespace pbd {
 namespace {
@@ -135,23 +136,36 @@ __device__ __forceinline__ double lin_s(double a, double b, int n, int k, double
     return (double)k * step + a;
 }
 
-// interp_lin with the interval estimated from x * (1 / step) and corrected against the grid
-// points themselves: the same interval, hence the same result, as the binary search.  step =
-// (b - a) / (n - 1) and inv ~ 1 / step come from the caller.
-__device__ double interp_lin_direct(double x, double a, double b, int n, const double* fp,
-                                    double left, double right, double step, double inv) {
-    if (x < a) return left;
-    if (x > b) return right;
-    if (x == b) return fp[n - 1];
+// The interval of x on linspace(a, b, n) that interp_lin's binary search finds, for a <= x <= b:
+// estimated from x * (1 / step) and corrected against the grid points themselves, whose values
+// fk * step + a (fk = (double)lo kept in step with lo -- integers below 2^53, so fk +- 1 is
+// exact) are those lin_s computes.  lo and its grid point x0 on return; x == b gives lo = n - 1,
+// x0 = b.  step = (b - a) / (n - 1) and inv ~ 1 / step come from the caller.
+__device__ __forceinline__ void locate_lin(double x, double a, double b, int n, double step,
+                                           double inv, int& lo_out, double& x0_out) {
+    if (x == b) {
+        lo_out = n - 1;
+        x0_out = b;
+        return;
+    }
     int lo = (int)((x - a) * inv);
     lo = lo < 0 ? 0 : (lo > n - 2 ? n - 2 : lo);
-    while (lo > 0 && lin_s(a, b, n, lo, step) > x) --lo;
-    while (lo < n - 2 && lin_s(a, b, n, lo + 1, step) <= x) ++lo;
-    double x0 = lin_s(a, b, n, lo, step);
-    if (x0 == x) return fp[lo];
-    double x1 = lin_s(a, b, n, lo + 1, step);
-    double slope = (fp[lo + 1] - fp[lo]) / (x1 - x0);
-    return slope * (x - x0) + fp[lo];
+    double fk = (double)lo;
+    double x0 = fk * step + a;
+    while (lo > 0 && x0 > x) {
+        --lo;
+        fk -= 1.0;
+        x0 = fk * step + a;
+    }
+    while (lo < n - 2) {
+        const double x1 = lo + 1 == n - 1 ? b : (fk + 1.0) * step + a;
+        if (!(x1 <= x)) break;
+        ++lo;
+        fk += 1.0;
+        x0 = x1;
+    }
+    lo_out = lo;
+    x0_out = x0;
 }
 
 __device__ __forceinline__ double csda(double e) {
@@ -437,71 +451,275 @@ __global__ void lut_output_kernel(pbd_lut_spec spec, LutDims dm, const LayerScal
 // interpolation as the tables (lut_output_kernel).  Accumulated in FP64, in layer order.
 constexpr int kWedLayers = 256;   // layers whose curve scalars are staged in shared memory
 
-__global__ void wed_combine_kernel(LutDims dm, const LayerScal* scal, const double* smooth,
-                                   const float* lateral, const double* wed, size_t nvox,
-                                   int n_layers, float* dose) {
+// The combine streams each layer's lateral values of a 1024-voxel tile into a ring of
+// shared-memory stages with 1-D bulk copies (cp.async.bulk, completion on an mbarrier), so the
+// bytes in flight do not depend on the registers the FP64 interpolation needs.  Layers that
+// no voxel of the tile reaches (tile's smallest WED above zmax, or largest below 0) are
+// neither copied nor evaluated.  Waits are bounded (2 s); a block whose wait runs out sets
+// the error word, waits (bounded) for its own copies in flight and leaves, and the poison pass
+// turns the dose into NaN.
+constexpr int kCmbThreads = 256;
+constexpr int kCmbPer = 4;                              // voxels per thread
+constexpr int kCmbTile = kCmbThreads * kCmbPer;         // voxels per tile (4 KB of one layer)
+constexpr int kCmbStages = 6;
+
+__device__ __forceinline__ void bulk_load_s(void* dst, const void* src, uint32_t bytes,
+                                            uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            tc::smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kCmbThreads) wed_combine_kernel(
+    LutDims dm, const LayerScal* scal, const double2* pts, const float* lateral, size_t lstride,
+    const double* wed, size_t nvox, int n_layers, float* dose, int* err) {
+    __shared__ __align__(128) float lat[kCmbStages][kCmbTile];
+    __shared__ __align__(8) uint64_t full[kCmbStages];
     __shared__ double zmax[kWedLayers], stp[kWedLayers], istp[kWedLayers];
-    for (int l = threadIdx.x; l < n_layers && l < kWedLayers; l += blockDim.x) {
+    __shared__ double rmin[kCmbThreads / 32], rmax[kCmbThreads / 32];
+    __shared__ int rnan[kCmbThreads / 32];
+    __shared__ int abort_s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int l = tid; l < n_layers && l < kWedLayers; l += kCmbThreads) {
         zmax[l] = scal[l].zmax;
         stp[l] = (scal[l].zmax - 0.0) / (double)(dm.n_idd - 1);
         istp[l] = 1.0 / stp[l];
     }
+    if (tid == 0) {
+        for (int q = 0; q < kCmbStages; ++q) tc::mbar_init(&full[q], 1);
+        tc::fence_mbar_init();
+        abort_s = 0;
+    }
     __syncthreads();
-    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
-         v += (size_t)gridDim.x * blockDim.x) {
-        const double d = wed[v];
-        double acc = 0.0;
-        for (int l = 0; l < n_layers; ++l) {
-            const double zm = l < kWedLayers ? zmax[l] : scal[l].zmax;
-            const double st = l < kWedLayers ? stp[l] : (zm - 0.0) / (double)(dm.n_idd - 1);
-            const double is = l < kWedLayers ? istp[l] : 1.0 / st;
-            const double idd = interp_lin_direct(d, 0.0, zm, dm.n_idd, smooth + (size_t)l * dm.n_idd,
-                                                 0.0, 0.0, st, is);
-            // a (layer, slice) the activity table marked inactive has IDD 0 at every voxel;
-            // its lateral map is not read
-            if (idd == 0.0) continue;
-            acc += idd * (double)lateral[(size_t)l * nvox + v];
+    const int n = dm.n_idd;
+    const double inf = __longlong_as_double(0x7FF0000000000000ll);
+    const size_t n_tiles = (nvox + kCmbTile - 1) / kCmbTile;
+    uint32_t it = 0;       // copies consumed: stage it % kCmbStages, parity (it / kCmbStages) & 1
+    uint32_t issued = 0;   // copies issued (thread 0)
+    int next_l = 0;        // next layer thread 0 considers (thread 0)
+    for (size_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const size_t v0 = t * kCmbTile;
+        const int cnt = (int)((nvox - v0) < (size_t)kCmbTile ? (nvox - v0) : (size_t)kCmbTile);
+        double d[kCmbPer], acc[kCmbPer];
+        double mn = inf, mx = -inf;
+        int has_nan = 0;
+#pragma unroll
+        for (int j = 0; j < kCmbPer; ++j) {
+            const int i = tid + j * kCmbThreads;
+            acc[j] = 0.0;
+            d[j] = 0.0;
+            if (i < cnt) {
+                d[j] = __ldcs(wed + v0 + i);
+                if (d[j] != d[j]) {
+                    has_nan = 1;
+                } else {
+                    mn = fmin(mn, d[j]);
+                    mx = fmax(mx, d[j]);
+                }
+            }
         }
-        dose[v] = (float)acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            has_nan |= __shfl_xor_sync(0xffffffffu, has_nan, o);
+        }
+        if (lane == 0) {
+            rmin[warp] = mn;
+            rmax[warp] = mx;
+            rnan[warp] = has_nan;
+        }
+        __syncthreads();
+        double tmin = inf, tmax = -inf;
+        bool tnan = false;
+#pragma unroll
+        for (int q = 0; q < kCmbThreads / 32; ++q) {
+            tmin = fmin(tmin, rmin[q]);
+            tmax = fmax(tmax, rmax[q]);
+            tnan = tnan || rnan[q] != 0;
+        }
+        // the same answer in every thread: layer l is copied and evaluated for this tile
+        auto active = [&](int l) -> bool {
+            const double zm = l < kWedLayers ? zmax[l] : scal[l].zmax;
+            return tnan || (tmin <= zm && tmax >= 0.0);
+        };
+        const uint32_t bytes = (uint32_t)((cnt + 3) / 4) * 16u;
+        auto refill = [&]() {
+            while (issued - it < (uint32_t)kCmbStages && next_l < n_layers) {
+                if (active(next_l)) {
+                    const uint32_t q = issued % kCmbStages;
+                    bulk_load_s(lat[q], lateral + (size_t)next_l * lstride + v0, bytes, &full[q]);
+                    ++issued;
+                }
+                ++next_l;
+            }
+        };
+        if (tid == 0) {
+            next_l = 0;
+            refill();
+        }
+        for (int l = 0; l < n_layers; ++l) {
+            if (!active(l)) continue;
+            const uint32_t q = it % kCmbStages;
+            if (!tcc::wait_bar(&full[q], (it / kCmbStages) & 1u)) {
+                abort_s = 1;
+                atomicExch(err, 1);
+            } else {
+                const double zm = l < kWedLayers ? zmax[l] : scal[l].zmax;
+                const double st = l < kWedLayers ? stp[l] : (zm - 0.0) / (double)(n - 1);
+                const double is = l < kWedLayers ? istp[l] : 1.0 / st;
+                const double2* lp = pts + (size_t)l * n;
+                // A voxel counts only where its WED lies inside the curve (or is NaN): outside
+                // [0, zmax] the curve's fill values are 0 and nothing is added, and a (layer,
+                // slice) the activity table marked inactive has every WED above zmax, so the
+                // unwritten part of a lateral map is copied at most, never used.
+                int lo[kCmbPer];
+                double x0[kCmbPer];
+#pragma unroll
+                for (int j = 0; j < kCmbPer; ++j) {
+                    lo[j] = 0;
+                    x0[j] = 0.0;
+                    if (tid + j * kCmbThreads < cnt && !(d[j] < 0.0 || d[j] > zm))
+                        locate_lin(d[j], 0.0, zm, n, st, is, lo[j], x0[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < kCmbPer; ++j) {
+                    const int i = tid + j * kCmbThreads;
+                    if (i >= cnt || d[j] < 0.0 || d[j] > zm) continue;
+                    const double2 pt = __ldg(lp + lo[j]);
+                    // interp_lin's value: fp[lo] on a grid point, else slope * (x - x0) + fp[lo]
+                    // with the slope np.interp rounds; the sum in layer order
+                    const double idd = x0[j] == d[j] ? pt.x : pt.y * (d[j] - x0[j]) + pt.x;
+                    if (idd == 0.0) continue;
+                    acc[j] += idd * (double)lat[q][i];
+                }
+            }
+            __syncthreads();   // stage q is free again; abort_s is visible to every thread
+            ++it;
+            if (abort_s) break;
+            if (tid == 0) refill();
+        }
+        if (abort_s) {
+            // the copies still in flight (the one whose wait ran out included) land before
+            // the block's shared memory is released
+            if (tid == 0)
+                for (uint32_t c = it - 1; c != issued; ++c)
+                    (void)tcc::wait_bar(&full[c % kCmbStages], (c / kCmbStages) & 1u);
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < kCmbPer; ++j) {
+            const int i = tid + j * kCmbThreads;
+            if (i < cnt) __stcs(dose + v0 + i, (float)acc[j]);
+        }
+        __syncthreads();   // the next tile's reduction reuses rmin / rmax / rnan
+    }
+}
+
+// After a combine whose wait ran out: the whole dose is invalid, NaN.
+__global__ void wed_poison_kernel(float* dose, size_t nvox, const int* err) {
+    if (*err == 0) return;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (size_t)gridDim.x * blockDim.x)
+        dose[v] = __int_as_float(0x7fc00000);
+}
+
+// Curve points of the smoothed depth curves: {fp[k], slope_k} with slope_k = (fp[k+1] - fp[k])
+// / (x[k+1] - x[k]) on the grid linspace(0, zmax, n) -- the operands and the single rounding
+// of np.interp's slope (and of interp_lin) -- and 0 at the last point.  Value and slope share a
+// 16-byte load in the combine, which needs no division per voxel.
+__global__ void wed_slope_kernel(LutDims dm, const LayerScal* scal, const double* smooth,
+                                 double2* pts) {
+    const int l = blockIdx.x;
+    const int n = dm.n_idd;
+    const double zm = scal[l].zmax;
+    const double st = (zm - 0.0) / (double)(n - 1);
+    const double* fp = smooth + (size_t)l * n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double s = 0.0;
+        if (k < n - 1) {
+            const double x0 = lin_s(0.0, zm, n, k, st), x1 = lin_s(0.0, zm, n, k + 1, st);
+            s = (fp[k + 1] - fp[k]) / (x1 - x0);
+        }
+        pts[(size_t)l * n + k] = make_double2(fp[k], s);
     }
 }
 
 // Per (layer, slice) activity of the heterogeneous dose: 1 when some voxel of the slice has a
 // WED inside the layer's depth curve (<= zmax), else 0 (the layer adds nothing there).  One
 // block per slice: the slice's smallest WED, then one entry per layer.
-__global__ void wed_activity_kernel(const LayerScal* scal, const double* wed, size_t nslice,
-                                   int nz, int n_layers, double* act) {
-    __shared__ double red[256];
+constexpr int kActThreads = 1024;
+
+__global__ void __launch_bounds__(kActThreads) wed_activity_kernel(const LayerScal* scal,
+                                                                   const double* wed,
+                                                                   size_t nslice, int nz,
+                                                                   int n_layers, double* act) {
+    __shared__ double red[kActThreads / 32];
     const int z = blockIdx.x;
-    double m = __longlong_as_double(0x7FF0000000000000ll);   // +inf
-    for (size_t v = threadIdx.x; v < nslice; v += blockDim.x) m = fmin(m, wed[(size_t)z * nslice + v]);
-    red[threadIdx.x] = m;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) red[threadIdx.x] = fmin(red[threadIdx.x], red[threadIdx.x + w]);
-        __syncthreads();
+    const double* p = wed + (size_t)z * nslice;
+    const double inf = __longlong_as_double(0x7FF0000000000000ll);
+    // eight independent loads in flight per thread; fmin is exact in any order (NaN ignored)
+    double m[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) m[q] = inf;
+    size_t v = threadIdx.x;
+    for (; v + 7 * (size_t)kActThreads < nslice; v += 8 * (size_t)kActThreads) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) m[q] = fmin(m[q], __ldcs(p + v + (size_t)q * kActThreads));
     }
-    for (int l = threadIdx.x; l < n_layers; l += blockDim.x)
-        act[(size_t)l * nz + z] = red[0] <= scal[l].zmax ? 1.0 : 0.0;
+    for (; v < nslice; v += kActThreads) m[0] = fmin(m[0], __ldcs(p + v));
+    double t = fmin(fmin(fmin(m[0], m[1]), fmin(m[2], m[3])), fmin(fmin(m[4], m[5]), fmin(m[6], m[7])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t = fmin(t, __shfl_xor_sync(0xffffffffu, t, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        t = red[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t = fmin(t, __shfl_xor_sync(0xffffffffu, t, o));
+        if (threadIdx.x == 0) red[0] = t;
+    }
+    __syncthreads();
+    const double smin = red[0];
+    for (int l = threadIdx.x; l < n_layers; l += kActThreads)
+        act[(size_t)l * nz + z] = smin <= scal[l].zmax ? 1.0 : 0.0;
 }
 
 // Water-equivalent depth at the voxel centres z_k = oz + k dz along +z (the beam axis):
 // the sum of rho * path length from depth 0 (physics.py:421-423 per voxel path), voxel i
 // filling [z_i - dz/2, z_i + dz/2] with rho_i, water above the first voxel, path lengths
 // clipped at depth 0.  One thread per (y, x) column, FP64, in depth order.
-__global__ void wed_raytrace_kernel(int nz, size_t ncol, double oz, double dz, const float* rho,
-                                    double* wed) {
+constexpr int kRayThreads = 64;   // 64-thread blocks: a 128 x 128 field still fills every SM
+constexpr int kRayBatch = 16;     // depths whose rho one thread loads before the running sum
+
+__global__ void __launch_bounds__(kRayThreads) wed_raytrace_kernel(int nz, size_t ncol, double oz,
+                                                                   double dz, const float* rho,
+                                                                   double* wed) {
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncol;
          c += (size_t)gridDim.x * blockDim.x) {
         const double top0 = oz - 0.5 * dz;
         double acc = top0 > 0.0 ? top0 : 0.0;          // water above the first voxel
-        for (int k = 0; k < nz; ++k) {
-            const double zc = oz + (double)k * dz;
-            const double lo = fmax(zc - 0.5 * dz, 0.0), mid = fmax(zc, 0.0);
-            const double hi = fmax(zc + 0.5 * dz, 0.0);
-            const double r = (double)rho[(size_t)k * ncol + c];
-            wed[(size_t)k * ncol + c] = acc + r * (mid - lo);
-            acc += r * (hi - lo);
+        for (int k0 = 0; k0 < nz; k0 += kRayBatch) {
+            float r[kRayBatch];
+#pragma unroll
+            for (int q = 0; q < kRayBatch; ++q)
+                r[q] = k0 + q < nz ? __ldcs(rho + (size_t)(k0 + q) * ncol + c) : 0.0f;
+#pragma unroll
+            for (int q = 0; q < kRayBatch; ++q) {
+                const int k = k0 + q;
+                if (k >= nz) break;
+                const double zc = oz + (double)k * dz;
+                const double lo = fmax(zc - 0.5 * dz, 0.0), mid = fmax(zc, 0.0);
+                const double hi = fmax(zc + 0.5 * dz, 0.0);
+                const double rr = (double)r[q];
+                __stcs(wed + (size_t)k * ncol + c, acc + rr * (mid - lo));
+                acc += rr * (hi - lo);
+            }
         }
     }
 }
@@ -650,17 +868,30 @@ int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const
     return PBD_OK;
 }
 
+// The depth-curve blob of the heterogeneous dose: the table builder's nominal-variant
+// workspace followed by the curve points {value, slope} (n_layers, n_idd).
+static size_t carve_curves(Carve& c, LutWs& w, double2*& pts, int n_layers, int n_idd, int n_fe) {
+    carve_lut(c, w, n_layers, 1, n_idd, n_fe);
+    pts = c.take<double2>((size_t)n_layers * n_idd);
+    return c.used;
+}
+
 int lut_curve_workspace(const pbd_lut_spec* s, int n_layers, size_t* bytes) {
     PBD_TRY(validate_spec(s, n_layers));
     if (!bytes) return PBD_ERR_NULL_ARG;
     FeList fl = fe_list(s);
     Carve c(nullptr);
     LutWs w;
-    *bytes = carve_lut(c, w, n_layers, 1, s->idd_n_fine, fl.n_fine) + 256;
+    double2* pts = nullptr;
+    *bytes = carve_curves(c, w, pts, n_layers, s->idd_n_fine, fl.n_fine) + 256;
     return PBD_OK;
 }
 
-static int wed_dims(const pbd_lut_spec* s, int n_layers, void* ws, LutDims& dm, LutWs& w) {
+static int wed_dims(const pbd_lut_spec* s, int n_layers, const void* ws, size_t ws_bytes,
+                    LutDims& dm, LutWs& w, double2*& pts) {
+    size_t need = 0;
+    PBD_TRY(lut_curve_workspace(s, n_layers, &need));
+    if (!ws || ws_bytes < need) return PBD_ERR_WORKSPACE;
     FeList fl = fe_list(s);
     dm.n_layers = n_layers;
     dm.nvar = 1;
@@ -670,22 +901,19 @@ static int wed_dims(const pbd_lut_spec* s, int n_layers, void* ws, LutDims& dm, 
     dm.fe_lo = fl.lo;
     dm.fe_hi = fl.hi;
     dm.fd_step = 0.0;
-    Carve c(ws);
-    carve_lut(c, w, n_layers, 1, dm.n_idd, dm.n_fe);
+    Carve c(const_cast<void*>(ws));
+    carve_curves(c, w, pts, n_layers, dm.n_idd, dm.n_fe);
     return PBD_OK;
 }
 
-int lut_wed_prepare(const pbd_lut_spec* s, int n_layers, const double* energies,
-                    const double* shift, const double* wed, int nz, size_t nslice, double* act,
-                    void* ws, size_t ws_bytes, cudaStream_t st) {
+int lut_wed_curves(const pbd_lut_spec* s, int n_layers, const double* energies,
+                   const double* shift, void* curves, size_t curves_bytes, cudaStream_t st) {
     PBD_TRY(validate_spec(s, n_layers));
-    if (!energies || !wed || !act) return PBD_ERR_NULL_ARG;
-    size_t need = 0;
-    PBD_TRY(lut_curve_workspace(s, n_layers, &need));
-    if (!ws || ws_bytes < need) return PBD_ERR_WORKSPACE;
+    if (!energies) return PBD_ERR_NULL_ARG;
     LutDims dm;
     LutWs w;
-    PBD_TRY(wed_dims(s, n_layers, ws, dm, w));
+    double2* pts = nullptr;
+    PBD_TRY(wed_dims(s, n_layers, curves, curves_bytes, dm, w, pts));
     PBD_TRY(ensure_range_table(st));
     layer_setup_kernel<<<n_layers, 256, 0, st>>>(*s, dm, energies, shift, w.scal, w.binned, w.ker,
                                                  w.t_fe);
@@ -693,27 +921,57 @@ int lut_wed_prepare(const pbd_lut_spec* s, int n_layers, const double* energies,
     conv_kernel<<<dim3(n_layers, (dm.n_idd + kConvSeg - 1) / kConvSeg), kConvThreads, kConvSmem, st>>>(
         dm, w.scal, w.binned, w.ker, w.smooth);
     PBD_LAUNCH_CHECK();
-    wed_activity_kernel<<<nz, 256, 0, st>>>(w.scal, wed, nslice, nz, n_layers, act);
+    wed_slope_kernel<<<n_layers, 256, 0, st>>>(dm, w.scal, w.smooth, pts);
     PBD_LAUNCH_CHECK();
     count_launch(3);
     return PBD_OK;
 }
 
-int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, const double* wed,
-                    size_t nvox, float* dose, void* ws, size_t ws_bytes, cudaStream_t st) {
+int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, size_t curves_bytes,
+                     const double* wed, int nz, size_t nslice, double* act, cudaStream_t st) {
     PBD_TRY(validate_spec(s, n_layers));
-    if (!lateral || !wed || !dose) return PBD_ERR_NULL_ARG;
-    size_t need = 0;
-    PBD_TRY(lut_curve_workspace(s, n_layers, &need));
-    if (!ws || ws_bytes < need) return PBD_ERR_WORKSPACE;
+    if (!wed || !act) return PBD_ERR_NULL_ARG;
     LutDims dm;
     LutWs w;
-    PBD_TRY(wed_dims(s, n_layers, ws, dm, w));
-    const int blocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 8);
-    wed_combine_kernel<<<std::max(blocks, 1), 256, 0, st>>>(dm, w.scal, w.smooth, lateral, wed, nvox,
-                                                            n_layers, dose);
+    double2* pts = nullptr;
+    PBD_TRY(wed_dims(s, n_layers, curves, curves_bytes, dm, w, pts));
+    wed_activity_kernel<<<nz, kActThreads, 0, st>>>(w.scal, wed, nslice, nz, n_layers, act);
     PBD_LAUNCH_CHECK();
     count_launch(1);
+    return PBD_OK;
+}
+
+int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, size_t lstride,
+                    const double* wed, size_t nvox, float* dose, int* err, const void* curves,
+                    size_t curves_bytes, cudaStream_t st) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!lateral || !wed || !dose || !err) return PBD_ERR_NULL_ARG;
+    // 1-D bulk copies: 16-byte aligned rows, the tile's copy rounded up to 16 bytes inside
+    // the row
+    if ((reinterpret_cast<size_t>(lateral) & 15) || (lstride & 3) || lstride < ((nvox + 3) & ~(size_t)3))
+        return PBD_ERR_BAD_VALUE;
+    LutDims dm;
+    LutWs w;
+    double2* pts = nullptr;
+    PBD_TRY(wed_dims(s, n_layers, curves, curves_bytes, dm, w, pts));
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wed_combine_kernel, kCmbThreads, 0) !=
+                cudaSuccess || b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    const size_t n_tiles = (nvox + kCmbTile - 1) / kCmbTile;
+    const int blocks = (int)std::min<size_t>(n_tiles, (size_t)num_sms() * per_sm);
+    wed_combine_kernel<<<std::max(blocks, 1), kCmbThreads, 0, st>>>(dm, w.scal, pts, lateral,
+                                                                    lstride, wed, nvox, n_layers,
+                                                                    dose, err);
+    PBD_LAUNCH_CHECK();
+    const int pb = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 4);
+    wed_poison_kernel<<<std::max(pb, 1), 256, 0, st>>>(dose, nvox, err);
+    PBD_LAUNCH_CHECK();
+    count_launch(2);
     return PBD_OK;
 }
 
@@ -723,8 +981,9 @@ int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* 
     if (nz <= 0 || ny <= 0 || nx <= 0) return PBD_ERR_BAD_DIM;
     if (!isfinite(oz) || !(dz > 0.0) || !isfinite(dz)) return PBD_ERR_BAD_VALUE;
     const size_t ncol = (size_t)ny * nx;
-    const int blocks = (int)std::min<size_t>((ncol + 255) / 256, (size_t)num_sms() * 8);
-    wed_raytrace_kernel<<<std::max(blocks, 1), 256, 0, st>>>(nz, ncol, oz, dz, rho, wed);
+    const int blocks = (int)std::min<size_t>((ncol + kRayThreads - 1) / kRayThreads,
+                                             (size_t)num_sms() * 32);
+    wed_raytrace_kernel<<<std::max(blocks, 1), kRayThreads, 0, st>>>(nz, ncol, oz, dz, rho, wed);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return PBD_OK;

@@ -98,13 +98,17 @@ int launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t sme
 }
 
 // Bump allocator over the caller's workspace.  With base == nullptr it only sizes.
+// Sub-arrays of a caller's workspace, each starting on a 256-byte ADDRESS boundary (the base
+// need not be aligned).  Sized with base = nullptr, which assumes an aligned base: every
+// workspace query adds 256 bytes of slack for the first alignment step of an unaligned one.
 struct Carve {
     char* base;
     size_t used;
     explicit Carve(void* b) : base(static_cast<char*>(b)), used(0) {}
     template <class T>
     T* take(size_t count) {
-        used = align_up(used, 256);
+        const size_t b = reinterpret_cast<size_t>(base);
+        used = align_up(b + used, 256) - b;
         T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
         used += count * sizeof(T);
         return p;
@@ -181,16 +185,20 @@ int lut_build(const pbd_lut_spec* s, int n_layers, const double* energies, const
               double* idd, double* sigma, double* didd, double* dsig, void* ws, size_t ws_bytes,
               cudaStream_t st);
 int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st);
-// Heterogeneous media (lut.cu): workspace of the per-layer depth curves; prepare builds the
-// curves and the (layer, slice) activity table act (L, nz); combine forms dose = sum_l
-// IDD_l(WED) * lateral_l with lateral (n_layers, nvox) from the curves prepare left in ws;
-// the WED ray trace along +z.
+// Heterogeneous media (lut.cu): size of the depth-curve blob; curves builds the per-layer
+// smoothed depth curves and their interval slopes into it; activity fills the (layer, slice)
+// table act (L, nz) from a WED map; combine forms dose = sum_l IDD_l(WED) * lateral_l with
+// layer l's lateral map at lateral + l * lstride (16-byte aligned, lstride a multiple of 4
+// floats, >= nvox rounded up to 4) and an error word err (set when a bounded wait ran out;
+// the dose is then NaN); the WED ray trace along +z.
 int lut_curve_workspace(const pbd_lut_spec* s, int n_layers, size_t* bytes);
-int lut_wed_prepare(const pbd_lut_spec* s, int n_layers, const double* energies,
-                    const double* shift, const double* wed, int nz, size_t nslice, double* act,
-                    void* ws, size_t ws_bytes, cudaStream_t st);
-int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, const double* wed,
-                    size_t nvox, float* dose, void* ws, size_t ws_bytes, cudaStream_t st);
+int lut_wed_curves(const pbd_lut_spec* s, int n_layers, const double* energies,
+                   const double* shift, void* curves, size_t curves_bytes, cudaStream_t st);
+int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, size_t curves_bytes,
+                     const double* wed, int nz, size_t nslice, double* act, cudaStream_t st);
+int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, size_t lstride,
+                    const double* wed, size_t nvox, float* dose, int* err, const void* curves,
+                    size_t curves_bytes, cudaStream_t st);
 int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
                      cudaStream_t st);
 

@@ -12,7 +12,8 @@ implemented.  Here, on the device:
   voxel's WED instead of its geometric depth: the same smoothed depth curve and interpolation
   as the depth tables (physics.py:328-387), the lateral widths of water at the geometric
   depth (a broad-beam ray-casting approximation; the lateral scattering in the material is
-  not modelled) (``pbd_forward_wed``).  In water it reproduces the homogeneous dose.
+  not modelled) (``pbd_build_wed_curves`` once, then ``pbd_forward_wed_curves``).  In water it
+  reproduces the homogeneous dose.
 """
 from __future__ import annotations
 
@@ -48,7 +49,8 @@ def wed_raytrace(rho, grid, device=None):
 
 class WedPlan:
     """One field in a heterogeneous medium: the lateral widths of water at the geometric
-    depths (built once on the device) and the workspace of ``pbd_forward_wed``."""
+    depths and the layers' depth curves (``pbd_build_wed_curves``), built once on the device,
+    and the workspace of ``pbd_forward_wed_curves``."""
 
     def __init__(self, problem, *, precision: str = "tf32x3", device=None,
                  idd_model: ph.IDDModel = ph.DEFAULT_IDD, sigma_x0: float = 0.30):
@@ -70,6 +72,12 @@ class WedPlan:
         nbytes = _lib.query("pbd_forward_wed_workspace", ctypes.byref(self.field),
                             ctypes.byref(self.spec), self.precision)
         self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        # the depth curves depend on the energies only: built once, reused by every forward
+        cbytes = _lib.query("pbd_wed_curves_workspace", ctypes.byref(self.spec), len(L.energies))
+        self.curves = torch.empty(cbytes, dtype=torch.uint8, device=self.device)
+        _lib.call("pbd_build_wed_curves", ctypes.byref(self.spec), len(L.energies),
+                  _lib.ptr(self.energies), None, _lib.ptr(self.curves), cbytes,
+                  _lib.stream_handle(self.device))
         self.shape = (g.nz, g.ny, g.nx)
 
     def forward(self, wed, w=None, out=None):
@@ -83,10 +91,10 @@ class WedPlan:
         if out is None:
             out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
         wd = wed.to(self.device).contiguous()
-        _lib.call("pbd_forward_wed", ctypes.byref(self.field), ctypes.byref(self.spec),
-                  _lib.ptr(self.energies), None, _lib.ptr(wt), _lib.ptr(self.sigma), _lib.ptr(wd),
-                  _lib.ptr(out), self.precision, _lib.ptr(self.ws), self.ws.numel(),
-                  _lib.stream_handle(self.device))
+        _lib.call("pbd_forward_wed_curves", ctypes.byref(self.field), ctypes.byref(self.spec),
+                  _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(wt), _lib.ptr(self.sigma),
+                  _lib.ptr(wd), _lib.ptr(out), self.precision, _lib.ptr(self.ws),
+                  self.ws.numel(), _lib.stream_handle(self.device))
         return out
 
 

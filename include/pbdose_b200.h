@@ -218,8 +218,13 @@ PBD_API int pbd_loss_grad_batch(const pbd_grad_job *jobs, int n_jobs, int precis
  * instead of its depth -- the same curve and interpolation as the depth tables --
  *   D[z,y,x] = sum_l IDD_l(WED[z,y,x]) * sum_{j,i} Gy_l(z)[y,j] W_l[j,i] Gx_l(z)[x,i]
  * with the lateral widths sigma (L, nz) of water at the geometric depth (the tables of
- * pbd_build_luts).  spec / energies / range_shift: as for pbd_build_luts (the depth curves
- * are rebuilt per call).  The per-layer lateral maps go through the batched forward. */
+ * pbd_build_luts).  spec / energies / range_shift: as for pbd_build_luts.  The per-layer
+ * lateral maps go through the batched forward.
+ * pbd_build_wed_curves: the per-layer smoothed depth curves and their interval slopes, built
+ * once into an opaque device blob of pbd_wed_curves_workspace bytes; pbd_forward_wed_curves
+ * computes the dose from such a blob (built with the same spec and n_layers) without
+ * rebuilding it; pbd_forward_wed builds the curves inside its workspace on every call.  Both
+ * forwards take a workspace of pbd_forward_wed_workspace bytes. */
 PBD_API int pbd_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float *rho,
                              double *wed, void *stream);
 PBD_API int pbd_forward_wed_workspace(const pbd_field *f, const pbd_lut_spec *spec, int precision,
@@ -228,6 +233,15 @@ PBD_API int pbd_forward_wed(const pbd_field *f, const pbd_lut_spec *spec, const 
                             const double *range_shift, const float *w, const double *sigma,
                             const double *wed, float *dose, int precision, void *workspace,
                             size_t workspace_bytes, void *stream);
+PBD_API int pbd_wed_curves_workspace(const pbd_lut_spec *spec, int n_layers, size_t *bytes);
+PBD_API int pbd_build_wed_curves(const pbd_lut_spec *spec, int n_layers, const double *energies,
+                                 const double *range_shift, void *curves, size_t curves_bytes,
+                                 void *stream);
+PBD_API int pbd_forward_wed_curves(const pbd_field *f, const pbd_lut_spec *spec,
+                                   const void *curves, size_t curves_bytes, const float *w,
+                                   const double *sigma, const double *wed, float *dose,
+                                   int precision, void *workspace, size_t workspace_bytes,
+                                   void *stream);
 
 /* ---- plan-optimisation steps (no counterpart in the reference) ---------------------
  * Device-resident state, so that an optimisation iteration (tables, loss gradient,

@@ -80,3 +80,65 @@ def test_slab_phantom_vs_oracle(pb):
     # the slabs move the dose: not the water result
     d_water = pb.engines.DosePlan(prob, tables="device", precision="fp32").forward().cpu().numpy()
     assert rel(d, d_water) > 1e-2
+
+
+def test_one_shot_entry_point_equals_plan(pb):
+    """pbd_forward_wed (curves rebuilt inside its workspace) gives the plan's dose (curves
+    built once by pbd_build_wed_curves) bit for bit, call after call, also from a workspace
+    whose base is not 256-byte aligned."""
+    import ctypes
+    import torch
+    lib = pb._lib
+    wl, en, prob = _cfg0(pb)
+    g = prob.grid
+    zc = g.oz + np.arange(g.nz) * g.dz
+    rho = np.ones((g.nz, g.ny, g.nx), dtype=np.float32)
+    rho[(zc >= 1.0) & (zc < 2.5), :, g.nx // 3:] = 0.4
+    wed = pb.hetero.wed_raytrace(rho, g)
+    plan = pb.hetero.WedPlan(prob, precision="tf32x3")
+    a = plan.forward(wed).clone()
+    b = plan.forward(wed).clone()
+    out = torch.empty_like(a)
+    lib.call("pbd_forward_wed", ctypes.byref(plan.field), ctypes.byref(plan.spec),
+             lib.ptr(plan.energies), None, lib.ptr(plan.w), lib.ptr(plan.sigma), lib.ptr(wed),
+             lib.ptr(out), plan.precision, lib.ptr(plan.ws), plan.ws.numel(),
+             lib.stream_handle(plan.device))
+    torch.cuda.synchronize()
+    assert torch.equal(a, b) and torch.equal(a, out)
+    # a workspace whose base is only 8-byte aligned: the library aligns its sub-arrays itself
+    need = plan.ws.numel()
+    raw = torch.empty(need + 64, dtype=torch.uint8, device=plan.device)
+    out2 = torch.empty_like(a)
+    lib.call("pbd_forward_wed", ctypes.byref(plan.field), ctypes.byref(plan.spec),
+             lib.ptr(plan.energies), None, lib.ptr(plan.w), lib.ptr(plan.sigma), lib.ptr(wed),
+             lib.ptr(out2), plan.precision, ctypes.c_void_p(raw.data_ptr() + 8), need,
+             lib.stream_handle(plan.device))
+    torch.cuda.synchronize()
+    assert torch.equal(a, out2)
+
+
+def test_ragged_grid_random_medium_vs_oracle(pb):
+    """A 29 x 23 x 37 grid (24,679 voxels: the last 1024-voxel tile holds 103, not a multiple
+    of 4) in a random medium (rho 0.2 to 2.0) that takes some voxels past every layer's range."""
+    wl = dict(pb.workloads.build_workload(0))
+    nx, ny, nz = 29, 23, 37
+    wl["grid"] = {"nx": nx, "ny": ny, "nz": nz, "dx": 0.15, "dy": 0.2, "dz": 0.3,
+                  "ox": -(nx - 1) * 0.075, "oy": -(ny - 1) * 0.1, "oz": 0.0}
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    g = prob.grid
+    rng = np.random.default_rng(29)
+    rho = rng.uniform(0.2, 2.0, (nz, ny, nx)).astype(np.float32)
+    zc = g.oz + np.arange(g.nz) * g.dz
+    wed_ref = hr.wed_ref(rho, g.oz, g.dz)
+    sig = pr.layer_luts(zc, en)[1]
+    want = hr.dose_ref(g.x, g.y, prob.lattice.spot_x, prob.lattice.spot_y, wl["weights"], en, sig,
+                       wed_ref)
+    wed = pb.hetero.wed_raytrace(rho, g)
+    assert rel(wed.cpu().numpy(), wed_ref) <= 1e-13
+    assert wed_ref.max() > 1.2 * wl["r_max"]               # past every layer's range
+    for prec in ("fp32", "tf32x3"):
+        d = pb.hetero.WedPlan(prob, precision=prec).forward(wed).cpu().numpy()
+        err = rel(d, want)
+        print(f"ragged {prec}: heterogeneous dose max rel err {err:.2e}")
+        assert err < 1e-6, prec

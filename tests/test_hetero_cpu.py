@@ -53,3 +53,19 @@ def test_wed_entry_points_validate_before_device_work():
     bad = list(args)
     bad[6] = None                                   # no WED map
     assert lib.pbd_forward_wed(*bad, fake, sz.value, None) == -1
+    # the curve blob: size query, build and forward validate before any device work
+    cb = ctypes.c_size_t(0)
+    assert lib.pbd_wed_curves_workspace(ctypes.byref(spec), 8, ctypes.byref(cb)) == 0
+    assert cb.value > 0
+    assert lib.pbd_wed_curves_workspace(None, 8, ctypes.byref(cb)) == -1
+    assert lib.pbd_wed_curves_workspace(ctypes.byref(spec), 0, ctypes.byref(cb)) < 0
+    assert lib.pbd_build_wed_curves(ctypes.byref(spec), 8, None, None, fake, cb.value, None) == -1
+    assert lib.pbd_build_wed_curves(ctypes.byref(spec), 8, fake, None, fake, 16, None) == -7
+    cargs = [ctypes.byref(f), ctypes.byref(spec), fake, cb.value, fake, fake, fake, fake, 1]
+    assert lib.pbd_forward_wed_curves(*cargs, None, 0, None) == -7
+    short = list(cargs)
+    short[3] = 16                                   # curve blob too small
+    assert lib.pbd_forward_wed_curves(*short, fake, sz.value, None) == -7
+    nul = list(cargs)
+    nul[2] = None                                   # no curve blob
+    assert lib.pbd_forward_wed_curves(*nul, fake, sz.value, None) == -1
