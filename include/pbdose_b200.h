@@ -19,7 +19,9 @@
  * are DEVICE pointers unless stated otherwise.  Work is enqueued on `stream` (a
  * cudaStream_t passed as void*; NULL = legacy default stream) and is asynchronous: the
  * caller synchronises.  The caller owns all memory; scratch comes from the caller's
- * `workspace`, sized by the matching *_workspace() query.
+ * `workspace`, sized by the matching *_workspace() query; a workspace needs no particular
+ * alignment (the library starts each of its sub-arrays on a 256-byte address boundary inside
+ * it, and the queries include the slack for that).
  */
 #ifndef PBDOSE_B200_H
 #define PBDOSE_B200_H
