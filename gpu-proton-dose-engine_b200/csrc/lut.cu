@@ -475,7 +475,8 @@ __device__ __forceinline__ void bulk_load_s(void* dst, const void* src, uint32_t
         : "memory");
 }
 
-__global__ void __launch_bounds__(kCmbThreads) wed_combine_kernel(
+// 48 registers, no spills: 5 blocks per SM (64 registers without the bound: 4)
+__global__ void __launch_bounds__(kCmbThreads, 5) wed_combine_kernel(
     LutDims dm, const LayerScal* scal, const double2* pts, const float* lateral, size_t lstride,
     const double* wed, size_t nvox, int n_layers, float* dose, int* err) {
     __shared__ __align__(128) float lat[kCmbStages][kCmbTile];
