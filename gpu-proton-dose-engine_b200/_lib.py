@@ -198,6 +198,35 @@ def profile_end() -> dict:
     return {"fwd_ms": fm.value, "n_fwd": fn.value, "adj_ms": am.value, "n_adj": an.value}
 
 
+def same_device(a, b) -> bool:
+    """Whether two torch devices name the same GPU ("cuda" means the current one)."""
+    if a.type != b.type:
+        return False
+    if a.type != "cuda":
+        return True
+    import torch
+    cur = torch.cuda.current_device()
+    return (cur if a.index is None else a.index) == (cur if b.index is None else b.index)
+
+
+def check_arg(t, name: str, numel: int, dtype, device):
+    """A tensor the library reads or writes through a raw pointer: on ``device``, of ``dtype``,
+    contiguous, ``numel`` elements -- anything else would be read or written out of bounds,
+    so it is refused here, before any launch."""
+    import torch
+    if not torch.is_tensor(t):
+        raise TypeError(f"{name} must be a torch tensor")
+    if not same_device(t.device, device):
+        raise ValueError(f"{name} is on {t.device}, expected {device}")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if t.numel() != numel:
+        raise ValueError(f"{name} has {t.numel()} elements, expected {numel}")
+    return t
+
+
 def ptr(t) -> int | None:
     """Device address of a torch tensor (None for None)."""
     if t is None:

@@ -171,9 +171,15 @@ class DosePlan:
             return self.w
         if not torch.is_tensor(w):
             w = torch.as_tensor(np.asarray(w, dtype=np.float32))
-        if w.device != self.device:
+        if not _lib.same_device(w.device, self.device):
             w = w.to(self.device, non_blocking=True)
-        return w.to(torch.float32).contiguous()
+        w = w.to(torch.float32).contiguous()
+        return _lib.check_arg(w, "w", self.w.numel(), torch.float32, self.device)
+
+    def _check_tables(self, idd, sigma):
+        n = self.w.shape[0] * self.shape[0]
+        _lib.check_arg(idd, "idd", n, self.torch.float64, self.device)
+        _lib.check_arg(sigma, "sigma", n, self.torch.float64, self.device)
 
     # -- forward -------------------------------------------------------------------
     def forward(self, w=None, out=None, idd=None, sigma=None):
@@ -181,8 +187,11 @@ class DosePlan:
         w = self._weights(w)
         idd = self.idd if idd is None else idd
         sigma = self.sigma if sigma is None else sigma
+        self._check_tables(idd, sigma)
         if out is None:
             out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        nvox = self.shape[0] * self.shape[1] * self.shape[2]
+        _lib.check_arg(out, "out", nvox, torch.float32, self.device)
         with self._sched():
             nbytes = _lib.query("pbd_forward_workspace", ctypes.byref(self.field), self.precision)
             ws = self.ws.get("fwd", nbytes)
@@ -201,7 +210,12 @@ class DosePlan:
         didd = self.didd if didd is None else didd
         dsig = self.dsig if dsig is None else dsig
         with_range = with_range and didd is not None and dsig is not None
+        self._check_tables(idd, sigma)
+        if with_range:
+            self._check_tables(didd, dsig)
         g = grad_dose.to(self.device, torch.float32).contiguous()
+        _lib.check_arg(g, "grad_dose", self.shape[0] * self.shape[1] * self.shape[2],
+                       torch.float32, self.device)
         gw = torch.empty_like(w)
         gr = torch.zeros(w.shape[0], dtype=torch.float32, device=self.device) if with_range else None
         with self._sched():
@@ -224,6 +238,16 @@ class DosePlan:
         w = self._weights(w)
         o = outputs or self.alloc_outputs()
         with_range = self.didd is not None
+        nvox = self.shape[0] * self.shape[1] * self.shape[2]
+        f32, dev = torch.float32, self.device
+        _lib.check_arg(mask, "mask", nvox, f32, dev)
+        _lib.check_arg(presc, "presc", nvox, f32, dev)
+        _lib.check_arg(o["dose"], "outputs['dose']", nvox, f32, dev)
+        _lib.check_arg(o["grad_dose"], "outputs['grad_dose']", nvox, f32, dev)
+        _lib.check_arg(o["loss"], "outputs['loss']", 1, torch.float64, dev)
+        _lib.check_arg(o["grad_w"], "outputs['grad_w']", self.w.numel(), f32, dev)
+        if with_range:
+            _lib.check_arg(o["grad_range"], "outputs['grad_range']", self.w.shape[0], f32, dev)
         with self._sched():
             nbytes = _lib.query("pbd_loss_grad_workspace", ctypes.byref(self.field),
                                 self.precision)

@@ -88,8 +88,11 @@ class WedPlan:
             raise ValueError("wed must be a float64 tensor of the grid's shape")
         wt = self.w if w is None else torch.as_tensor(w, dtype=torch.float32,
                                                       device=self.device).contiguous()
+        _lib.check_arg(wt, "w", self.w.numel(), torch.float32, self.device)
         if out is None:
             out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        n = self.shape[0] * self.shape[1] * self.shape[2]
+        _lib.check_arg(out, "out", n, torch.float32, self.device)
         wd = wed.to(self.device).contiguous()
         _lib.call("pbd_forward_wed_curves", ctypes.byref(self.field), ctypes.byref(self.spec),
                   _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(wt), _lib.ptr(self.sigma),

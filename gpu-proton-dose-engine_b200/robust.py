@@ -168,6 +168,12 @@ class ScenarioBatch:
         ``batched`` (default: for the tensor-core precisions): every job's forward in one
         persistent launch and every adjoint in another (``pbd_loss_grad_batch``); otherwise
         one ``pbd_loss_grad`` call per job with a shared workspace."""
+        nvox = {p.grid.nz * p.grid.ny * p.grid.nx for p in self.problems}
+        if len(nvox) != 1:
+            raise ValueError("one mask and prescription need every field on the same grid")
+        n = nvox.pop()
+        _lib.check_arg(mask, "mask", n, self.torch.float32, self.device)
+        _lib.check_arg(presc, "presc", n, self.torch.float32, self.device)
         if not getattr(self, "grad_outputs", None):
             self.alloc_grad_outputs()
         if batched is None:

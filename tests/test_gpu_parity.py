@@ -342,3 +342,47 @@ def test_scenario_batch_matches_single(pb, torch):
     torch.cuda.synchronize()
     for d0, d1 in zip(doses, replay):
         assert torch.equal(d0, d1)
+
+
+def test_plans_refuse_mis_sized_tensors(pb, torch):
+    """Tensors the library would read or write through raw pointers are checked first: a
+    wrong size, dtype, device or layout raises ValueError before any launch."""
+    wl = pb.workloads.build_workload(0)
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    prob = pb.model.problem_from_workload(wl, energies=en)
+    plan = pb.engines.DosePlan(prob, tables="device")
+    g = prob.grid
+    shape = (g.nz, g.ny, g.nx)
+    ok = plan.forward()
+    bad_out = [torch.empty((g.nz, g.ny, g.nx - 1), device="cuda"),
+               torch.empty(shape, dtype=torch.float64, device="cuda"),
+               torch.empty((g.nz, g.nx, g.ny), device="cuda").transpose(1, 2),
+               torch.empty(shape)]
+    for out in bad_out:
+        with pytest.raises(ValueError):
+            plan.forward(out=out)
+    with pytest.raises(ValueError):
+        plan.forward(w=plan.w[:-1])
+    with pytest.raises(ValueError):
+        plan.forward(idd=plan.idd[:, :-1].contiguous())
+    with pytest.raises(ValueError):
+        plan.adjoint(torch.zeros((g.nz - 1, g.ny, g.nx), device="cuda"))
+    mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
+    m = torch.as_tensor(mask, device="cuda")
+    p = torch.as_tensor(presc, device="cuda")
+    with pytest.raises(ValueError):
+        plan.loss_grad(m.double(), p)
+    with pytest.raises(ValueError):
+        plan.loss_grad(m, p[:-1])
+    outs = plan.alloc_outputs()
+    outs["grad_w"] = outs["grad_w"][:-1]
+    with pytest.raises(ValueError):
+        plan.loss_grad(m, p, outputs=outs)
+    # the valid calls still work and agree
+    assert torch.equal(plan.forward(), ok)
+    wp = pb.hetero.WedPlan(prob)
+    wed = pb.hetero.wed_raytrace(np.ones(shape, dtype=np.float32), g)
+    with pytest.raises(ValueError):
+        wp.forward(wed, out=torch.empty((g.nz, g.ny, g.nx + 1), device="cuda"))
+    with pytest.raises(ValueError):
+        wp.forward(wed, w=np.ones(3, dtype=np.float32))
