@@ -102,6 +102,8 @@ class GammaPlan:
         ref = reference.contiguous()
         ev = evaluation.contiguous()
         nz, ny, nx = self.shape
+        _lib.check_arg(ref, "reference", nz * ny * nx, ref.dtype, self.device)
+        _lib.check_arg(ev, "evaluation", nz * ny * nx, ev.dtype, self.device)
         _lib.call("pbd_gamma_index", ctypes.byref(self.spec), nz, ny, nx, _lib.ptr(ref),
                   _lib.ptr(ev), dt, _lib.ptr(self.gamma), _lib.ptr(self.mask),
                   _lib.ptr(self.stats_dev), _lib.ptr(self.ws), self.ws.numel(),

@@ -149,6 +149,12 @@ def test_gamma_errors(pb):
     with pytest.raises(ValueError):
         # a normalisation dose with no positive reference voxel: nothing to evaluate
         pb.gamma.gamma_index(-np.ones((8, 8, 8)), z, ref_dose=1.0)
+    # a plan refuses doses that are not on its device
+    import torch
+    plan = pb.gamma.GammaPlan((8, 8, 8), pb.gamma.gamma_spec())
+    on_dev = torch.ones((8, 8, 8), dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        plan.run(torch.ones((8, 8, 8), dtype=torch.float64), on_dev)
     # all-equal doses: every gamma is 0
     one = np.ones((9, 10, 11))
     r = pb.gamma.gamma_index(one, one)
