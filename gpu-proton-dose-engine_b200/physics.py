@@ -125,10 +125,9 @@ class TableBuilder:
     def build(self, range_shift=None) -> DepthTables:
         """Enqueue the rebuild at CSDA ranges R0_l + range_shift_l (``range_shift``: a device
         float64 tensor of L entries, or None) on the current stream."""
-        if range_shift is not None and (range_shift.dtype != self.torch.float64
-                                        or range_shift.numel() != self.n_layers
-                                        or not range_shift.is_contiguous()):
-            raise ValueError("range_shift must be a contiguous float64 tensor of L entries")
+        if range_shift is not None:
+            _lib.check_arg(range_shift, "range_shift", self.n_layers, self.torch.float64,
+                           self.device)
         t = self.tables
         _lib.call("pbd_build_luts", ctypes.byref(self.spec), self.n_layers, _lib.ptr(self.energies),
                   _lib.ptr(range_shift), _lib.ptr(t.idd), _lib.ptr(t.sigma), _lib.ptr(t.didd_dr),
