@@ -226,10 +226,10 @@ def reference_arm(args):
     cpu_port_grad_eval(wl, tables, torch)          # first warm-up, also sizes the sample
     t_eval = time.perf_counter() - t0
     steps = max(1, min(args.steps, int(120.0 / max(t_eval, 1e-3))))
-    rate, n, el, cores, _ = run_cpu_port(wl, budget_s=0.0, max_evals=steps,
-                                         warmup=max(0, min(args.warmup, 2) - 1))
+    W = max(3, min(args.warmup, 5))                # warm-up evaluations, the first included
+    rate, n, el, cores, _ = run_cpu_port(wl, budget_s=0.0, max_evals=steps, warmup=W - 1)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": 1e3 * el / n,
+            "steps": n, "warmup": W, "ms_per_step": 1e3 * el / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": wl["name"], "grid": [128, 128, 128], "spots": 67240,
