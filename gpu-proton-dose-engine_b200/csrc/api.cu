@@ -320,7 +320,7 @@ struct WedCarve {
     float* lateral;      // (L, wed_lateral_stride) per-layer lateral maps
     void* curves;
     size_t curves_bytes;
-    void* batch;
+    void* batch;         // the lateral maps' forward: batch (FP32) or single-job workspace
     size_t batch_bytes;
 };
 
@@ -331,7 +331,12 @@ static int carve_wed(const pbd_field* f, const pbd_lut_spec* spec, int precision
     const int nb = L < PBD_MAX_JOBS ? L : PBD_MAX_JOBS;
     wed_jobs(f, 0, nb, nullptr, nullptr, nullptr, nullptr, jobs);
     size_t bb = 0, cb = 0;
-    PBD_TRY(pbd_forward_batch_workspace(jobs, nb, precision, &bb));
+    if (precision == PBD_PREC_FP32) {
+        PBD_TRY(pbd_forward_batch_workspace(jobs, nb, precision, &bb));
+    } else {
+        Ws fw;
+        PBD_TRY(carve_ws(f, true, false, false, precision, nullptr, fw, &bb));
+    }
     PBD_TRY(lut_curve_workspace(spec, L, &cb));
     Carve c(base);
     w.act = c.take<double>((size_t)L * f->nz);
@@ -798,24 +803,62 @@ int pbd_build_wed_curves(const pbd_lut_spec* spec, int n_layers, const double* e
                           (cudaStream_t)stream);
 }
 
-// Activity table, the per-layer lateral maps through the batched forward, then the combine.
+// Tensor-core precisions: every layer's lateral map (depth dose = the activity table) from
+// one launch of the forward in its per-layer-maps mode, so that a unit's layers share its
+// distance tables.  *fwd_err: the forward's error word.
+static int forward_layer_maps(const pbd_field* f, const float* w, const double* act,
+                              const double* sigma, float* lateral, size_t lstride, int precision,
+                              void* base, size_t bytes, cudaStream_t s, const int** fwd_err) {
+    size_t need = 0;
+    Ws ws;
+    PBD_TRY(carve_ws(f, true, false, false, precision, nullptr, ws, &need));
+    if (!base || bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_ws(f, true, false, false, precision, base, ws, &need));
+    JobPair p;
+    memset(&p, 0, sizeof(p));
+    p.n = 1;
+    JobDev& J = p.j[0];
+    fill_job(f, &J);
+    J.w = w; J.idd = act; J.sigma = sigma; J.dose = lateral;
+    J.layer_stride = lstride;
+    J.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
+    J.item_base = 0; J.max_items = ws.f_items;
+    J.partial = ws.fpart; J.nchunks = ws.fnch; J.arrive = ws.farr;
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    *fwd_err = ws.counters + 1;
+    // no poison pass here: the combine's poison pass reads this error word too
+    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
+                          ws.f_chunk, 0, precision, 0, s);
+}
+
+// Activity table, the per-layer lateral maps, then the combine.
 static int forward_wed_body(const pbd_field* f, const pbd_lut_spec* spec, const void* curves,
                             size_t curves_bytes, const float* w, const double* sigma,
                             const double* wed, float* dose, int precision, const WedCarve& wc,
                             void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nslice = (size_t)f->ny * f->nx;
+    const size_t lstride = wed_lateral_stride(f);
     PBD_TRY(lut_wed_activity(spec, f->n_layers, curves, curves_bytes, wed, f->nz, nslice, wc.act,
                              s));
-    pbd_job jobs[PBD_MAX_JOBS];
-    for (int l0 = 0; l0 < f->n_layers; l0 += PBD_MAX_JOBS) {
-        const int n = f->n_layers - l0 < PBD_MAX_JOBS ? f->n_layers - l0 : PBD_MAX_JOBS;
-        wed_jobs(f, l0, n, w, sigma, wc.act, wc.lateral, jobs);
-        PBD_TRY(pbd_forward_batch(jobs, n, precision, wc.batch, wc.batch_bytes, stream));
+    const int* fwd_err = nullptr;
+    if (precision != PBD_PREC_FP32) {
+        PBD_TRY(forward_layer_maps(f, w, wc.act, sigma, wc.lateral, lstride, precision, wc.batch,
+                                   wc.batch_bytes, s, &fwd_err));
+    } else {
+        // FP32: one single-layer job per layer through the batched forward (its own poison)
+        pbd_job jobs[PBD_MAX_JOBS];
+        for (int l0 = 0; l0 < f->n_layers; l0 += PBD_MAX_JOBS) {
+            const int n = f->n_layers - l0 < PBD_MAX_JOBS ? f->n_layers - l0 : PBD_MAX_JOBS;
+            wed_jobs(f, l0, n, w, sigma, wc.act, wc.lateral, jobs);
+            PBD_TRY(pbd_forward_batch(jobs, n, precision, wc.batch, wc.batch_bytes, stream));
+        }
     }
     PBD_TRY(cuda_rc(cudaMemsetAsync(wc.err, 0, sizeof(int), s)));
-    return lut_wed_combine(spec, f->n_layers, wc.lateral, wed_lateral_stride(f), wed,
-                           (size_t)f->nz * nslice, dose, wc.err, curves, curves_bytes, s);
+    return lut_wed_combine(spec, f->n_layers, wc.lateral, lstride, wed, (size_t)f->nz * nslice,
+                           dose, wc.err, fwd_err, curves, curves_bytes, s);
 }
 
 static int wed_setup(const pbd_field* f, const pbd_lut_spec* spec, int precision, void* workspace,

@@ -622,9 +622,10 @@ __global__ void __launch_bounds__(kCmbThreads, 5) wed_combine_kernel(
     }
 }
 
-// After a combine whose wait ran out: the whole dose is invalid, NaN.
-__global__ void wed_poison_kernel(float* dose, size_t nvox, const int* err) {
-    if (*err == 0) return;
+// After a combine (or the lateral maps' forward, err2) whose wait ran out: the whole dose is
+// invalid, NaN.
+__global__ void wed_poison_kernel(float* dose, size_t nvox, const int* err, const int* err2) {
+    if (*err == 0 && (err2 == nullptr || *err2 == 0)) return;
     for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
          v += (size_t)gridDim.x * blockDim.x)
         dose[v] = __int_as_float(0x7fc00000);
@@ -943,8 +944,8 @@ int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, si
 }
 
 int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, size_t lstride,
-                    const double* wed, size_t nvox, float* dose, int* err, const void* curves,
-                    size_t curves_bytes, cudaStream_t st) {
+                    const double* wed, size_t nvox, float* dose, int* err, const int* err2,
+                    const void* curves, size_t curves_bytes, cudaStream_t st) {
     PBD_TRY(validate_spec(s, n_layers));
     if (!lateral || !wed || !dose || !err) return PBD_ERR_NULL_ARG;
     // 1-D bulk copies: 16-byte aligned rows, the tile's copy rounded up to 16 bytes inside
@@ -970,7 +971,7 @@ int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, s
                                                                     dose, err);
     PBD_LAUNCH_CHECK();
     const int pb = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 4);
-    wed_poison_kernel<<<std::max(pb, 1), 256, 0, st>>>(dose, nvox, err);
+    wed_poison_kernel<<<std::max(pb, 1), 256, 0, st>>>(dose, nvox, err, err2);
     PBD_LAUNCH_CHECK();
     count_launch(2);
     return PBD_OK;

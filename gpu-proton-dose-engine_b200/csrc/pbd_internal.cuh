@@ -44,6 +44,9 @@ struct JobDev {
     float* grad_range;            // (nl)
     float* dc;                    // (nl, nz) dL/dIDD
     float* dsg;                   // (nl, nz) dL/dsigma
+    size_t layer_stride;          // tensor-core forward: > 0 writes each layer's own dose
+                                  // (its lateral map times idd) to dose + l * layer_stride
+                                  // instead of the sum over layers; 0 = the dose
 };
 
 struct FwdItem { int job, z, ty, tx, lb, le, chunk, cost; };
@@ -189,16 +192,17 @@ int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st);
 // smoothed depth curves and their interval slopes into it; activity fills the (layer, slice)
 // table act (L, nz) from a WED map; combine forms dose = sum_l IDD_l(WED) * lateral_l with
 // layer l's lateral map at lateral + l * lstride (16-byte aligned, lstride a multiple of 4
-// floats, >= nvox rounded up to 4) and an error word err (set when a bounded wait ran out;
-// the dose is then NaN); the WED ray trace along +z.
+// floats, >= nvox rounded up to 4), its error word err (set when a bounded wait ran out) and
+// optionally the lateral maps' forward error word err2 (either one makes the dose NaN); the
+// WED ray trace along +z.
 int lut_curve_workspace(const pbd_lut_spec* s, int n_layers, size_t* bytes);
 int lut_wed_curves(const pbd_lut_spec* s, int n_layers, const double* energies,
                    const double* shift, void* curves, size_t curves_bytes, cudaStream_t st);
 int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, size_t curves_bytes,
                      const double* wed, int nz, size_t nslice, double* act, cudaStream_t st);
 int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, size_t lstride,
-                    const double* wed, size_t nvox, float* dose, int* err, const void* curves,
-                    size_t curves_bytes, cudaStream_t st);
+                    const double* wed, size_t nvox, float* dose, int* err, const int* err2,
+                    const void* curves, size_t curves_bytes, cudaStream_t st);
 int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
                      cudaStream_t st);
 

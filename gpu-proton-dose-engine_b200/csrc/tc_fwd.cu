@@ -42,6 +42,10 @@
 // tile, warp) arrival counter) sums the partials in chunk order -- deterministic whichever
 // CTA gets there -- and writes the dose.  With the masked quadratic loss the same writer
 // forms dL/dD = 2 m (D - P) and an FP64 partial sum of m (D - P)^2 for its rows.
+// Per-layer maps (a job with layer_stride > 0, no loss): every step is its own output --
+// the layer's dose rows go to dose + l * layer_stride -- while the unit's steps still share
+// its squared-distance tables (kTab on the first step only); slices no layer reaches are
+// not written.
 //
 // Every wait is bounded (2 s of %globaltimer).  A warp whose wait runs out sets the error
 // word and leaves its loop; the waits of the others then run out in turn.  The dose is
@@ -78,7 +82,9 @@ constexpr uint32_t kCols = 512;
 // [256, 256 + N1) / [320, 320 + N1), stage-1 A operand hi / lo [384, +K1) / [448, +K1)
 constexpr uint32_t kColD = 0, kColS = 128, kColUb = 256, kColUs = 320, kColAh = 384, kColAl = 448;
 
-enum : int { kFirst = 1, kLast = 2, kEnd = 4, kZero = 8 };
+// kFirst / kLast: the step opens / closes an accumulation (and its output); kTab: the step
+// builds the unit's squared-distance tables.
+enum : int { kFirst = 1, kLast = 2, kEnd = 4, kZero = 8, kTab = 16 };
 
 struct Step {
     int job, z, tile, l;
@@ -100,6 +106,7 @@ struct Params {
 // ------------------------------------------------------------------------------------------
 // Scheduler warp: units -> steps.
 // ------------------------------------------------------------------------------------------
+template <bool MAPS>
 __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint64_t* full, uint64_t* empty) {
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
@@ -141,7 +148,9 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
             tot += __popc(__ballot_sync(FULL, a));
         }
         if (tot == 0) {
-            if (c == 0) {   // a slice no layer reaches: the math warps write zeros (and loss)
+            // a slice no layer reaches: the math warps write zeros (and loss); per-layer
+            // maps have nothing to write
+            if (c == 0 && !MAPS) {
                 Step st{};
                 st.job = job; st.z = z; st.tile = tile;
                 st.nch = 1; st.flags = kFirst | kLast | kZero;
@@ -167,7 +176,8 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
                 st.chunk = c; st.nch = nch;
                 st.nsx = J.nsx; st.nsy = J.nsy;
                 st.w = J.w + (size_t)l * J.nsy * J.nsx;
-                st.flags = (my == r0 ? kFirst : 0) | (my == r1 - 1 ? kLast : 0);
+                st.flags = MAPS ? (kFirst | kLast | (my == r0 ? kTab : 0))
+                                : ((my == r0 ? kFirst | kTab : 0) | (my == r1 - 1 ? kLast : 0));
                 st.a2 = (float)(kLog2e / (2.0 * s * s));
                 st.scale = (float)(iv * kInv2Pi / (s * s));
             }
@@ -409,7 +419,7 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-template <int MODE>
+template <int MODE, bool MAPS>
 __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uint8_t* smem, uint32_t tb,
                            const Step* ring, uint64_t* full, uint64_t* empty, uint64_t* bars) {
     using Pr = Prec<MODE>;
@@ -487,7 +497,25 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
         const int y = ty * kTile + trow, xb = tx * kTile + half * 64;
         const int slot = (st.z * (J.ntx * J.nty) + st.tile) * kMathWarps + warp;
-        if (st.nch == 1) {
+        if constexpr (MAPS) {
+            // per-layer maps: this step's layer, written whole
+            if (y < J.ny) {
+                float* d = J.dose + (size_t)st.l * J.layer_stride +
+                           ((size_t)st.z * J.ny + y) * J.nx + xb;
+                const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
+#pragma unroll
+                for (int q = 0; q < 64; q += 4) {
+                    if (vec) {
+                        *reinterpret_cast<float4*>(d + q) =
+                            make_float4(dsum[q], dsum[q + 1], dsum[q + 2], dsum[q + 3]);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (xb + q + r < J.nx) d[q + r] = dsum[q + r];
+                    }
+                }
+            }
+        } else if (st.nch == 1) {
             const double ls = warp_sum(write_final(J, st.z, y, xb, dsum, P.with_loss));
             if (P.with_loss && lane == 0) J.loss_part[slot] = ls;
         } else {
@@ -584,7 +612,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             }
         }
         // ---- unit start: this thread's squared distances (FP64 differences) ----
-        if (cur.flags & kFirst) {
+        if (cur.flags & kTab) {
             const int ty = cur.tile / J.ntx, tx = cur.tile % J.ntx;
             const double cx = 0.5 * (double)(nsx - 1), cy = 0.5 * (double)(nsy - 1);
 #pragma unroll
@@ -770,7 +798,9 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
     if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
 }
 
-template <int MODE>
+// MAPS: the per-layer-maps mode, a separate instantiation so that the dose kernel's code and
+// registers are those of the plain build.
+template <int MODE, bool MAPS>
 __global__ void __launch_bounds__(kThreads, 1) fwd_tc_kernel(Params P) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t full[kRing];
@@ -805,7 +835,7 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc_kernel(Params P) {
     if (warp >= kMathWarps) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
         if (warp == kSchedWarp) {
-            scheduler_warp(P, ring, full, empty);
+            scheduler_warp<MAPS>(P, ring, full, empty);
         } else if (warp - kMmaWarp < kIssuers) {
             const Layout L = make_layout<MODE>(P.K1, P.N1, P.na2);
             mma_warp<MODE>(P, L, tc::smem_u32(smem), tmem_base_s, warp - kMmaWarp, ring, full,
@@ -814,7 +844,7 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc_kernel(Params P) {
     } else {
         asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kMathRegs));
         const Layout L = make_layout<MODE>(P.K1, P.N1, P.na2);
-        math_warps<MODE>(P, L, smem, tmem_base_s, ring, full, empty, bars);
+        math_warps<MODE, MAPS>(P, L, smem, tmem_base_s, ring, full, empty, bars);
     }
 
     tc::fence_before_sync();
@@ -857,7 +887,7 @@ size_t smem_bytes(int K1, int N1, int na2) {
            (size_t)(ty4 + tx4) * kMath * 16u;
 }
 
-template <int MODE>
+template <int MODE, bool MAPS>
 int launch_mode(const Params& P0, cudaStream_t s) {
     static thread_local int max_dyn = 0;
     if (max_dyn == 0) {
@@ -866,12 +896,12 @@ int launch_mode(const Params& P0, cudaStream_t s) {
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
                 cudaSuccess ||
-            cudaFuncGetAttributes(&fa, fwd_tc_kernel<MODE>) != cudaSuccess)
+            cudaFuncGetAttributes(&fa, fwd_tc_kernel<MODE, MAPS>) != cudaSuccess)
             return PBD_ERR_CUDA;
         // the setmaxnreg split needs the full launch allotment, or its increase never returns
         if (fa.numRegs < kLaunchRegsNeeded) return PBD_ERR_UNSUPPORTED;
         const int avail = optin - (int)fa.sharedSizeBytes;
-        if (avail <= 0 || cudaFuncSetAttribute(fwd_tc_kernel<MODE>,
+        if (avail <= 0 || cudaFuncSetAttribute(fwd_tc_kernel<MODE, MAPS>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                avail) != cudaSuccess)
             return PBD_ERR_NO_SMEM;
@@ -891,7 +921,7 @@ int launch_mode(const Params& P0, cudaStream_t s) {
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
     const int grid = std::max(1, std::min(P.n_units, num_sms()));
     prof_mark(kProfFwd, 0, s);
-    fwd_tc_kernel<MODE><<<grid, kThreads, smem, s>>>(P);
+    fwd_tc_kernel<MODE, MAPS><<<grid, kThreads, smem, s>>>(P);
     PBD_LAUNCH_CHECK();
     prof_mark(kProfFwd, 1, s);
     return PBD_OK;
@@ -937,12 +967,25 @@ int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
         P.N1 = std::max(P.N1, n1);
     }
     PBD_TRY(tc_forward_units(jobs_host, n_jobs, chunk, &P.cmax, &P.tmax, &P.n_units));
+    // per-layer maps (layer_stride > 0, no loss) or the dose: every job of a launch alike
+    const bool maps = jobs_host[0].layer_stride != 0;
+    for (int j = 1; j < n_jobs; ++j)
+        if ((jobs_host[j].layer_stride != 0) != maps) return PBD_ERR_UNSUPPORTED;
+    if (maps && with_loss) return PBD_ERR_UNSUPPORTED;
     int rc = PBD_ERR_BAD_VALUE;
     switch (precision) {
-        case PBD_PREC_TF32X3: rc = launch_mode<PBD_PREC_TF32X3>(P, s); break;
-        case PBD_PREC_TF32: rc = launch_mode<PBD_PREC_TF32>(P, s); break;
-        case PBD_PREC_BF16X3: rc = launch_mode<PBD_PREC_BF16X3>(P, s); break;
-        case PBD_PREC_BF16: rc = launch_mode<PBD_PREC_BF16>(P, s); break;
+        case PBD_PREC_TF32X3:
+            rc = maps ? launch_mode<PBD_PREC_TF32X3, true>(P, s) : launch_mode<PBD_PREC_TF32X3, false>(P, s);
+            break;
+        case PBD_PREC_TF32:
+            rc = maps ? launch_mode<PBD_PREC_TF32, true>(P, s) : launch_mode<PBD_PREC_TF32, false>(P, s);
+            break;
+        case PBD_PREC_BF16X3:
+            rc = maps ? launch_mode<PBD_PREC_BF16X3, true>(P, s) : launch_mode<PBD_PREC_BF16X3, false>(P, s);
+            break;
+        case PBD_PREC_BF16:
+            rc = maps ? launch_mode<PBD_PREC_BF16, true>(P, s) : launch_mode<PBD_PREC_BF16, false>(P, s);
+            break;
         default: break;
     }
     PBD_TRY(rc);

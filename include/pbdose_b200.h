@@ -221,7 +221,8 @@ PBD_API int pbd_loss_grad_batch(const pbd_grad_job *jobs, int n_jobs, int precis
  *   D[z,y,x] = sum_l IDD_l(WED[z,y,x]) * sum_{j,i} Gy_l(z)[y,j] W_l[j,i] Gx_l(z)[x,i]
  * with the lateral widths sigma (L, nz) of water at the geometric depth (the tables of
  * pbd_build_luts).  spec / energies / range_shift: as for pbd_build_luts.  The per-layer
- * lateral maps go through the batched forward.
+ * lateral maps come from one launch of the tensor-core forward that writes every layer's map
+ * (PBD_PREC_FP32: single-layer jobs of the batched forward).
  * pbd_build_wed_curves: the per-layer smoothed depth curves and their interval slopes, built
  * once into an opaque device blob of pbd_wed_curves_workspace bytes; pbd_forward_wed_curves
  * computes the dose from such a blob (built with the same spec and n_layers) without
