@@ -530,8 +530,8 @@ def luts_bench(args):
 def hetero_bench(args):
     """The clinical field (128^3, 41x41x40) in a slab phantom -- bone (1.6) from 3 to 5 cm,
     lung (0.25) from 7 to 10 cm on one side: the WED ray trace and the heterogeneous forward
-    (activity table, per-layer lateral maps in one batched tensor-core launch, then the depth
-    doses at the WED) from the plan's depth curves, built once per plan like the homogeneous
+    (activity table, every layer's lateral map from one tensor-core forward launch, then the
+    depth doses at the WED) from the plan's depth curves, built once per plan like the homogeneous
     plan's tables and timed as their own leg (wed_curves), each replayed from a CUDA graph, L2
     flushed between steps; the homogeneous forward of the same field beside them.  CPU
     baseline: the oracle's float64 heterogeneous dose."""
