@@ -69,3 +69,24 @@ def test_wed_entry_points_validate_before_device_work():
     nul = list(cargs)
     nul[2] = None                                   # no curve blob
     assert lib.pbd_forward_wed_curves(*nul, fake, sz.value, None) == -1
+
+
+def test_oracle_dose_in_water_equals_reference_dose():
+    """In water the oracle's whole heterogeneous chain -- the WED ray trace of rho = 1, then
+    the depth dose at that WED times each layer's lateral dose -- gives the reference's own
+    float64 dose of the 32 x 32 x 64 workload (tests/golden/dose_cfg0.npz, made by the
+    reference's separable_numpy with its own tables)."""
+    wl = load_pkg().workloads.build_workload(0)
+    lut = golden("luts_cfg0.npz")
+    ref = golden("dose_cfg0.npz")
+    gr = wl["grid"]
+    rho = np.ones((gr["nz"], gr["ny"], gr["nx"]))
+    wed = hr.wed_ref(rho, gr["oz"], gr["dz"])
+    assert np.max(np.abs(wed[:, 0, 0] - lut["z"])) <= 1e-13
+    xv = gr["ox"] + np.arange(gr["nx"]) * gr["dx"]
+    yv = gr["oy"] + np.arange(gr["ny"]) * gr["dy"]
+    xs = wl["x0"] + (np.arange(wl["n_sx"]) - (wl["n_sx"] - 1) / 2.0) * wl["spot_pitch"]
+    ys = wl["y0"] + (np.arange(wl["n_sy"]) - (wl["n_sy"] - 1) / 2.0) * wl["spot_pitch"]
+    d = hr.dose_ref(xv, yv, xs, ys, wl["weights"], lut["energies"], lut["sigma"], wed)
+    err = np.max(np.abs(d - ref["dose"])) / np.max(np.abs(ref["dose"]))
+    assert err < 1e-11, err
