@@ -81,9 +81,12 @@ class WedPlan:
         self.shape = (g.nz, g.ny, g.nx)
 
     def forward(self, wed, w=None, out=None):
-        """Dose (float32 device tensor (nz, ny, nx)) for the WED map ``wed`` (float64 device
-        tensor of the grid's shape, e.g. from ``wed_raytrace``), on the current stream."""
+        """Dose (float32 device tensor (nz, ny, nx)) for the WED map ``wed`` (float64 tensor or
+        array of the grid's shape, e.g. from ``wed_raytrace``; host data is uploaded), on the
+        current stream."""
         torch = self.torch
+        if not torch.is_tensor(wed):
+            wed = torch.as_tensor(np.ascontiguousarray(wed, dtype=np.float64))
         if tuple(wed.shape) != self.shape or wed.dtype != torch.float64:
             raise ValueError("wed must be a float64 tensor of the grid's shape")
         wt = self.w if w is None else torch.as_tensor(w, dtype=torch.float32,

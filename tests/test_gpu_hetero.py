@@ -51,10 +51,13 @@ def test_water_reproduces_homogeneous_dose(pb):
     zc = np.maximum(g.oz + np.arange(g.nz) * g.dz, 0.0)[:, None, None]
     assert np.max(np.abs(wed.cpu().numpy() - zc)) <= 1e-12
     for prec in ("fp32", "tf32x3"):
-        d_wed = pb.hetero.WedPlan(prob, precision=prec).forward(wed)
+        plan = pb.hetero.WedPlan(prob, precision=prec)
+        d_wed = plan.forward(wed)
         d_ref = pb.engines.DosePlan(prob, tables="device", precision=prec).forward()
         torch.cuda.synchronize()
         assert rel(d_wed.cpu().numpy(), d_ref.cpu().numpy()) < 1e-6, prec
+        # a host WED map is uploaded: the same dose
+        assert torch.equal(plan.forward(wed.cpu().numpy()), d_wed), prec
 
 
 def test_slab_phantom_vs_oracle(pb):
