@@ -145,3 +145,28 @@ def test_ragged_grid_random_medium_vs_oracle(pb):
         err = rel(d, want)
         print(f"ragged {prec}: heterogeneous dose max rel err {err:.2e}")
         assert err < 1e-6, prec
+
+
+def test_nan_and_out_of_range_wed(pb):
+    """A NaN WED gives a NaN dose at that voxel only (np.interp propagates NaN); the other
+    voxels -- the NaN's tile included, which then streams every layer -- keep their values bit
+    for bit.  WED maps beyond every layer's curve, or negative, give a dose of exactly 0 (no
+    (layer, slice) is active, nothing is written or read)."""
+    import torch
+    wl, en, prob = _cfg0(pb)
+    g = prob.grid
+    wed = pb.hetero.wed_raytrace(np.ones((g.nz, g.ny, g.nx), dtype=np.float32), g)
+    plan = pb.hetero.WedPlan(prob, precision="tf32x3")
+    base = plan.forward(wed).clone()
+    w2 = wed.clone()
+    w2[5, 3, 4] = float("nan")
+    d = plan.forward(w2)
+    torch.cuda.synchronize()
+    nan = torch.isnan(d)
+    assert nan.sum().item() == 1 and bool(nan[5, 3, 4])
+    keep = ~nan
+    assert torch.equal(d[keep], base[keep])
+    for fill in (1e3, -1.0):
+        z = plan.forward(torch.full_like(wed, fill))
+        torch.cuda.synchronize()
+        assert torch.count_nonzero(z).item() == 0, fill
