@@ -205,3 +205,25 @@ def test_no_cpu_path(pb):
         pb.engines.torch_separable(prob, "cuda")
     with pytest.raises(RuntimeError):
         pb.physics.csda_range(100.0)
+
+
+def test_tensor_argument_checks():
+    """The host-side check every plan applies to a tensor it hands to the library: refused
+    unless it has the expected element count, dtype, device and a contiguous layout."""
+    import torch
+    pkg = load_pkg()
+    chk, cpu = pkg._lib.check_arg, torch.device("cpu")
+    t = torch.zeros((4, 5), dtype=torch.float32)
+    assert chk(t, "t", 20, torch.float32, cpu) is t
+    with pytest.raises(ValueError):
+        chk(t, "t", 21, torch.float32, cpu)
+    with pytest.raises(ValueError):
+        chk(t.double(), "t", 20, torch.float32, cpu)
+    with pytest.raises(ValueError):
+        chk(t.t(), "t", 20, torch.float32, cpu)
+    with pytest.raises(TypeError):
+        chk(np.zeros(20, dtype=np.float32), "t", 20, torch.float32, cpu)
+    with pytest.raises(ValueError):
+        chk(t, "t", 20, torch.float32, torch.device("cuda", 0))
+    assert pkg._lib.same_device(cpu, torch.device("cpu"))
+    assert not pkg._lib.same_device(cpu, torch.device("cuda"))
