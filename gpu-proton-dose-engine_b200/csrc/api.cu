@@ -895,6 +895,72 @@ int pbd_forward_wed_curves(const pbd_field* f, const pbd_lut_spec* spec, const v
                             stream);
 }
 
+// ---- heterogeneous media: dL/dW -----------------------------------------------------
+struct WedAdjCarve {
+    double* act;         // (L, nz) activity table
+    float* maps;         // (L, wed_lateral_stride) dL/dD times each layer's depth dose
+    void* adj;           // one single-layer adjoint's workspace, reused layer after layer
+    size_t adj_bytes;
+};
+
+static int carve_wed_adj(const pbd_field* f, int precision, void* base, WedAdjCarve& w,
+                         size_t* used) {
+    pbd_field f1 = *f;
+    f1.n_layers = 1;
+    size_t ab = 0;
+    PBD_TRY(pbd_adjoint_workspace(&f1, precision, &ab));
+    Carve c(base);
+    w.act = c.take<double>((size_t)f->n_layers * f->nz);
+    w.maps = c.take<float>((size_t)f->n_layers * wed_lateral_stride(f));
+    w.adj = c.take<char>(ab);
+    w.adj_bytes = ab;
+    *used = c.used + 256;
+    return PBD_OK;
+}
+
+int pbd_adjoint_wed_workspace(const pbd_field* f, const pbd_lut_spec* spec, int precision,
+                              size_t* bytes) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    PBD_TRY(adjoint_supported(f));
+    if (!spec || !bytes) return PBD_ERR_NULL_ARG;
+    WedAdjCarve w;
+    return carve_wed_adj(f, precision, nullptr, w, bytes);
+}
+
+int pbd_adjoint_wed(const pbd_field* f, const pbd_lut_spec* spec, const void* curves,
+                    size_t curves_bytes, const float* w, const double* sigma, const double* wed,
+                    const float* grad_dose, float* grad_w, int precision, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+    if (!f || !spec || !curves || !w || !sigma || !wed || !grad_dose || !grad_w)
+        return PBD_ERR_NULL_ARG;
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    PBD_TRY(adjoint_supported(f));
+    WedAdjCarve wc;
+    size_t need = 0;
+    PBD_TRY(carve_wed_adj(f, precision, nullptr, wc, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_wed_adj(f, precision, workspace, wc, &need));
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nslice = (size_t)f->ny * f->nx, nvox = (size_t)f->nz * nslice;
+    const size_t lstride = wed_lateral_stride(f);
+    PBD_TRY(lut_wed_activity(spec, f->n_layers, curves, curves_bytes, wed, f->nz, nslice, wc.act,
+                             s));
+    PBD_TRY(lut_wed_grad_maps(spec, f->n_layers, curves, curves_bytes, grad_dose, wed, nvox,
+                              lstride, wc.maps, s));
+    // layer l: the adjoint of its lateral map with depth dose 1 on its active slices
+    pbd_field f1 = *f;
+    f1.n_layers = 1;
+    const size_t per = (size_t)f->n_sy * f->n_sx;
+    for (int l = 0; l < f->n_layers; ++l)
+        PBD_TRY(pbd_adjoint(&f1, w + (size_t)l * per, wc.act + (size_t)l * f->nz,
+                            sigma + (size_t)l * f->nz, nullptr, nullptr,
+                            wc.maps + (size_t)l * lstride, grad_w + (size_t)l * per, nullptr,
+                            precision, wc.adj, wc.adj_bytes, stream));
+    return PBD_OK;
+}
+
 int pbd_loss_grad_batch_workspace(const pbd_grad_job* jobs, int n_jobs, int precision,
                                   size_t* bytes) {
     if (!bytes) return PBD_ERR_NULL_ARG;

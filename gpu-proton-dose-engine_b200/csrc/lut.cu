@@ -631,6 +631,45 @@ __global__ void wed_poison_kernel(float* dose, size_t nvox, const int* err, cons
         dose[v] = __int_as_float(0x7fc00000);
 }
 
+// The heterogeneous dose's dL/dD seen by layer l: maps[l * lstride + v] = IDD_l(WED[v]) *
+// grad[v] (FP64 product, rounded once to FP32), 0 outside the curve.  The adjoint of layer l
+// with this map and depth dose 1 on its active slices is dL/dW_l.  Every (layer, voxel) entry
+// is written.
+__global__ void __launch_bounds__(256) wed_grad_maps_kernel(LutDims dm, const LayerScal* scal,
+                                                            const double2* pts, const float* grad,
+                                                            const double* wed, size_t nvox,
+                                                            int n_layers, size_t lstride,
+                                                            float* maps) {
+    __shared__ double zmax[kWedLayers], stp[kWedLayers], istp[kWedLayers];
+    for (int l = threadIdx.x; l < n_layers && l < kWedLayers; l += blockDim.x) {
+        zmax[l] = scal[l].zmax;
+        stp[l] = (scal[l].zmax - 0.0) / (double)(dm.n_idd - 1);
+        istp[l] = 1.0 / stp[l];
+    }
+    __syncthreads();
+    const int n = dm.n_idd;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (size_t)gridDim.x * blockDim.x) {
+        const double d = wed[v];
+        const double g = (double)grad[v];
+        for (int l = 0; l < n_layers; ++l) {
+            const double zm = l < kWedLayers ? zmax[l] : scal[l].zmax;
+            float out = 0.0f;
+            if (!(d < 0.0 || d > zm)) {
+                const double st = l < kWedLayers ? stp[l] : (zm - 0.0) / (double)(n - 1);
+                const double is = l < kWedLayers ? istp[l] : 1.0 / st;
+                int lo = 0;
+                double x0 = 0.0;
+                locate_lin(d, 0.0, zm, n, st, is, lo, x0);
+                const double2 pt = __ldg(pts + (size_t)l * n + lo);
+                const double idd = x0 == d ? pt.x : pt.y * (d - x0) + pt.x;
+                out = (float)(idd * g);
+            }
+            maps[(size_t)l * lstride + v] = out;
+        }
+    }
+}
+
 // Curve points of the smoothed depth curves: {fp[k], slope_k} with slope_k = (fp[k+1] - fp[k])
 // / (x[k+1] - x[k]) on the grid linspace(0, zmax, n) -- the operands and the single rounding
 // of np.interp's slope (and of interp_lin) -- and 0 at the last point.  Value and slope share a
@@ -974,6 +1013,24 @@ int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, s
     wed_poison_kernel<<<std::max(pb, 1), 256, 0, st>>>(dose, nvox, err, err2);
     PBD_LAUNCH_CHECK();
     count_launch(2);
+    return PBD_OK;
+}
+
+int lut_wed_grad_maps(const pbd_lut_spec* s, int n_layers, const void* curves,
+                      size_t curves_bytes, const float* grad, const double* wed, size_t nvox,
+                      size_t lstride, float* maps, cudaStream_t st) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!grad || !wed || !maps) return PBD_ERR_NULL_ARG;
+    if (lstride < nvox) return PBD_ERR_BAD_VALUE;
+    LutDims dm;
+    LutWs w;
+    double2* pts = nullptr;
+    PBD_TRY(wed_dims(s, n_layers, curves, curves_bytes, dm, w, pts));
+    const int blocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 8);
+    wed_grad_maps_kernel<<<std::max(blocks, 1), 256, 0, st>>>(dm, w.scal, pts, grad, wed, nvox,
+                                                              n_layers, lstride, maps);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
     return PBD_OK;
 }
 

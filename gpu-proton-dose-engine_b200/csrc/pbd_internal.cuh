@@ -203,6 +203,11 @@ int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, si
 int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, size_t lstride,
                     const double* wed, size_t nvox, float* dose, int* err, const int* err2,
                     const void* curves, size_t curves_bytes, cudaStream_t st);
+// maps (L, lstride): dL/dD times each layer's depth dose at the WED (the heterogeneous
+// adjoint's per-layer input).
+int lut_wed_grad_maps(const pbd_lut_spec* s, int n_layers, const void* curves,
+                      size_t curves_bytes, const float* grad, const double* wed, size_t nvox,
+                      size_t lstride, float* maps, cudaStream_t st);
 int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
                      cudaStream_t st);
 

@@ -13,7 +13,8 @@ implemented.  Here, on the device:
   as the depth tables (physics.py:328-387), the lateral widths of water at the geometric
   depth (a broad-beam ray-casting approximation; the lateral scattering in the material is
   not modelled) (``pbd_build_wed_curves`` once, then ``pbd_forward_wed_curves``).  In water it
-  reproduces the homogeneous dose.
+  reproduces the homogeneous dose.  ``WedPlan(problem).adjoint(grad_dose, wed)`` gives dL/dW
+  (``pbd_adjoint_wed``), for plan optimisation in the medium.
 """
 from __future__ import annotations
 
@@ -102,6 +103,38 @@ class WedPlan:
                   _lib.ptr(wd), _lib.ptr(out), self.precision, _lib.ptr(self.ws),
                   self.ws.numel(), _lib.stream_handle(self.device))
         return out
+
+
+    def _wed(self, wed):
+        torch = self.torch
+        if not torch.is_tensor(wed):
+            wed = torch.as_tensor(np.ascontiguousarray(wed, dtype=np.float64))
+        if tuple(wed.shape) != self.shape or wed.dtype != torch.float64:
+            raise ValueError("wed must be a float64 tensor of the grid's shape")
+        return wed.to(self.device).contiguous()
+
+    def adjoint(self, grad_dose, wed, w=None):
+        """dL/dW (float32 device tensor (L, nsy, nsx)) of the heterogeneous dose for the
+        dL/dD ``grad_dose`` ((nz, ny, nx)) and the WED map ``wed`` (``pbd_adjoint_wed``)."""
+        torch = self.torch
+        wd = self._wed(wed)
+        wt = self.w if w is None else torch.as_tensor(w, dtype=torch.float32,
+                                                      device=self.device).contiguous()
+        _lib.check_arg(wt, "w", self.w.numel(), torch.float32, self.device)
+        g = torch.as_tensor(grad_dose).to(self.device, torch.float32).contiguous()
+        n = self.shape[0] * self.shape[1] * self.shape[2]
+        _lib.check_arg(g, "grad_dose", n, torch.float32, self.device)
+        if getattr(self, "adj_ws", None) is None:
+            nbytes = _lib.query("pbd_adjoint_wed_workspace", ctypes.byref(self.field),
+                                ctypes.byref(self.spec), self.precision)
+            self.adj_ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        gw = torch.empty_like(self.w)
+        _lib.call("pbd_adjoint_wed", ctypes.byref(self.field), ctypes.byref(self.spec),
+                  _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(wt), _lib.ptr(self.sigma),
+                  _lib.ptr(wd), _lib.ptr(g), _lib.ptr(gw), self.precision, _lib.ptr(self.adj_ws),
+                  self.adj_ws.numel(), _lib.stream_handle(self.device))
+        self._keep = (wd, g, wt)
+        return gw
 
 
 def dose_heterogeneous(problem, rho, *, precision: str = "tf32x3", device=None):

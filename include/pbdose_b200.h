@@ -246,6 +246,18 @@ PBD_API int pbd_forward_wed_curves(const pbd_field *f, const pbd_lut_spec *spec,
                                    int precision, void *workspace, size_t workspace_bytes,
                                    void *stream);
 
+/* dL/dW of the heterogeneous dose for a given dL/dD (grad_dose, (nz, ny, nx) float32):
+ * grad_w (L, nsy, nsx) float32, sum over voxels of grad_dose * IDD_l(WED) * dLateral_l/dW_l --
+ * the adjoint of pbd_forward_wed_curves (same field, spec, curve blob, w, sigma, wed).  No
+ * counterpart in the reference.  Per layer: dL/dD times the layer's depth dose at the WED,
+ * then the layer's adjoint (the same kernels as pbd_adjoint). */
+PBD_API int pbd_adjoint_wed_workspace(const pbd_field *f, const pbd_lut_spec *spec, int precision,
+                                      size_t *bytes);
+PBD_API int pbd_adjoint_wed(const pbd_field *f, const pbd_lut_spec *spec, const void *curves,
+                            size_t curves_bytes, const float *w, const double *sigma,
+                            const double *wed, const float *grad_dose, float *grad_w,
+                            int precision, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- plan-optimisation steps (no counterpart in the reference) ---------------------
  * Device-resident state, so that an optimisation iteration (tables, loss gradient,
  * combination, update) can be captured into one CUDA graph and replayed. */

@@ -10,6 +10,7 @@ Oracle for ``pbd_wed_raytrace`` and ``pbd_forward_wed``.  Only ``tests/`` may im
 * ``wed_ref``   the same per voxel for a whole map, cumulated along z (float64).
 * ``dose_ref``  sum over layers of IDD_l(WED) (``physics_ref.idd_fluence`` evaluated at the
   WED) times the layer's separable lateral dose with unit depth dose (``engine_ref``).
+* ``grad_w_ref`` its dL/dW for a given dL/dD, by float64 autograd.
 Pinned: ``wed_path`` + the reference's helper reproduce tests/golden/hetero.npz, made by the
 reference itself.
 """
@@ -53,3 +54,18 @@ def dose_ref(xv, yv, xs, ys, w, energies, sigma, wed):
         lat = er.separable_f64(xv, yv, xs, ys, w[l:l + 1], np.ones((1, nz)), sigma[l:l + 1])
         d += pr.idd_fluence(wed.ravel(), e).reshape(wed.shape) * lat
     return d
+
+
+def grad_w_ref(xv, yv, xs, ys, w, energies, sigma, wed, grad_dose):
+    """dL/dW of L = sum(grad_dose * D(W)) for the heterogeneous dose of ``dose_ref`` (linear
+    in W), by float64 torch autograd through ``engine_ref.separable_torch``."""
+    import torch
+    wt = torch.tensor(np.asarray(w, dtype=np.float64), requires_grad=True)
+    nz = sigma.shape[1]
+    d = torch.zeros(wed.shape, dtype=torch.float64)
+    for l, e in enumerate(energies):
+        lat = er.separable_torch(xv, yv, xs, ys, wt[l:l + 1], np.ones((1, nz)), sigma[l:l + 1])
+        idd = torch.as_tensor(pr.idd_fluence(wed.ravel(), e).reshape(wed.shape))
+        d = d + idd * lat
+    (d * torch.as_tensor(np.asarray(grad_dose, dtype=np.float64))).sum().backward()
+    return wt.grad.numpy()

@@ -170,3 +170,36 @@ def test_nan_and_out_of_range_wed(pb):
         z = plan.forward(torch.full_like(wed, fill))
         torch.cuda.synchronize()
         assert torch.count_nonzero(z).item() == 0, fill
+
+
+def test_gradient_vs_oracle(pb):
+    """dL/dW of the heterogeneous dose (pbd_adjoint_wed) for a random dL/dD in the slab
+    phantom against float64 autograd through the oracle's dose.  Tolerance 1e-4 of max
+    (the adjoint's split-BF16 products); with a positive dL/dD, sum(dL/dW * W) equals
+    <dL/dD, D> (D is linear in W) to 1e-5."""
+    import torch
+    wl, en, prob = _cfg0(pb)
+    g = prob.grid
+    zc = g.oz + np.arange(g.nz) * g.dz
+    rho = np.ones((g.nz, g.ny, g.nx), dtype=np.float32)
+    rho[(zc >= 2.0) & (zc < 3.0)] = 1.6
+    rho[(zc >= 4.0) & (zc < 5.4), :, : g.nx // 2] = 0.25
+    wed_np = hr.wed_ref(rho, g.oz, g.dz)
+    sig = pr.layer_luts(zc, en)[1]
+    rng = np.random.default_rng(3)
+    grad = rng.standard_normal((g.nz, g.ny, g.nx)).astype(np.float32)
+    want = hr.grad_w_ref(g.x, g.y, prob.lattice.spot_x, prob.lattice.spot_y, wl["weights"], en,
+                         sig, wed_np, grad.astype(np.float64))
+    wed = pb.hetero.wed_raytrace(rho, g)
+    pos = np.abs(grad) + 0.1
+    for prec in ("fp32", "tf32x3"):
+        plan = pb.hetero.WedPlan(prob, precision=prec)
+        got = plan.adjoint(torch.as_tensor(grad, device="cuda"), wed).cpu().numpy()
+        err = rel(got, want)
+        print(f"{prec}: heterogeneous dL/dW max rel err {err:.2e}")
+        assert err < 1e-4, prec
+        d = plan.forward(wed).double().cpu().numpy()
+        gp = plan.adjoint(torch.as_tensor(pos, device="cuda"), wed).double().cpu().numpy()
+        lhs = float(np.sum(gp * wl["weights"]))
+        rhs = float(np.sum(pos * d))
+        assert abs(lhs - rhs) <= 1e-5 * abs(rhs), (prec, lhs, rhs)

@@ -69,6 +69,16 @@ def test_wed_entry_points_validate_before_device_work():
     nul = list(cargs)
     nul[2] = None                                   # no curve blob
     assert lib.pbd_forward_wed_curves(*nul, fake, sz.value, None) == -1
+    # dL/dW of the heterogeneous dose
+    ab = ctypes.c_size_t(0)
+    assert lib.pbd_adjoint_wed_workspace(ctypes.byref(f), ctypes.byref(spec), 1,
+                                         ctypes.byref(ab)) == 0 and ab.value > 0
+    assert lib.pbd_adjoint_wed_workspace(ctypes.byref(f), None, 1, ctypes.byref(ab)) == -1
+    aargs = [ctypes.byref(f), ctypes.byref(spec), fake, cb.value, fake, fake, fake, fake, fake, 1]
+    assert lib.pbd_adjoint_wed(*aargs, None, 0, None) == -7
+    nog = list(aargs)
+    nog[7] = None                                   # no dL/dD
+    assert lib.pbd_adjoint_wed(*nog, fake, ab.value, None) == -1
 
 
 def test_oracle_dose_in_water_equals_reference_dose():
@@ -90,3 +100,32 @@ def test_oracle_dose_in_water_equals_reference_dose():
     d = hr.dose_ref(xv, yv, xs, ys, wl["weights"], lut["energies"], lut["sigma"], wed)
     err = np.max(np.abs(d - ref["dose"])) / np.max(np.abs(ref["dose"]))
     assert err < 1e-11, err
+
+
+def test_oracle_gradient_is_the_dose_derivative():
+    """The oracle's dL/dW of L = <g, D(W)> equals L(W + e_k) - L(W) (D is linear in W) on a
+    small field in a slab medium."""
+    rng = np.random.default_rng(5)
+    nz, ny, nx, nl = 12, 7, 9, 3
+    dz = 0.25
+    xv = (np.arange(nx) - (nx - 1) / 2) * 0.2
+    yv = (np.arange(ny) - (ny - 1) / 2) * 0.2
+    xs = (np.arange(4) - 1.5) * 0.4
+    ys = (np.arange(3) - 1.0) * 0.4
+    en = np.array([45.0, 55.0, 62.0])
+    rho = np.ones((nz, ny, nx))
+    rho[4:7] = 1.7
+    wed = hr.wed_ref(rho, 0.0, dz)
+    z = np.arange(nz) * dz
+    sig = np.stack([np.linspace(0.3, 0.5, nz) + 0.02 * l for l in range(nl)])
+    w = rng.uniform(0.5, 1.5, (nl, 3, 4))
+    g = rng.standard_normal((nz, ny, nx))
+    gw = hr.grad_w_ref(xv, yv, xs, ys, w, en, sig, wed, g)
+    base = float(np.sum(g * hr.dose_ref(xv, yv, xs, ys, w, en, sig, wed)))
+    scale = np.max(np.abs(gw))
+    for k in [(0, 0, 0), (1, 2, 3), (2, 1, 2)]:
+        w1 = w.copy()
+        w1[k] += 1.0
+        diff = float(np.sum(g * hr.dose_ref(xv, yv, xs, ys, w1, en, sig, wed))) - base
+        assert abs(diff - gw[k]) <= 1e-10 * scale, k
+    assert z.size == nz
