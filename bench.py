@@ -533,7 +533,8 @@ def hetero_bench(args):
     (activity table, every layer's lateral map from one tensor-core forward launch, then the
     depth doses at the WED) from the plan's depth curves, built once per plan like the homogeneous
     plan's tables and timed as their own leg (wed_curves), each replayed from a CUDA graph, L2
-    flushed between steps; the homogeneous forward of the same field beside them.  CPU
+    flushed between steps; the homogeneous forward of the same field beside them, and dL/dW
+    of the heterogeneous dose for a dL/dD (one single-layer adjoint per layer).  CPU
     baseline: the oracle's float64 heterogeneous dose."""
     import torch
     pb, wl = workload_arrays()
@@ -554,6 +555,8 @@ def hetero_bench(args):
     homog = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
     out = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device=dev)
     out_h = torch.empty_like(out)
+    gdose = torch.as_tensor(np.random.default_rng(3).standard_normal((g.nz, g.ny, g.nx)),
+                            dtype=torch.float32, device=dev)
     clocks = ClockSampler(0)
     clocks.start()
 
@@ -569,6 +572,7 @@ def hetero_bench(args):
     for name, fn in (("wed_raytrace", lambda: pb.hetero.wed_raytrace(rho, g, device=dev)),
                      ("wed_curves", curves),
                      ("heterogeneous_forward", lambda: plan.forward(wed, out=out)),
+                     ("heterogeneous_adjoint", lambda: plan.adjoint(gdose, wed)),
                      ("homogeneous_forward", lambda: homog.forward(out=out_h))):
         trace()
         fn()
