@@ -51,7 +51,7 @@ def wed_raytrace(rho, grid, device=None):
 class WedPlan:
     """One field in a heterogeneous medium: the lateral widths of water at the geometric
     depths and the layers' depth curves (``pbd_build_wed_curves``), built once on the device,
-    and the workspace of ``pbd_forward_wed_curves``."""
+    and the workspaces of ``pbd_forward_wed_curves`` and (on first use) ``pbd_adjoint_wed``."""
 
     def __init__(self, problem, *, precision: str = "tf32x3", device=None,
                  idd_model: ph.IDDModel = ph.DEFAULT_IDD, sigma_x0: float = 0.30):
@@ -73,39 +73,18 @@ class WedPlan:
         nbytes = _lib.query("pbd_forward_wed_workspace", ctypes.byref(self.field),
                             ctypes.byref(self.spec), self.precision)
         self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
-        # the depth curves depend on the energies only: built once, reused by every forward
+        self.adj_ws = None
+        # the depth curves depend on the energies only: built once, reused by every call
         cbytes = _lib.query("pbd_wed_curves_workspace", ctypes.byref(self.spec), len(L.energies))
         self.curves = torch.empty(cbytes, dtype=torch.uint8, device=self.device)
         _lib.call("pbd_build_wed_curves", ctypes.byref(self.spec), len(L.energies),
                   _lib.ptr(self.energies), None, _lib.ptr(self.curves), cbytes,
                   _lib.stream_handle(self.device))
         self.shape = (g.nz, g.ny, g.nx)
-
-    def forward(self, wed, w=None, out=None):
-        """Dose (float32 device tensor (nz, ny, nx)) for the WED map ``wed`` (float64 tensor or
-        array of the grid's shape, e.g. from ``wed_raytrace``; host data is uploaded), on the
-        current stream."""
-        torch = self.torch
-        if not torch.is_tensor(wed):
-            wed = torch.as_tensor(np.ascontiguousarray(wed, dtype=np.float64))
-        if tuple(wed.shape) != self.shape or wed.dtype != torch.float64:
-            raise ValueError("wed must be a float64 tensor of the grid's shape")
-        wt = self.w if w is None else torch.as_tensor(w, dtype=torch.float32,
-                                                      device=self.device).contiguous()
-        _lib.check_arg(wt, "w", self.w.numel(), torch.float32, self.device)
-        if out is None:
-            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
-        n = self.shape[0] * self.shape[1] * self.shape[2]
-        _lib.check_arg(out, "out", n, torch.float32, self.device)
-        wd = wed.to(self.device).contiguous()
-        _lib.call("pbd_forward_wed_curves", ctypes.byref(self.field), ctypes.byref(self.spec),
-                  _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(wt), _lib.ptr(self.sigma),
-                  _lib.ptr(wd), _lib.ptr(out), self.precision, _lib.ptr(self.ws),
-                  self.ws.numel(), _lib.stream_handle(self.device))
-        return out
-
+        self.nvox = g.nz * g.ny * g.nx
 
     def _wed(self, wed):
+        """The WED map as a contiguous float64 device tensor (host data is uploaded)."""
         torch = self.torch
         if not torch.is_tensor(wed):
             wed = torch.as_tensor(np.ascontiguousarray(wed, dtype=np.float64))
@@ -113,18 +92,37 @@ class WedPlan:
             raise ValueError("wed must be a float64 tensor of the grid's shape")
         return wed.to(self.device).contiguous()
 
+    def _weights(self, w):
+        torch = self.torch
+        if w is None:
+            return self.w
+        wt = torch.as_tensor(w, dtype=torch.float32, device=self.device).contiguous()
+        return _lib.check_arg(wt, "w", self.w.numel(), torch.float32, self.device)
+
+    def forward(self, wed, w=None, out=None):
+        """Dose (float32 device tensor (nz, ny, nx)) for the WED map ``wed`` (float64 tensor or
+        array of the grid's shape, e.g. from ``wed_raytrace``), on the current stream."""
+        torch = self.torch
+        wd = self._wed(wed)
+        wt = self._weights(w)
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        _lib.check_arg(out, "out", self.nvox, torch.float32, self.device)
+        _lib.call("pbd_forward_wed_curves", ctypes.byref(self.field), ctypes.byref(self.spec),
+                  _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(wt), _lib.ptr(self.sigma),
+                  _lib.ptr(wd), _lib.ptr(out), self.precision, _lib.ptr(self.ws),
+                  self.ws.numel(), _lib.stream_handle(self.device))
+        return out
+
     def adjoint(self, grad_dose, wed, w=None):
         """dL/dW (float32 device tensor (L, nsy, nsx)) of the heterogeneous dose for the
         dL/dD ``grad_dose`` ((nz, ny, nx)) and the WED map ``wed`` (``pbd_adjoint_wed``)."""
         torch = self.torch
         wd = self._wed(wed)
-        wt = self.w if w is None else torch.as_tensor(w, dtype=torch.float32,
-                                                      device=self.device).contiguous()
-        _lib.check_arg(wt, "w", self.w.numel(), torch.float32, self.device)
+        wt = self._weights(w)
         g = torch.as_tensor(grad_dose).to(self.device, torch.float32).contiguous()
-        n = self.shape[0] * self.shape[1] * self.shape[2]
-        _lib.check_arg(g, "grad_dose", n, torch.float32, self.device)
-        if getattr(self, "adj_ws", None) is None:
+        _lib.check_arg(g, "grad_dose", self.nvox, torch.float32, self.device)
+        if self.adj_ws is None:
             nbytes = _lib.query("pbd_adjoint_wed_workspace", ctypes.byref(self.field),
                                 ctypes.byref(self.spec), self.precision)
             self.adj_ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
@@ -133,7 +131,6 @@ class WedPlan:
                   _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(wt), _lib.ptr(self.sigma),
                   _lib.ptr(wd), _lib.ptr(g), _lib.ptr(gw), self.precision, _lib.ptr(self.adj_ws),
                   self.adj_ws.numel(), _lib.stream_handle(self.device))
-        self._keep = (wd, g, wt)
         return gw
 
 
