@@ -17,7 +17,6 @@ import numpy as np
 
 from . import _lib
 from . import physics as ph
-from .model import PBProblem
 
 
 @dataclass

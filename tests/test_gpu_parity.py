@@ -6,7 +6,6 @@ Tolerances (written here, not tuned per run):
   * gradients: dL/dW within 1e-4 (relative to max |g|) of float64 autograd through the
     oracle's separable engine; dL/dR within 1e-4 of float64 central differences.
 """
-import ctypes
 
 import numpy as np
 import pytest
