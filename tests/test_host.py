@@ -227,3 +227,42 @@ def test_tensor_argument_checks():
         chk(t, "t", 20, torch.float32, torch.device("cuda", 0))
     assert pkg._lib.same_device(cpu, torch.device("cpu"))
     assert not pkg._lib.same_device(cpu, torch.device("cuda"))
+
+
+def test_tuning_cache_and_schedule(pb, lib, tmp_path, monkeypatch):
+    """The tuner's host side: the JSON cache (round trip; a missing or corrupt file reads as
+    empty), the geometry key, lookup, and the schedule context -- its layers per forward unit
+    reach the library (the forward's workspace grows with the number of layer chunks) and are
+    reset on exit, also after an exception."""
+    import types
+    tun = pb.tuning
+    cache = tmp_path / "sub" / "tuning.json"
+    monkeypatch.setenv("PBD_TUNING_CACHE", str(cache))
+    assert tun.cache_path() == str(cache)
+    assert tun._load() == {}
+    f = pb._lib.Field(nx=128, ny=128, nz=128, dx=0.2, dy=0.2, dz=0.2, ox=-12.7, oy=-12.7,
+                      oz=0.0, n_sx=41, n_sy=41, n_layers=40, dx_spot=0.25, dy_spot=0.25,
+                      x0=0.0, y0=0.0)
+    plan = types.SimpleNamespace(field=f, precision=1, active_pairs=lambda: 2727)
+    key = tun.geometry_key(plan, "loss_grad")
+    assert key == "loss_grad|128x128x128|41x41x40|p1|a2727"
+    assert tun.lookup(plan, "loss_grad") is None
+    tun._store({key: {"schedule": [24, 4], "ms": 0.35}})
+    assert tun.lookup(plan, "loss_grad") == (24, 4)
+    assert tun.lookup(plan, "forward") is None
+    cache.write_text("{not json")
+    assert tun._load() == {} and tun.lookup(plan, "loss_grad") is None
+
+    def fwd_ws():
+        n = ctypes.c_size_t(0)
+        assert lib.pbd_forward_workspace(ctypes.byref(f), 1, ctypes.byref(n)) == 0
+        return n.value
+
+    base = fwd_ws()
+    with tun.schedule(8, 4):
+        small_units = fwd_ws()
+    assert small_units > base and fwd_ws() == base
+    with pytest.raises(RuntimeError):
+        with tun.schedule(8, 4):
+            raise RuntimeError("inside")
+    assert fwd_ws() == base
