@@ -266,3 +266,40 @@ def test_tuning_cache_and_schedule(pb, lib, tmp_path, monkeypatch):
         with tun.schedule(8, 4):
             raise RuntimeError("inside")
     assert fwd_ws() == base
+
+
+def test_engine_host_utilities_match_oracle(pb):
+    """The reference's host utilities kept in engines.py (lateral_kernel, relative_error,
+    normalize_dose, operation_counts) against the oracle's restatements and the FLOP count the
+    bench credits (2 x 2727 active pairs x (nsx nsy ny + nx nsx ny) at 128^3 / 41x41x40)."""
+    import torch
+    from oracle import engine_ref as er
+    E, M = pb.engines, pb.model
+    rng = np.random.default_rng(9)
+    vox = np.linspace(-3.0, 3.0, 17)
+    spots = np.linspace(-2.0, 2.0, 5)
+    sig = rng.uniform(0.2, 0.6, (3, 4))
+    sig[0, 0] = 0.0                                  # clipped at 1e-9
+    assert np.array_equal(E.lateral_kernel(vox, spots, sig), er.lateral_kernel(vox, spots, sig))
+    raw = E.lateral_kernel(vox, spots, 0.4, normalized=False)
+    assert np.array_equal(raw, np.exp(-(vox[:, None] - spots[None, :]) ** 2 / (2 * 0.4 ** 2)))
+    a = rng.standard_normal((6, 7, 8))
+    b = rng.standard_normal((6, 7, 8))
+    mask = rng.random((6, 7, 8)) < 0.3
+    for m in (None, mask, np.zeros_like(mask)):
+        assert E.relative_error(a, b, m) == er.relative_error(a, b, m)
+    assert E.relative_error(torch.as_tensor(a), torch.as_tensor(b)) == er.relative_error(a, b)
+    d = np.abs(b)
+    nd, ref = E.normalize_dose(d)
+    assert ref == d.max() and nd.max() == 1.0
+    roi = np.zeros_like(mask)
+    roi[2, 3, 4] = True
+    nd2, ref2 = E.normalize_dose(d, "roi_max", roi)
+    assert ref2 == d[2, 3, 4] and np.array_equal(nd2, d / d[2, 3, 4])
+    grid = M.DoseGrid(128, 128, 128, 0.2, 0.2, 0.2, -12.7, -12.7, 0.0)
+    lat = M.SpotLattice(41, 41, 40, 0.25, 0.25, weights=np.ones((40, 41, 41)))
+    prob = M.PBProblem(grid, lat, np.ones((40, 128)), np.full((40, 128), 0.4))
+    oc = E.operation_counts(prob, active_pairs=2727)
+    assert 2 * oc["separable_exact"] == 4837218048 and oc["pairs"] == 2727
+    assert E.operation_counts(prob)["pairs"] == 40 * 128
+    assert oc["naive"] == 41 * 41 * 40 * 128 ** 3
