@@ -303,3 +303,29 @@ def test_engine_host_utilities_match_oracle(pb):
     assert 2 * oc["separable_exact"] == 4837218048 and oc["pairs"] == 2727
     assert E.operation_counts(prob)["pairs"] == 40 * 128
     assert oc["naive"] == 41 * 41 * 40 * 128 ** 3
+
+
+def test_model_builders_match_reference_fixture(pb):
+    """DoseGrid axes, SpotLattice positions, the flat spot table (default seeded weights) and
+    flat_field_weights equal the reference's own model.py outputs bit for bit
+    (tests/golden/builders.npz, made by tests/golden/make_golden_builders.py)."""
+    from conftest import golden
+    z = golden("builders.npz")
+    M = pb.model
+    grids = {"centered_z": M.DoseGrid.centered(64, 0.25),
+             "centered_xyz": M.DoseGrid.centered(33, 0.3, axis="xyz"),
+             "aniso": M.DoseGrid(20, 30, 40, 0.15, 0.2, 0.3, -1.4, -2.9, 0.5)}
+    for name, g in grids.items():
+        for ax in ("x", "y", "z"):
+            assert np.array_equal(getattr(g, ax), z[f"{name}__{ax}"]), (name, ax)
+        assert [g.nx, g.ny, g.nz, g.n_vox] == z[f"{name}__dims"].tolist()
+    lat = M.SpotLattice(7, 5, 3, 0.4, 0.6, x0=0.07, y0=-0.11)
+    assert np.array_equal(lat.spot_x, z["lat__spot_x"])
+    assert np.array_equal(lat.spot_y, z["lat__spot_y"])
+    for got, key in zip(lat.flat_spot_table(), ("x", "y", "l", "w")):
+        assert np.array_equal(got, z[f"lat__table_{key}"]), key
+    assert np.array_equal(M.flat_field_weights(41, 41, 4), z["flat_default"])
+    assert np.array_equal(M.flat_field_weights(21, 21, 3, field_half_width=3.0, spot_spacing=0.4,
+                                               edge=0.5, radial_falloff=0.1, layer_jitter=0.3,
+                                               seed=7), z["flat_args"])
+    assert np.array_equal(M.flat_field_weights(15, 15, 2, layer_jitter=0.0), z["flat_nojitter"])
