@@ -329,3 +329,25 @@ def test_model_builders_match_reference_fixture(pb):
                                                edge=0.5, radial_falloff=0.1, layer_jitter=0.3,
                                                seed=7), z["flat_args"])
     assert np.array_equal(M.flat_field_weights(15, 15, 2, layer_jitter=0.0), z["flat_nojitter"])
+
+
+def test_reference_arm_json_contract():
+    """``bench.py --impl reference`` (the oracle's CPU port, host cores only) prints one JSON
+    line with the bench contract's keys: the metric and unit of the device arm, at least three
+    warm-up evaluations, a cpu_baseline describing the run and an e2e object with no copies."""
+    import json
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "3"], capture_output=True, text=True,
+                       timeout=600, cwd=REPO)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "grad_evals/s" and d["value"] > 0
+    assert d["higher_is_better"] is True and d["warmup"] >= 3 and d["steps"] == 1
+    assert d["metric"].startswith("fwd+adjoint dose-gradient evals/s")
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
