@@ -351,3 +351,16 @@ def test_reference_arm_json_contract():
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+
+
+def test_depth_axis_check(pb):
+    """The device table builder takes a uniform depth axis (nz, z0, dz); layer_luts derives it
+    from the caller's axis and refuses what it cannot represent."""
+    ua = pb.physics._uniform_axis
+    assert ua(np.arange(64) * 0.2) == (64, 0.0, (63 * 0.2) / 63)
+    assert ua([3.5]) == (1, 3.5, 1.0)
+    n, z0, dz = ua(0.1 + np.arange(10) * 0.25)
+    assert n == 10 and z0 == 0.1 and abs(dz - 0.25) < 1e-15
+    for bad in ([], [[0.0, 1.0]], [0.0, 0.1, 0.3]):
+        with pytest.raises(ValueError):
+            ua(bad)
