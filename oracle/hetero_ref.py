@@ -1,7 +1,8 @@
 """CPU restatement of the water-equivalent depth and the heterogeneous dose (TEST
 INFRASTRUCTURE ONLY).
 
-Oracle for ``pbd_wed_raytrace`` and ``pbd_forward_wed``.  Only ``tests/`` may import it.
+Oracle for ``pbd_wed_raytrace``, ``pbd_forward_wed`` and ``pbd_adjoint_wed``.  Only
+``tests/`` and ``bench.py``'s CPU-baseline leg may import it; the product path never does.
 
 * ``wed_path``  the (densities, lengths) of the path from depth 0 to voxel k of a column:
   water above the first voxel, voxels i < k in full, half of voxel k, each voxel filling
