@@ -129,3 +129,28 @@ def test_oracle_gradient_is_the_dose_derivative():
         diff = float(np.sum(g * hr.dose_ref(xv, yv, xs, ys, w1, en, sig, wed))) - base
         assert abs(diff - gw[k]) <= 1e-10 * scale, k
     assert z.size == nz
+
+
+def test_oracle_nan_and_out_of_range_semantics():
+    """The oracle's dose at a WED follows np.interp: NaN in, NaN out at that voxel only;
+    beyond every layer's curve, or at a negative WED, exactly 0 -- the behaviour the device
+    test checks against."""
+    nz, ny, nx = 6, 5, 4
+    xv = (np.arange(nx) - 1.5) * 0.3
+    yv = (np.arange(ny) - 2.0) * 0.3
+    xs = np.array([-0.2, 0.2])
+    ys = np.array([-0.2, 0.0, 0.2])
+    en = np.array([60.0, 70.0])
+    sig = np.full((2, nz), 0.35)
+    w = np.ones((2, 3, 2))
+    wed = np.tile((np.arange(nz) * 0.5)[:, None, None], (1, ny, nx))
+    base = hr.dose_ref(xv, yv, xs, ys, w, en, sig, wed)
+    wn = wed.copy()
+    wn[2, 1, 3] = np.nan
+    d = hr.dose_ref(xv, yv, xs, ys, w, en, sig, wn)
+    nan = np.isnan(d)
+    assert nan.sum() == 1 and nan[2, 1, 3]
+    assert np.array_equal(d[~nan], base[~nan])
+    for fill in (1e3, -1.0):
+        assert np.count_nonzero(hr.dose_ref(xv, yv, xs, ys, w, en, sig,
+                                            np.full_like(wed, fill))) == 0
