@@ -139,6 +139,18 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def blas_threads() -> int:
+    """Threads of the BLAS pool NumPy's float64 work ran on (all host cores if unknown)."""
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads") or 0 for i in threadpool_info() if i.get("user_api") == "blas"]
+        if n and max(n) > 0:
+            return int(max(n))
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
 def read_traffic(kernel):
     """Per-launch DRAM bytes of ``kernel`` from the committed ncu summary, if present."""
     path = os.path.join(REPO, "profiles", "traffic_per_launch.txt")
@@ -598,7 +610,7 @@ def hetero_bench(args):
         el = time.perf_counter() - t0
         d = out.double().cpu().numpy()
         legs["max_rel_err_vs_fp64"] = float(np.max(np.abs(d - ref)) / np.max(np.abs(ref)))
-        cpu = {"value": 1.0 / el, "unit": "doses/s", "cores": 16, "kind": "port",
+        cpu = {"value": 1.0 / el, "unit": "doses/s", "cores": blas_threads(), "kind": "port",
                "sample": "1 heterogeneous 128^3 dose (NumPy / torch float64, incl. the tables)"}
     head = legs["heterogeneous_forward"]
     line = {"workload": "hetero", "metric": "heterogeneous-medium doses/s, 128^3 / 41x41x40",
