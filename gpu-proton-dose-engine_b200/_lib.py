@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpbdose_b200.so")
 
 PBD_OK = 0
+PBD_ERR_TIMEOUT = -8
 PREC = {"fp32": 0, "tf32x3": 1, "tf32": 2, "bf16x3": 3, "bf16": 4}
 MAX_JOBS = 128
 
@@ -34,6 +35,60 @@ class Field(ctypes.Structure):
                 ("n_sx", c_int), ("n_sy", c_int), ("n_layers", c_int),
                 ("dx_spot", c_double), ("dy_spot", c_double),
                 ("x0", c_double), ("y0", c_double)]
+
+
+def _uniform(axis, name):
+    """(first value, spacing) of a uniform axis; its centre and spacing for a lattice."""
+    import numpy as np
+    a = np.asarray(axis, dtype=np.float64).reshape(-1)
+    if a.size == 0:
+        raise ValueError(f"{name} is empty")
+    if a.size == 1:
+        return float(a[0]), 1.0
+    d = np.diff(a)
+    step = float((a[-1] - a[0]) / (a.size - 1))
+    if step <= 0 or np.max(np.abs(d - step)) > 1e-9 * max(abs(step), 1.0):
+        raise ValueError(f"{name} is not a uniform increasing axis")
+    return float(a[0]), step
+
+
+def field_from(grid, lattice) -> Field:
+    """The C ABI's pbd_field from a dose grid and a spot lattice.
+
+    Takes the reference's DoseGrid / SpotLattice as they are (model.py:27-113): the grid's
+    nx, ny, nz and origin / spacing fields (or, when an object lacks those, its voxel-centre
+    axes x, y -- the attributes the reference's engine reads, engines.py:227-234) and the
+    lattice's n_sx, n_sy, n_layers and pitch / offset fields (or its spot_x, spot_y
+    positions).  The depth origin and spacing default to 0 and 1 when absent: the dose
+    kernels do not use them (the depth tables are per slice)."""
+    g, L = grid, lattice
+    nx, ny, nz = int(g.nx), int(g.ny), int(g.nz)
+    if all(hasattr(g, a) for a in ("ox", "dx", "oy", "dy")):
+        ox, dx, oy, dy = float(g.ox), float(g.dx), float(g.oy), float(g.dy)
+    else:
+        ox, dx = _uniform(g.x, "grid.x")
+        oy, dy = _uniform(g.y, "grid.y")
+    oz = float(getattr(g, "oz", 0.0))
+    dz = float(getattr(g, "dz", 1.0))
+    if all(hasattr(L, a) for a in ("x0", "dx_spot", "y0", "dy_spot")):
+        x0, dxs, y0, dys = float(L.x0), float(L.dx_spot), float(L.y0), float(L.dy_spot)
+    else:
+        import numpy as np
+        sx = np.asarray(L.spot_x, dtype=np.float64)
+        sy = np.asarray(L.spot_y, dtype=np.float64)
+        _, dxs = _uniform(sx, "lattice.spot_x")
+        _, dys = _uniform(sy, "lattice.spot_y")
+        x0 = float(0.5 * (sx[0] + sx[-1]))       # spot_x = x0 + (i - (n-1)/2) dx_spot
+        y0 = float(0.5 * (sy[0] + sy[-1]))
+    return Field(nx=nx, ny=ny, nz=nz, dx=dx, dy=dy, dz=dz, ox=ox, oy=oy, oz=oz,
+                 n_sx=int(L.n_sx), n_sy=int(L.n_sy), n_layers=int(L.n_layers),
+                 dx_spot=dxs, dy_spot=dys, x0=x0, y0=y0)
+
+
+def field_of(problem) -> Field:
+    """pbd_field of a problem: anything with ``grid`` and ``lattice`` (the reference's
+    PBProblem or this package's)."""
+    return field_from(problem.grid, problem.lattice)
 
 
 class LutSpec(ctypes.Structure):
@@ -93,6 +148,9 @@ _SIGS = {
     "pbd_profile_end": (c_int, [POINTER(c_double), POINTER(c_int), POINTER(c_double),
                                 POINTER(c_int)]),
     "pbd_launch_count": (c_int, [POINTER(ctypes.c_longlong)]),
+    "pbd_workspace_status": (c_int, [c_void_p, c_size_t, POINTER(c_int), c_void_p]),
+    "pbd_test_hook": (c_int, [ctypes.c_ulonglong, c_int]),
+    "pbd_forward_f64": (c_int, [POINTER(Field), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "pbd_lut_workspace": (c_int, [POINTER(LutSpec), c_int, POINTER(c_size_t)]),
     "pbd_build_luts": (c_int, [POINTER(LutSpec), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
@@ -190,6 +248,27 @@ def launch_count() -> int:
     n = ctypes.c_longlong(0)
     call("pbd_launch_count", ctypes.byref(n))
     return int(n.value)
+
+
+def workspace_status(ws, stream=None) -> int:
+    """Status of the last library call that used the device workspace tensor ``ws``:
+    PBD_OK or PBD_ERR_TIMEOUT (synchronises the stream)."""
+    st = c_int(0)
+    call("pbd_workspace_status", ptr(ws), ws.numel(), ctypes.byref(st),
+         stream if stream is not None else stream_handle(ws.device))
+    return int(st.value)
+
+
+def check_workspace(ws, fn: str, stream=None) -> None:
+    """Raise PbdError(PBD_ERR_TIMEOUT) when the last call on ``ws`` ran out of a device wait."""
+    st = workspace_status(ws, stream)
+    if st != PBD_OK:
+        raise PbdError(fn, st, strerror(st))
+
+
+def test_hook(wait_limit_ns: int = 0, hold: bool = False) -> None:
+    """Test hook of the timeout path (pbd_test_hook): per calling thread."""
+    call("pbd_test_hook", int(wait_limit_ns), 1 if hold else 0)
 
 
 def profile_begin() -> None:

@@ -26,6 +26,7 @@ SOURCES = {
     "api.cu": [],
     "lut.cu": ["-fmad=false"],
     "fwd_simt.cu": [],
+    "fwd_f64.cu": [],
     "adj_simt.cu": [],
     "tc_fwd.cu": [],
     "noalloc.cu": [],

@@ -325,13 +325,8 @@ int adj_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 int launch_adjoint(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, AdjItem* items,
                    int total_items, int* counter, int chunk, int with_range, int finalize_loss,
                    cudaStream_t s) {
-    static thread_local bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(adj_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kAdjSmemBytes) != cudaSuccess)
-            return PBD_ERR_NO_SMEM;
-        attr_set = true;
-    }
+    int set = 0;
+    PBD_TRY(smem_optin((const void*)adj_simt_kernel, (int)kAdjSmemBytes, 0, &set));
     PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, sizeof(int), s)));
     adj_schedule_kernel<<<n_jobs, 256, kActStage, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();

@@ -43,9 +43,9 @@
 //
 // dL/dW_l = sum over active slices of IDD * slot P in slice order, and the dot products
 // <slot, W> for dL/dIDD and dL/dsigma, are formed by one follow-up kernel in a fixed order
-// (deterministic).  Every wait is bounded (2 s of %globaltimer); a warp whose wait
-// runs out sets the error word and leaves, the others' waits then run out in turn, and
-// the finalize pass turns the gradients into NaN.
+// (deterministic).  Every wait is bounded (2 s of %globaltimer, or a test limit); a warp
+// whose wait runs out sets the error word and leaves, the others' waits then run out in
+// turn, and the finalize pass turns the gradients into NaN.
 // Grids of at most 128 x 128 voxels per slice; lattices up to 64 x 64 spots.
 #include <algorithm>
 #include <math.h>
@@ -83,7 +83,10 @@ struct Step {
 struct Params {
     const JobDev* jobs;
     int n_jobs, chunk, cmax, n_units;
-    int* counter;        // [0] unit counter, [1] error word
+    int* counter;        // [0] unit counter
+    int* err;            // error word: set when a bounded wait ran out
+    unsigned long long wait_ns;   // limit of every bounded wait
+    int hold;            // test of the timeout path: the scheduler publishes no step
     int N1;              // x-lattice padded to 16
 };
 
@@ -133,7 +136,7 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
     bool ok = true;
     auto push = [&](int src, const Step& st) -> bool {
         const int slot = k % kRing, n = k / kRing;
-        const bool w = wait_bar(&empty[slot], (uint32_t)((n & 1) ^ 1));
+        const bool w = wait_bar(&empty[slot], (uint32_t)((n & 1) ^ 1), P.wait_ns);
         if (!__all_sync(FULL, w)) return false;
         if (lane == src) {
             ring[slot] = st;
@@ -143,6 +146,8 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
         ++k;
         return true;
     };
+    // timeout-path test: publish nothing, so that every consumer's first wait runs out
+    if (P.hold) return;
     for (;;) {
         int u = 0;
         if (lane == 0) u = atomicAdd(P.counter, 1);
@@ -220,14 +225,14 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
     bool ok = true;
     for (;;) {
         const int slot = k % kRing;
-        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1));
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
         const int flags = ring[slot].flags;
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[slot]);
         ++k;
         if (!__all_sync(0xffffffffu, ok)) break;
         if (flags & kEnd) break;
-        ok = wait_bar(ops, (uint32_t)(n & 1));
+        ok = wait_bar(ops, (uint32_t)(n & 1), P.wait_ns);
         if (!__all_sync(0xffffffffu, ok)) break;
         tc::fence_after_sync();
         if (lane == 0) {
@@ -259,8 +264,8 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
         __syncwarp();
         ++n;
     }
-    if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
-    if (n > 0) (void)wait_bar(done, (uint32_t)((n - 1) & 1));
+    if (!ok && lane == 0) atomicExch(P.err, 1);
+    if (n > 0) (void)wait_bar(done, (uint32_t)((n - 1) & 1), P.wait_ns);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -294,7 +299,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
 
     for (;;) {
         const int slot = k % kRing;
-        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1));
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
         const Step cur = ring[slot];
         if (cur.flags != kEnd && (cur.job < 0 || cur.job >= P.n_jobs)) ok = false;
         __syncwarp();
@@ -381,7 +386,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
 
         // ---- DR: Q of the previous pair -> the two slots ----
         if (have_prev) {
-            ok = ok && wait_bar(mma2, ph2);
+            ok = ok && wait_bar(mma2, ph2, P.wait_ns);
             if (ok) ph2 ^= 1;
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::fence_after_sync();
@@ -448,7 +453,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             }
         }
         // ---- E1: Y of this pair -> split -> TMEM A[b] (row m, x columns [64 half, +64)) ----
-        ok = ok && wait_bar(mma1, ph1);
+        ok = ok && wait_bar(mma1, ph1, P.wait_ns);
         if (ok) ph1 ^= 1;
         if (!__all_sync(0xffffffffu, ok)) break;
         tc::fence_after_sync();
@@ -488,7 +493,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
     }
     // last pair's Q
     if (ok && have_prev) {
-        ok = wait_bar(mma2, ph2);
+        ok = wait_bar(mma2, ph2, P.wait_ns);
         if (__all_sync(0xffffffffu, ok)) {
             tc::fence_after_sync();
             const JobDev& Jp = P.jobs[prev.job];
@@ -522,7 +527,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             }
         }
     }
-    if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
+    if (!ok && lane == 0) atomicExch(P.err, 1);
 }
 
 template <int MODE>
@@ -738,24 +743,9 @@ size_t adj_smem_bytes(int N1) {
 
 template <int MODE>
 int launch_mode(const Params& P0, cudaStream_t s) {
-    static thread_local int max_dyn = 0;
-    if (max_dyn == 0) {
-        int dev = 0, optin = 0;
-        cudaFuncAttributes fa;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
-                cudaSuccess ||
-            cudaFuncGetAttributes(&fa, adj_tc_kernel<MODE>) != cudaSuccess)
-            return PBD_ERR_CUDA;
-        // the setmaxnreg split needs the full launch allotment, or its increase never returns
-        if (fa.numRegs < kLaunchRegsNeeded) return PBD_ERR_UNSUPPORTED;
-        const int avail = optin - (int)fa.sharedSizeBytes;
-        if (avail <= 0 || cudaFuncSetAttribute(adj_tc_kernel<MODE>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               avail) != cudaSuccess)
-            return PBD_ERR_NO_SMEM;
-        max_dyn = avail;
-    }
+    // the setmaxnreg split needs the full launch allotment, or its increase never returns
+    int max_dyn = 0;
+    PBD_TRY(smem_optin((const void*)adj_tc_kernel<MODE>, -1, kLaunchRegsNeeded, &max_dyn));
     const Params P = P0;
     size_t smem = adj_smem_bytes<MODE>(P.N1);
     // >= 116 KiB: one CTA, and its 512 TMEM columns, per SM
@@ -788,13 +778,16 @@ size_t tc_adjoint_slot_elems(const pbd_field* f) {
 }
 
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      int* counter, int chunk, int with_range, int finalize_loss,
+                      int* counter, int* err, int chunk, int with_range, int finalize_loss,
                       int counters_zeroed, cudaStream_t s) {
     Params P{};
     P.jobs = jobs_dev;
     P.n_jobs = n_jobs;
     P.chunk = chunk;
     P.counter = counter;
+    P.err = err;
+    P.wait_ns = wait_limit_ns();
+    P.hold = test_hold();
     int cm = 1, nzm = 1, max_l = 1, max_per = 1;
     for (int j = 0; j < n_jobs; ++j) {
         pbd_field f{};
@@ -822,7 +815,7 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     (void)max_per;
     PBD_TRY(launch_dependent(adj_tc_reduce_kernel, dim3((nzm + kRedZ - 1) / kRedZ, max_l, n_jobs),
                              dim3(kRedThreads), 0, s, (const JobDev*)jobs_dev, with_range,
-                             finalize_loss, (const int*)(counter + 1), counter + 2, max_l));
+                             finalize_loss, (const int*)err, counter + 2, max_l));
     count_launch(2);
     return PBD_OK;
 }

@@ -25,8 +25,10 @@ struct JobPair {
     int n;
 };
 
-__global__ void install_jobs_kernel(JobPair p, JobDev* dst) {
+// Installs the call's job views and clears its status header (may be null).
+__global__ void install_jobs_kernel(JobPair p, JobDev* dst, int* status) {
     if ((int)threadIdx.x < p.n) dst[threadIdx.x] = p.j[threadIdx.x];
+    if (status && (int)threadIdx.x < kStatusInts) status[threadIdx.x] = 0;
 }
 
 struct JobLite {
@@ -47,8 +49,9 @@ struct JobTable {
 static_assert(sizeof(JobTable) < 32000, "kernel parameter limit");
 
 __global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_base, int* nchunk_base,
-                                     int* arrive_base) {
+                                     int* arrive_base, int* status) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < kStatusInts) status[k] = 0;
     if (k >= t.n) return;
     const JobLite& a = t.j[k];
     JobDev J;
@@ -94,10 +97,12 @@ struct GradBufs {
     double* lpart;
     float *apart, *dcs, *dsgs;
     const int* fwd_err;
+    int* status;         // cleared by the first group's launch
 };
 
 __global__ void install_grad_kernel(GradTable t, GradBufs b) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t.base == 0 && k < kStatusInts) b.status[k] = 0;
     if (k >= t.n) return;
     const GradLite& a = t.j[k];
     JobDev J;
@@ -127,6 +132,19 @@ __global__ void install_grad_kernel(GradTable t, GradBufs b) {
 
 int g_sms[64] = {0};
 std::mutex g_sms_mu;
+
+// smem_optin's cache: one entry per (device, kernel).
+struct OptIn {
+    int dev;
+    const void* fn;
+    int bytes;   // value set, or a negative error code
+};
+std::vector<OptIn> g_optin;
+std::mutex g_optin_mu;
+
+// pbd_test_hook's settings (calling thread)
+thread_local unsigned long long g_wait_ns = 0;   // 0 = the default 2 s
+thread_local int g_hold = 0;
 
 struct ProfState {
     bool on = false;
@@ -166,9 +184,10 @@ int adjoint_supported(const pbd_field* f) {
 
 // Workspace of the single-job paths.
 struct Ws {
+    int* status;         // status header: [kStatFwd], [kStatAdj] error words
     JobDev* jobs;        // [0] forward view, [1] adjoint view
-    int* counters;       // [0] forward items, [1] forward error word, [2] adjoint items,
-                         // [3] adjoint error word; then the forward's arrival counters
+    int* counters;       // [0] forward items, [2] adjoint items (FP32); then the forward's
+                         // arrival counters
     int* farr;           // tensor-core forward: per (slice, tile) arrival counters
     size_t n_fcount;     // ints the forward clears at launch (counters + arrivals)
     int n_loss_part;
@@ -189,6 +208,7 @@ struct Ws {
 int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, void* base, Ws& w,
              size_t* used) {
     Carve c(base);
+    w.status = c.take<int>(kStatusInts);
     w.jobs = c.take<JobDev>(2);
     const int tiles = ((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile);
     const size_t narr = fwd ? (size_t)f->nz * tiles * kTcFwdWarps : 0;
@@ -234,6 +254,39 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
 }
 
 }  // namespace
+
+int smem_optin(const void* fn, int bytes, int min_regs, int* set_bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PBD_ERR_CUDA;
+    std::lock_guard<std::mutex> g(g_optin_mu);
+    for (const OptIn& o : g_optin)
+        if (o.dev == dev && o.fn == fn) {
+            if (o.bytes < 0) return o.bytes;
+            *set_bytes = o.bytes;
+            return PBD_OK;
+        }
+    int optin = 0;
+    cudaFuncAttributes fa;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+            cudaSuccess ||
+        cudaFuncGetAttributes(&fa, fn) != cudaSuccess)
+        return PBD_ERR_CUDA;
+    int rc = PBD_OK;
+    const int want = bytes >= 0 ? bytes : optin - (int)fa.sharedSizeBytes;
+    if (min_regs > 0 && fa.numRegs < min_regs) {
+        rc = PBD_ERR_UNSUPPORTED;
+    } else if (want <= 0 || want + (int)fa.sharedSizeBytes > optin ||
+               cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, want) !=
+                   cudaSuccess) {
+        rc = PBD_ERR_NO_SMEM;
+    }
+    g_optin.push_back({dev, fn, rc == PBD_OK ? want : rc});
+    if (rc == PBD_OK) *set_bytes = want;
+    return rc;
+}
+
+unsigned long long wait_limit_ns() { return g_wait_ns ? g_wait_ns : 2000000000ull; }
+int test_hold() { return g_hold; }
 
 int num_sms() {
     int dev = 0;
@@ -315,8 +368,8 @@ static void wed_jobs(const pbd_field* f, int l0, int n, const float* w, const do
 }
 
 struct WedCarve {
+    int* status;         // status header: forward, combine error words
     double* act;
-    int* err;            // the combine's error word
     float* lateral;      // (L, wed_lateral_stride) per-layer lateral maps
     void* curves;
     size_t curves_bytes;
@@ -339,8 +392,8 @@ static int carve_wed(const pbd_field* f, const pbd_lut_spec* spec, int precision
     }
     PBD_TRY(lut_curve_workspace(spec, L, &cb));
     Carve c(base);
+    w.status = c.take<int>(kStatusInts);
     w.act = c.take<double>((size_t)L * f->nz);
-    w.err = c.take<int>(1);
     w.lateral = c.take<float>((size_t)L * wed_lateral_stride(f));
     w.curves = c.take<char>(cb);
     w.curves_bytes = cb;
@@ -422,6 +475,41 @@ int pbd_launch_count(long long* n) {
     return PBD_OK;
 }
 
+int pbd_test_hook(unsigned long long wait_limit_ns, int hold_schedulers) {
+    if (hold_schedulers != 0 && hold_schedulers != 1) return PBD_ERR_BAD_VALUE;
+    if (hold_schedulers && wait_limit_ns == 0) return PBD_ERR_BAD_VALUE;   // keep 2 s holds out
+    g_wait_ns = wait_limit_ns;
+    g_hold = hold_schedulers;
+    return PBD_OK;
+}
+
+int pbd_workspace_status(const void* workspace, size_t workspace_bytes, int* status,
+                         void* stream) {
+    if (!workspace || !status) return PBD_ERR_NULL_ARG;
+    Carve c(const_cast<void*>(workspace));
+    const int* hdr = c.take<int>(kStatusInts);
+    if (c.used > workspace_bytes) return PBD_ERR_WORKSPACE;
+    int h[kStatusInts];
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(h, hdr, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return PBD_ERR_CUDA;
+    int st = PBD_OK;
+    for (int k = 0; k < kStatusInts; ++k)
+        if (h[k] != 0) st = PBD_ERR_TIMEOUT;
+    *status = st;
+    return PBD_OK;
+}
+
+int pbd_forward_f64(const pbd_field* f, const double* w, const double* idd, const double* sigma,
+                    double* dose, void* stream) {
+    PBD_TRY(host_validate_field(f));
+    if (!w || !idd || !sigma || !dose) return PBD_ERR_NULL_ARG;
+    PBD_TRY(launch_forward_f64(f, w, idd, sigma, dose, (cudaStream_t)stream));
+    count_launch(1);
+    return PBD_OK;
+}
+
 int pbd_lut_workspace(const pbd_lut_spec* spec, int n_layers, size_t* bytes) {
     return lut_workspace_bytes(spec, n_layers, bytes);
 }
@@ -469,18 +557,20 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
     J.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
     J.item_base = 0; J.max_items = ws.f_items;
     J.partial = ws.fpart; J.nchunks = ws.fnch; J.arrive = ws.farr;
-    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
-                          ws.f_chunk, 0, precision, 1, s);
+                          ws.status + kStatFwd, ws.f_chunk, 0, precision, 1, s);
 }
 
+// err: the adjoint's error word (the workspace's own status word unless a caller passes its
+// own, as the heterogeneous adjoint does for its per-layer calls)
 static int run_adjoint(const Ws& ws, int precision, const JobDev* A, int with_range,
-                       int finalize_loss, int counters_zeroed, cudaStream_t s) {
+                       int finalize_loss, int counters_zeroed, int* err, cudaStream_t s) {
     if (ws.adj_tc)
-        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, ws.acnt, ws.a_chunk, with_range,
-                                 finalize_loss, counters_zeroed, s);
+        return launch_adjoint_tc(precision, ws.jobs + 1, A, 1, ws.acnt, err, ws.a_chunk,
+                                 with_range, finalize_loss, counters_zeroed, s);
     return launch_adjoint(ws.jobs + 1, A, 1, static_cast<AdjItem*>(ws.aitems), ws.a_items,
                           ws.counters + 2, ws.a_chunk, with_range, finalize_loss, s);
 }
@@ -505,10 +595,12 @@ static void fill_adj_view(const pbd_field* f, const Ws& ws, JobDev& A) {
     A.dsg = ws.dsg;
 }
 
-int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const double* sigma,
-                const double* didd_dr, const double* dsigma_dr, const float* grad_dose,
-                float* grad_w, float* grad_range, int precision, void* workspace,
-                size_t workspace_bytes, void* stream) {
+// One adjoint call; `err` (may be null: the workspace's own status word) receives a timed-out
+// wait.
+static int adjoint_one(const pbd_field* f, const float* w, const double* idd, const double* sigma,
+                       const double* didd_dr, const double* dsigma_dr, const float* grad_dose,
+                       float* grad_w, float* grad_range, int precision, void* workspace,
+                       size_t workspace_bytes, int* err, cudaStream_t s) {
     PBD_TRY(host_validate_field(f));
     PBD_TRY(check_field_precision(f, precision));
     PBD_TRY(adjoint_supported(f));
@@ -520,7 +612,6 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
     PBD_TRY(carve_ws(f, false, true, false, precision, nullptr, ws, &need));
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
     PBD_TRY(carve_ws(f, false, true, false, precision, workspace, ws, &need));
-    cudaStream_t s = (cudaStream_t)stream;
     JobPair p;
     memset(&p, 0, sizeof(p));
     p.n = 2;
@@ -531,10 +622,18 @@ int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const dou
     A.grad_w = grad_w; A.grad_range = grad_range;
     fill_adj_view(f, ws, A);
     p.j[0] = A;
-    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return run_adjoint(ws, precision, &A, with_range, 0, 0, s);
+    return run_adjoint(ws, precision, &A, with_range, 0, 0, err ? err : ws.status + kStatAdj, s);
+}
+
+int pbd_adjoint(const pbd_field* f, const float* w, const double* idd, const double* sigma,
+                const double* didd_dr, const double* dsigma_dr, const float* grad_dose,
+                float* grad_w, float* grad_range, int precision, void* workspace,
+                size_t workspace_bytes, void* stream) {
+    return adjoint_one(f, w, idd, sigma, didd_dr, dsigma_dr, grad_dose, grad_w, grad_range,
+                       precision, workspace, workspace_bytes, nullptr, (cudaStream_t)stream);
 }
 
 int pbd_loss_grad_workspace(const pbd_field* f, int precision, size_t* bytes) {
@@ -578,19 +677,19 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     F.item_base = 0; F.max_items = ws.f_items;
     F.partial = ws.fpart; F.nchunks = ws.fnch; F.arrive = ws.farr;
     fill_adj_view(f, ws, A);
-    A.fwd_err = ws.counters + 1;
+    A.fwd_err = ws.status + kStatFwd;
     p.j[1] = A;
     // the adjoint's counters are cleared before the forward, so that forward -> adjoint ->
     // reduce run back to back (programmatic dependent launches)
     if (ws.adj_tc)
         PBD_TRY(cuda_rc(cudaMemsetAsync(ws.acnt, 0,
                                         tc_adjoint_counter_ints(1, f->n_layers) * sizeof(int), s)));
-    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
-                           ws.f_chunk, 1, precision, 0, s));
-    return run_adjoint(ws, precision, &A, with_range, 1, ws.adj_tc, s);
+                           ws.status + kStatFwd, ws.f_chunk, 1, precision, 0, s));
+    return run_adjoint(ws, precision, &A, with_range, 1, ws.adj_tc, ws.status + kStatAdj, s);
 }
 
 // ---- batched loss gradient ------------------------------------------------------------
@@ -643,6 +742,7 @@ static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, 
 }
 
 struct GradCarve {
+    int* status;
     JobDev *fwd, *adj;
     int *fcnt, *acnt;
     float* fpart;
@@ -652,6 +752,7 @@ struct GradCarve {
 
 static size_t carve_grad(void* base, int n_jobs, const GradPlan& gp, GradCarve& g) {
     Carve c(base);
+    g.status = c.take<int>(kStatusInts);
     g.fwd = c.take<JobDev>(n_jobs);
     g.adj = c.take<JobDev>(n_jobs);
     g.fcnt = c.take<int>(2 + gp.arr);
@@ -713,6 +814,7 @@ int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, 
     BatchPlan bp;
     PBD_TRY(plan_batch(jobs, n_jobs, precision, &bp));
     Carve c(nullptr);
+    c.take<int>(kStatusInts);
     c.take<JobDev>(n_jobs);
     c.take<int>(2 + bp.arr);
     c.take<FwdItem>(bp.items);
@@ -762,17 +864,19 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
         part_off += bp.direct ? 0 : pe;
     }
     Carve c(workspace);
+    int* status = c.take<int>(kStatusInts);
     JobDev* jd = c.take<JobDev>(n_jobs);
     int* counter = c.take<int>(2 + arr_off);
     FwdItem* items = c.take<FwdItem>(item_base);
     int* nchb = c.take<int>(nch_off);
     float* partb = c.take<float>(part_off);
     cudaStream_t s = (cudaStream_t)stream;
-    install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb, counter + 2);
+    install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb, counter + 2,
+                                                             status);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, 2 + arr_off, bp.chunk,
-                          0, precision, 1, s);
+    return launch_forward(jd, host_view, n_jobs, items, item_base, counter, 2 + arr_off,
+                          status + kStatFwd, bp.chunk, 0, precision, 1, s);
 }
 
 // ---- heterogeneous media ------------------------------------------------------------
@@ -805,10 +909,10 @@ int pbd_build_wed_curves(const pbd_lut_spec* spec, int n_layers, const double* e
 
 // Tensor-core precisions: every layer's lateral map (depth dose = the activity table) from
 // one launch of the forward in its per-layer-maps mode, so that a unit's layers share its
-// distance tables.  *fwd_err: the forward's error word.
+// distance tables.  err: the forward's error word (the caller's status header).
 static int forward_layer_maps(const pbd_field* f, const float* w, const double* act,
                               const double* sigma, float* lateral, size_t lstride, int precision,
-                              void* base, size_t bytes, cudaStream_t s, const int** fwd_err) {
+                              void* base, size_t bytes, cudaStream_t s, int* err) {
     size_t need = 0;
     Ws ws;
     PBD_TRY(carve_ws(f, true, false, false, precision, nullptr, ws, &need));
@@ -824,12 +928,11 @@ static int forward_layer_maps(const pbd_field* f, const float* w, const double* 
     J.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
     J.item_base = 0; J.max_items = ws.f_items;
     J.partial = ws.fpart; J.nchunks = ws.fnch; J.arrive = ws.farr;
-    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs);
+    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, nullptr);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    *fwd_err = ws.counters + 1;
     // no poison pass here: the combine's poison pass reads this error word too
-    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
+    return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount, err,
                           ws.f_chunk, 0, precision, 0, s);
 }
 
@@ -843,10 +946,12 @@ static int forward_wed_body(const pbd_field* f, const pbd_lut_spec* spec, const 
     const size_t lstride = wed_lateral_stride(f);
     PBD_TRY(lut_wed_activity(spec, f->n_layers, curves, curves_bytes, wed, f->nz, nslice, wc.act,
                              s));
+    PBD_TRY(cuda_rc(cudaMemsetAsync(wc.status, 0, kStatusInts * sizeof(int), s)));
     const int* fwd_err = nullptr;
     if (precision != PBD_PREC_FP32) {
         PBD_TRY(forward_layer_maps(f, w, wc.act, sigma, wc.lateral, lstride, precision, wc.batch,
-                                   wc.batch_bytes, s, &fwd_err));
+                                   wc.batch_bytes, s, wc.status + kStatFwd));
+        fwd_err = wc.status + kStatFwd;
     } else {
         // FP32: one single-layer job per layer through the batched forward (its own poison)
         pbd_job jobs[PBD_MAX_JOBS];
@@ -856,9 +961,8 @@ static int forward_wed_body(const pbd_field* f, const pbd_lut_spec* spec, const 
             PBD_TRY(pbd_forward_batch(jobs, n, precision, wc.batch, wc.batch_bytes, stream));
         }
     }
-    PBD_TRY(cuda_rc(cudaMemsetAsync(wc.err, 0, sizeof(int), s)));
     return lut_wed_combine(spec, f->n_layers, wc.lateral, lstride, wed, (size_t)f->nz * nslice,
-                           dose, wc.err, fwd_err, curves, curves_bytes, s);
+                           dose, wc.status + kStatCmb, fwd_err, curves, curves_bytes, s);
 }
 
 static int wed_setup(const pbd_field* f, const pbd_lut_spec* spec, int precision, void* workspace,
@@ -897,6 +1001,7 @@ int pbd_forward_wed_curves(const pbd_field* f, const pbd_lut_spec* spec, const v
 
 // ---- heterogeneous media: dL/dW -----------------------------------------------------
 struct WedAdjCarve {
+    int* status;         // status header: the per-layer adjoints' error word
     double* act;         // (L, nz) activity table
     float* maps;         // (L, wed_lateral_stride) dL/dD times each layer's depth dose
     void* adj;           // one single-layer adjoint's workspace, reused layer after layer
@@ -910,6 +1015,7 @@ static int carve_wed_adj(const pbd_field* f, int precision, void* base, WedAdjCa
     size_t ab = 0;
     PBD_TRY(pbd_adjoint_workspace(&f1, precision, &ab));
     Carve c(base);
+    w.status = c.take<int>(kStatusInts);
     w.act = c.take<double>((size_t)f->n_layers * f->nz);
     w.maps = c.take<float>((size_t)f->n_layers * wed_lateral_stride(f));
     w.adj = c.take<char>(ab);
@@ -949,15 +1055,16 @@ int pbd_adjoint_wed(const pbd_field* f, const pbd_lut_spec* spec, const void* cu
                              s));
     PBD_TRY(lut_wed_grad_maps(spec, f->n_layers, curves, curves_bytes, grad_dose, wed, nvox,
                               lstride, wc.maps, s));
+    PBD_TRY(cuda_rc(cudaMemsetAsync(wc.status, 0, kStatusInts * sizeof(int), s)));
     // layer l: the adjoint of its lateral map with depth dose 1 on its active slices
     pbd_field f1 = *f;
     f1.n_layers = 1;
     const size_t per = (size_t)f->n_sy * f->n_sx;
     for (int l = 0; l < f->n_layers; ++l)
-        PBD_TRY(pbd_adjoint(&f1, w + (size_t)l * per, wc.act + (size_t)l * f->nz,
+        PBD_TRY(adjoint_one(&f1, w + (size_t)l * per, wc.act + (size_t)l * f->nz,
                             sigma + (size_t)l * f->nz, nullptr, nullptr,
                             wc.maps + (size_t)l * lstride, grad_w + (size_t)l * per, nullptr,
-                            precision, wc.adj, wc.adj_bytes, stream));
+                            precision, wc.adj, wc.adj_bytes, wc.status + kStatAdj, s));
     return PBD_OK;
 }
 
@@ -987,7 +1094,8 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
     carve_grad(workspace, n_jobs, gp, g);
     cudaStream_t s = (cudaStream_t)stream;
-    GradBufs b{g.fwd, g.adj, g.fpart, g.fcnt + 2, g.lpart, g.apart, g.dcs, g.dsgs, g.fcnt + 1};
+    GradBufs b{g.fwd, g.adj, g.fpart, g.fcnt + 2, g.lpart, g.apart, g.dcs, g.dsgs,
+               g.status + kStatFwd, g.status};
     PBD_TRY(cuda_rc(cudaMemsetAsync(g.acnt, 0,
                                     tc_adjoint_counter_ints(n_jobs, gp.max_l) * sizeof(int), s)));
     const int a_chunk = g_adj_chunk > 0 ? g_adj_chunk : kBatchAdjChunk;
@@ -1035,10 +1143,10 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
         PBD_LAUNCH_CHECK();
         count_launch(1);
     }
-    PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr, gp.chunk, 1,
-                           precision, 0, s));
-    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, a_chunk, gp.with_range, 1, 1,
-                             s);
+    PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr,
+                           g.status + kStatFwd, gp.chunk, 1, precision, 0, s));
+    return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, g.status + kStatAdj, a_chunk,
+                             gp.with_range, 1, 1, s);
 }
 
 }  // extern "C"

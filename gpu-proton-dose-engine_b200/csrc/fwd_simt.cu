@@ -289,21 +289,16 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 }
 
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
-                   int total_items, int* counter, size_t n_counter_ints, int chunk, int with_loss,
-                   int precision, int poison, cudaStream_t s) {
+                   int total_items, int* counter, size_t n_counter_ints, int* err, int chunk,
+                   int with_loss, int precision, int poison, cudaStream_t s) {
     if (precision != PBD_PREC_FP32) {
         PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, n_counter_ints * sizeof(int), s)));
-        return launch_forward_tc(precision, jobs_dev, jobs_host, n_jobs, counter, chunk,
+        return launch_forward_tc(precision, jobs_dev, jobs_host, n_jobs, counter, err, chunk,
                                  with_loss, poison, s);
     }
-    static thread_local bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(fwd_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kFwdSmemBytes) != cudaSuccess)
-            return PBD_ERR_NO_SMEM;
-        attr_set = true;
-    }
-    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s)));
+    int set = 0;
+    PBD_TRY(smem_optin((const void*)fwd_simt_kernel, (int)kFwdSmemBytes, 0, &set));
+    PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, sizeof(int), s)));
     fwd_schedule_kernel<<<n_jobs, 256, kActStage, s>>>(jobs_dev, items, chunk);
     PBD_LAUNCH_CHECK();
     {
@@ -319,7 +314,7 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
         max_blocks = max(max_blocks, (int)std::min<size_t>((n + 255) / 256, 4096));
     }
     const int fin_blocks = with_loss ? kLossBlocks : max_blocks;
-    fwd_finalize_kernel<<<dim3(fin_blocks, n_jobs), 256, 0, s>>>(jobs_dev, with_loss, counter + 1);
+    fwd_finalize_kernel<<<dim3(fin_blocks, n_jobs), 256, 0, s>>>(jobs_dev, with_loss, err);
     PBD_LAUNCH_CHECK();
     count_launch(3);
     return PBD_OK;

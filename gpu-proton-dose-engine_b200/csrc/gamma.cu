@@ -644,16 +644,9 @@ int launch_gamma(const GammaParams& P, const T* ref, const T* ev, double* gmap,
     const size_t smem = (size_t)(kTX + 2 * P.hx) * (kTY + 2 * P.hy) * (kTZ + 2 * P.hz) *
                             sizeof(double) +
                         (size_t)P.n_off * (sizeof(double) + sizeof(int));
-    static bool attr_set = false;               // one per input type
-    if (!attr_set) {
-        PBD_TRY(cuda_rc(cudaFuncSetAttribute(gamma_kernel<T, false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kGMaxSmem)));
-        PBD_TRY(cuda_rc(cudaFuncSetAttribute(gamma_kernel<T, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kGMaxSmem)));
-        attr_set = true;
-    }
+    int set = 0;                                // once per (device, kernel)
+    PBD_TRY(smem_optin((const void*)gamma_kernel<T, false>, kGMaxSmem, 0, &set));
+    PBD_TRY(smem_optin((const void*)gamma_kernel<T, true>, kGMaxSmem, 0, &set));
     const int gx = (P.nx + kTX - 1) / kTX, gy = (P.ny + kTY - 1) / kTY;
     const int n_bricks = w.n_blocks;
     int occ = 0;

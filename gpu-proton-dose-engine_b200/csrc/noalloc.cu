@@ -20,6 +20,11 @@
 // counter and error word are cleared on every call and the work list is rewritten, but two
 // calls that overlap on the GPU (different streams, no ordering between them) race on the
 // array and must not be issued.
+//
+// The cached address belongs to the device's primary context, the one the CUDA runtime
+// uses.  It stays valid until that context is destroyed: a caller that runs
+// cudaDeviceReset() after its first call on a device, or drives the device through a
+// context of its own (the driver API), must not use this entry point on that device.
 #include <mutex>
 
 #include "pbd_internal.cuh"
@@ -50,8 +55,12 @@ int noalloc_scratch(void** out) {
     return PBD_OK;
 }
 
-__global__ void noalloc_install_kernel(JobDev J, JobDev* dst) {
-    if (threadIdx.x == 0) *dst = J;
+// Installs the job view and clears the error word (counters[1]).
+__global__ void noalloc_install_kernel(JobDev J, JobDev* dst, int* err) {
+    if (threadIdx.x == 0) {
+        *dst = J;
+        *err = 0;
+    }
 }
 
 }  // namespace
@@ -100,8 +109,9 @@ extern "C" int pbd_forward_noalloc(const pbd_field* f, const float* w, const dou
     J.partial = dose;     // chunk 0 of every slice is the output itself
     J.nchunks = nch;
     cudaStream_t s = (cudaStream_t)stream;
-    noalloc_install_kernel<<<1, 32, 0, s>>>(J, jd);
+    noalloc_install_kernel<<<1, 32, 0, s>>>(J, jd, counters + 1);
     PBD_LAUNCH_CHECK();
     count_launch(1);
-    return launch_forward(jd, &J, 1, it, items, counters, 2, chunk, 0, precision, 1, s);
+    return launch_forward(jd, &J, 1, it, items, counters, 2, counters + 1, chunk, 0, precision, 1,
+                          s);
 }

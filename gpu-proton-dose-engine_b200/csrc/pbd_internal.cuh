@@ -128,6 +128,27 @@ struct JobPlan {
 
 int fill_job(const pbd_field* f, JobDev* j);
 
+// Status header: the first sub-array of every workspace whose kernels run bounded waits
+// (kStatusInts ints at the workspace's first 256-byte boundary).  Word kStatFwd is the
+// forward's error word, kStatAdj the adjoint's, kStatCmb the heterogeneous combine's; the
+// call's first kernel (or memset) clears the header, a wait that runs out sets its word, and
+// pbd_workspace_status() reads them back.
+constexpr int kStatusInts = 16;
+enum StatusWord { kStatFwd = 0, kStatAdj = 1, kStatCmb = 2 };
+
+// Dynamic shared memory opt-in of kernel `fn` on the CURRENT device, done once per (device,
+// kernel) and cached: bytes >= 0 sets that size; bytes < 0 sets the device's opt-in maximum
+// minus the kernel's static shared memory.  *set_bytes receives the value in force.  With
+// min_regs > 0 a kernel compiled with fewer registers per thread is refused
+// (PBD_ERR_UNSUPPORTED): a setmaxnreg split needs the launch allotment it was written for.
+int smem_optin(const void* fn, int bytes, int min_regs, int* set_bytes);
+
+// Bounded device waits: the limit in ns (2 s unless the calling thread set a test limit) and
+// whether the calling thread asked the tensor-core schedulers to publish no work (a test of
+// the timeout path: every consumer wait then runs out).  Both from pbd_test_hook().
+unsigned long long wait_limit_ns();
+int test_hold();
+
 // Profiling hooks (api.cu): event pairs around the dominant kernels while enabled on
 // the calling thread, and a per-thread count of kernels this library launched.
 enum ProfKernel { kProfFwd = 0, kProfAdj = 1 };
@@ -139,13 +160,14 @@ int num_sms();
 // forward (FP32 SIMT) -- fwd_simt.cu
 int fwd_chunk_layers(const pbd_field* f, int precision);
 int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* items);
-// counter[0] = item counter, counter[1] = error word (set by a timed-out device wait).
-// FP32 path: schedule + persistent kernel + finalize.  Tensor-core precisions go to
-// launch_forward_tc after clearing `n_counter_ints` ints from `counter` (the counters and
-// the jobs' arrival arrays, laid out contiguously by the caller).
+// counter[0] = item counter; `err` = the error word (set by a timed-out device wait, read by
+// the finalize / poison passes; the caller clears it).  FP32 path: schedule + persistent
+// kernel + finalize.  Tensor-core precisions go to launch_forward_tc after clearing
+// `n_counter_ints` ints from `counter` (the counters and the jobs' arrival arrays, laid out
+// contiguously by the caller).
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
-                   int total_items, int* counter, size_t n_counter_ints, int chunk, int with_loss,
-                   int precision, int poison, cudaStream_t s);
+                   int total_items, int* counter, size_t n_counter_ints, int* err, int chunk,
+                   int with_loss, int precision, int poison, cudaStream_t s);
 
 // (slice, tile, layer-chunk) work items sorted longest-first, one CTA per job.
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
@@ -153,7 +175,8 @@ int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_job
 // adjoint (tcgen05) -- adj_tc.cu.  Units (slice, chunk of `chunk` active layers) are
 // pulled z-major; `partial` holds two (layer, slice) slot planes of nsy * nsx floats and
 // the reduction's segment partials (tc_adjoint_slot_elems); counter[0] = unit counter,
-// counter[1] = error word, then per job max_layers per-layer arrival counters.
+// counter[1] unused, then per job max_layers per-layer arrival counters; `err` = the error
+// word (cleared by the caller).
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
 size_t tc_adjoint_slot_elems(const pbd_field* f);
 // Ints of the adjoint's counter block: unit counter, error word, then per job one arrival
@@ -162,18 +185,24 @@ size_t tc_adjoint_counter_ints(int n_jobs, int max_layers);
 // counters_zeroed: the caller cleared the counter block earlier on the stream (so that no
 // memset sits between the forward and this launch, which runs as its programmatic dependent).
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      int* counter, int chunk, int with_range, int finalize_loss,
+                      int* counter, int* err, int chunk, int with_range, int finalize_loss,
                       int counters_zeroed, cudaStream_t s);
 
 // forward (tcgen05) -- tc_fwd.cu.  Work units (slice, layer chunk, tile) are enumerated
-// z-major; counter[0] = unit counter, counter[1] = error word; every job's `arrive` array
-// (nz * tiles ints, only read when a slice spans several chunks) must be zero at launch.
+// z-major; counter[0] = unit counter; every job's `arrive` array (nz * tiles ints, only read
+// when a slice spans several chunks) must be zero at launch; `err` = the error word.
 // `poison`: a follow-up kernel turns every job's dose into NaN if a device wait ran out.
 int tc_operand_dims(int precision, int nsx, int nsy, int* K1, int* N1);
 int tc_forward_units(const JobDev* jobs_host, int n_jobs, int chunk, int* cmax, int* tmax,
                      int* n_units);
 int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      int* counter, int chunk, int with_loss, int poison, cudaStream_t s);
+                      int* counter, int* err, int chunk, int with_loss, int poison,
+                      cudaStream_t s);
+
+// forward in FP64 on the CUDA cores -- fwd_f64.cu.  One block per (slice, 64 x 64 tile)
+// over all layers, writing the dose directly (no scratch).
+int launch_forward_f64(const pbd_field* f, const double* w, const double* idd,
+                       const double* sigma, double* dose, cudaStream_t s);
 
 // adjoint (FP32 SIMT) -- adj_simt.cu
 int adj_chunk_depths(const pbd_field* f);

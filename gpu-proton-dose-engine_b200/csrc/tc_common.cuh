@@ -40,11 +40,14 @@ __device__ __forceinline__ uint64_t now_ns() {
     return t;
 }
 
-__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity) {
+// Wait for phase `parity` of `bar` for at most `limit_ns` of %globaltimer; false when the
+// limit ran out (the caller sets its error word and leaves).
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity,
+                                         uint64_t limit_ns = kWaitNs) {
     if (tc::mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = now_ns();
     while (!tc::mbar_try_wait(bar, parity))
-        if (now_ns() - t0 > kWaitNs) return false;
+        if (now_ns() - t0 > limit_ns) return false;
     return true;
 }
 

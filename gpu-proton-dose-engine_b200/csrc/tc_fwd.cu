@@ -47,9 +47,11 @@
 // its squared-distance tables (kTab on the first step only); slices no layer reaches are
 // not written.
 //
-// Every wait is bounded (2 s of %globaltimer).  A warp whose wait runs out sets the error
-// word and leaves its loop; the waits of the others then run out in turn.  The dose is
-// invalid after that and the callers poison the results (NaN) from the error word.
+// Every wait is bounded (2 s of %globaltimer, or a test limit).  A warp whose wait runs out
+// sets the error word and leaves its loop; the waits of the others then run out in turn.
+// The dose is invalid after that and the callers poison the results (NaN) from the error
+// word.  A warp leaves only after the MMAs it issued have completed (or its wait for them ran
+// out), and the block frees its TMEM after a final barrier of all warps.
 //
 // Precision modes (accumulation always FP32):
 //   TF32X3  a b ~ ah bh + ah bl + al bh with ah = tf32(a), al = tf32(a - ah)  (~1e-7)
@@ -97,7 +99,10 @@ struct Step {
 struct Params {
     const JobDev* jobs;
     int n_jobs, chunk, cmax, tmax, n_units;
-    int* counter;       // [0] unit counter, [1] error word
+    int* counter;       // [0] unit counter
+    int* err;           // error word: set when a bounded wait ran out
+    unsigned long long wait_ns;   // limit of every bounded wait
+    int hold;           // test of the timeout path: the scheduler publishes no step
     int with_loss;
     int K1, N1, na2;    // operand dims; A2 buffers (1 or 2)
     int ty4, tx4;       // float4 groups of the per-thread distance table: y part, x part
@@ -116,7 +121,7 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
     // Wait for slot k to be free; lane `src` writes it and arrives on `full`.
     auto push = [&](int src, const Step& st) -> bool {
         const int slot = k % kRing, n = k / kRing;
-        const bool w = wait_bar(&empty[slot], (uint32_t)((n & 1) ^ 1));
+        const bool w = wait_bar(&empty[slot], (uint32_t)((n & 1) ^ 1), P.wait_ns);
         if (!__all_sync(FULL, w)) return false;
         if (lane == src) {
             ring[slot] = st;
@@ -127,6 +132,8 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
         return true;
     };
 
+    // timeout-path test: publish nothing, so that every consumer's first wait runs out
+    if (P.hold) return;
     for (;;) {
         int u = 0;
         if (lane == 0) u = atomicAdd(P.counter, 1);
@@ -303,7 +310,7 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
     bool ok = true;
     for (;;) {
         const int slot = k % kRing;
-        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1));
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
         const int flags = ring[slot].flags;
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[slot]);
@@ -314,7 +321,7 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
         const uint32_t par = (uint32_t)(n & 1);
         const uint32_t a2h = sbase + L.a2 + (P.na2 == 2 ? (uint32_t)(n & 1) * L.a2_stride : 0u);
         if (do1) {
-            ok = wait_bar(ops1, par);
+            ok = wait_bar(ops1, par, P.wait_ns);
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::fence_after_sync();
             if (lane == 0) {
@@ -325,7 +332,7 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
             __syncwarp();
         }
         if (do2) {
-            ok = wait_bar(ops2, par);
+            ok = wait_bar(ops2, par, P.wait_ns);
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::fence_after_sync();
             if (lane == 0) {
@@ -340,11 +347,11 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
         }
         ++n;
     }
-    if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
+    if (!ok && lane == 0) atomicExch(P.err, 1);
     // this warp's last MMAs must be complete before the block frees its TMEM
     if (n > 0) {
-        if (do1) (void)wait_bar(mma1, (uint32_t)((n - 1) & 1));
-        if (do2) (void)wait_bar(mma2, (uint32_t)((n - 1) & 1));
+        if (do1) (void)wait_bar(mma1, (uint32_t)((n - 1) & 1), P.wait_ns);
+        if (do2) (void)wait_bar(mma2, (uint32_t)((n - 1) & 1), P.wait_ns);
     }
 }
 
@@ -467,7 +474,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
 
     // D of the previous step into the registers (+ the unit's small sum when it ended it).
     auto drain = [&]() {
-        ok = ok && wait_bar(mma2, ph2);
+        ok = ok && wait_bar(mma2, ph2, P.wait_ns);
         if (ok) ph2 ^= 1;
         tc::fence_after_sync();
         uint32_t r[4][16];
@@ -575,7 +582,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
     for (;;) {
         // ---- next step ----
         const int slot = k % kRing;
-        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1));
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
         const Step cur = ring[slot];
         if (cur.flags != kEnd && (cur.job < 0 || cur.job >= P.n_jobs)) ok = false;
         __syncwarp();
@@ -744,7 +751,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         }
 
         // ---- E1: U = stage-1 result, scaled and split -> B2 (x rows, K2 = j) ----
-        ok = ok && wait_bar(mma1, ph1);
+        ok = ok && wait_bar(mma1, ph1, P.wait_ns);
         if (ok) ph1 ^= 1;
         if (!__all_sync(0xffffffffu, ok)) break;
         tc::fence_after_sync();
@@ -795,7 +802,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         drain();
         if (__all_sync(0xffffffffu, ok)) output(prev);
     }
-    if (!ok && lane == 0) atomicExch(P.counter + 1, 1);
+    if (!ok && lane == 0) atomicExch(P.err, 1);
 }
 
 // MAPS: the per-layer-maps mode, a separate instantiation so that the dose kernel's code and
@@ -889,24 +896,9 @@ size_t smem_bytes(int K1, int N1, int na2) {
 
 template <int MODE, bool MAPS>
 int launch_mode(const Params& P0, cudaStream_t s) {
-    static thread_local int max_dyn = 0;
-    if (max_dyn == 0) {
-        int dev = 0, optin = 0;
-        cudaFuncAttributes fa;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
-                cudaSuccess ||
-            cudaFuncGetAttributes(&fa, fwd_tc_kernel<MODE, MAPS>) != cudaSuccess)
-            return PBD_ERR_CUDA;
-        // the setmaxnreg split needs the full launch allotment, or its increase never returns
-        if (fa.numRegs < kLaunchRegsNeeded) return PBD_ERR_UNSUPPORTED;
-        const int avail = optin - (int)fa.sharedSizeBytes;
-        if (avail <= 0 || cudaFuncSetAttribute(fwd_tc_kernel<MODE, MAPS>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               avail) != cudaSuccess)
-            return PBD_ERR_NO_SMEM;
-        max_dyn = avail;
-    }
+    // the setmaxnreg split needs the full launch allotment, or its increase never returns
+    int max_dyn = 0;
+    PBD_TRY(smem_optin((const void*)fwd_tc_kernel<MODE, MAPS>, -1, kLaunchRegsNeeded, &max_dyn));
     Params P = P0;
     table_groups<MODE>(P.K1, P.N1, &P.ty4, &P.tx4);
     P.na2 = 2;
@@ -953,12 +945,16 @@ int tc_forward_units(const JobDev* jobs_host, int n_jobs, int chunk, int* cmax, 
 }
 
 int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
-                      int* counter, int chunk, int with_loss, int poison, cudaStream_t s) {
+                      int* counter, int* err, int chunk, int with_loss, int poison,
+                      cudaStream_t s) {
     Params P{};
     P.jobs = jobs_dev;
     P.n_jobs = n_jobs;
     P.chunk = chunk;
     P.counter = counter;
+    P.err = err;
+    P.wait_ns = wait_limit_ns();
+    P.hold = test_hold();
     P.with_loss = with_loss;
     for (int j = 0; j < n_jobs; ++j) {
         int k1 = 0, n1 = 0;
@@ -991,7 +987,7 @@ int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     PBD_TRY(rc);
     count_launch(1);
     if (poison) {
-        fwd_poison_kernel<<<num_sms(), 256, 0, s>>>(jobs_dev, n_jobs, counter + 1);
+        fwd_poison_kernel<<<num_sms(), 256, 0, s>>>(jobs_dev, n_jobs, err);
         PBD_LAUNCH_CHECK();
         count_launch(1);
     }

@@ -22,7 +22,7 @@ from . import physics as ph
 from .model import PBProblem
 
 INV_SQRT_2PI = 1.0 / np.sqrt(2.0 * np.pi)
-DEFAULT_PRECISION = "fp32"
+DEFAULT_PRECISION = "tf32x3"   # tcgen05 hi/lo split: within 1e-6 of FP64 and faster than FP32
 DEFAULT_FD_STEP = 0.005   # cm: central-difference step of the range-derivative tables
 
 
@@ -103,7 +103,7 @@ class DosePlan:
         self.torch = torch
         self.device = torch.device(device or "cuda")
         self.problem = problem
-        self.field = problem.field_descriptor()
+        self.field = _lib.field_of(problem)
         _lib.call("pbd_field_validate", ctypes.byref(self.field))
         self.precision = _lib.precision_code(precision)
         self.fd_step = float(fd_step)
@@ -111,7 +111,8 @@ class DosePlan:
         self.shape = (g.nz, g.ny, g.nx)
         self.w = torch.as_tensor(np.ascontiguousarray(L.ensure_weights(), dtype=np.float32),
                                  device=self.device)
-        self.energies = None if L.energies is None else np.asarray(L.energies, dtype=np.float64)
+        en = getattr(L, "energies", None)
+        self.energies = None if en is None else np.asarray(en, dtype=np.float64)
         self.ws = _Workspace(self.device)
         self.schedule = None          # (layers per forward item, adjoint item size) or None
         self._tuned = False           # cached tuning lookup (False = not looked up yet)
@@ -199,6 +200,33 @@ class DosePlan:
                       _lib.ptr(sigma), _lib.ptr(out), self.precision, _lib.ptr(ws), ws.numel(),
                       _lib.stream_handle(self.device))
         return out
+
+    def forward_f64(self, w=None, out=None):
+        """The dose in FP64 on the CUDA cores (pbd_forward_f64): weights, Gaussians, products
+        and sums in float64.  ``w`` defaults to the plan's weights (float32 values, exact in
+        float64); returns a float64 (nz, ny, nx) tensor."""
+        torch = self.torch
+        if w is None:
+            w = self.w
+        elif not torch.is_tensor(w):
+            w = torch.as_tensor(np.asarray(w, dtype=np.float64))
+        w = w.to(self.device, torch.float64).contiguous()
+        _lib.check_arg(w, "w", self.w.numel(), torch.float64, self.device)
+        self._check_tables(self.idd, self.sigma)
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float64, device=self.device)
+        nvox = self.shape[0] * self.shape[1] * self.shape[2]
+        _lib.check_arg(out, "out", nvox, torch.float64, self.device)
+        _lib.call("pbd_forward_f64", ctypes.byref(self.field), _lib.ptr(w), _lib.ptr(self.idd),
+                  _lib.ptr(self.sigma), _lib.ptr(out), _lib.stream_handle(self.device))
+        return out
+
+    def check(self, op: str = "fwd") -> None:
+        """Raise PbdError(PBD_ERR_TIMEOUT) if a device wait of the plan's last ``op`` call
+        ("fwd", "adj" or "lossgrad") ran out (its outputs are NaN then); synchronises."""
+        ws = self.ws._bufs.get(op)
+        if ws is not None:
+            _lib.check_workspace(ws, f"DosePlan.{op}", _lib.stream_handle(self.device))
 
     # -- adjoint -------------------------------------------------------------------
     def adjoint(self, grad_dose, w=None, idd=None, sigma=None, didd=None, dsig=None,
@@ -349,38 +377,51 @@ def separable_dose(w, range_shift, plan: DosePlan):
     return _SEPARABLE_DOSE.apply(w, range_shift, plan)
 
 
-def torch_separable(problem: PBProblem, device: str = "cuda", dtype=None, allow_tf32: bool = False,
+def torch_separable(problem, device: str = "cuda", dtype=None, allow_tf32: bool = False,
                     per_layer: bool = True, layer_chunk: Optional[int] = None,
                     return_timing: bool = False, return_intermediates: bool = False,
                     precision: Optional[str] = None):
     """Drop-in for the reference's per-layer batched-matmul engine (engines.py:208-283).
 
-    Same arguments and return value: a float32 CUDA tensor D of shape (nz, ny, nx), or
-    (D, seconds) with ``return_timing``.  Like the reference it uploads the problem's
-    arrays on every call and synchronises before returning.  Differences, all loud:
-    ``device`` must be CUDA (no CPU path), ``dtype`` must be float32 (the contraction
-    is FP32 or a split tensor-core form, within 1e-6 of FP64), and ``per_layer=False``
-    (the single-sigma approximation) is not provided.  ``allow_tf32=True`` selects
-    plain TF32 tensor cores; ``precision`` picks any mode explicitly; ``layer_chunk``
-    sets the layers per work item."""
+    Same arguments and return value: a CUDA tensor D of shape (nz, ny, nx), or
+    (D, seconds) with ``return_timing``.  ``problem`` may be the reference's own
+    PBProblem: only ``grid``, ``lattice`` (axes, spot pitch and offsets,
+    ``ensure_weights()``) and ``idd`` / ``sigma`` are read, as the reference does
+    (engines.py:227-234, 257-259).  Like the reference it uploads the problem's arrays on
+    every call and synchronises before returning.
+
+    * ``dtype``: None or torch.float32 give a float32 dose from the tensor cores (split
+      TF32, three products: within 1e-6 of FP64); torch.float64 gives a float64 dose
+      computed in FP64 on the CUDA cores (the reference's float64 mode, ~1e-15).
+    * ``allow_tf32``: the reference's flag for TF32 tensor cores; its run with the flag
+      kept FP32 accuracy (1.51e-7, benchmark_full.json:68-81), so it maps to the split TF32
+      form as well.  One-product TF32 (~1e-4) is available only as ``precision="tf32"``.
+    * ``precision``: any mode explicitly ("fp32", "tf32x3", "bf16x3", "tf32", "bf16").
+    * ``layer_chunk``: active layers per forward work item, for this call only (the
+      reference used it to bound memory; here it only sets the work granularity).
+
+    Differences, all loud: ``device`` must be CUDA (no CPU path) and ``per_layer=False``
+    (the single-sigma approximation) is not provided.  A device wait that ran out raises
+    PbdError (PBD_ERR_TIMEOUT)."""
     torch = _lib.require_cuda()
     if not str(device).startswith("cuda"):
         raise RuntimeError("torch_separable: this engine runs on CUDA only (no CPU path)")
-    if dtype not in (None, torch.float32):
-        raise NotImplementedError("torch_separable: the device contraction returns float32")
+    if dtype not in (None, torch.float32, torch.float64):
+        raise NotImplementedError(f"torch_separable: dtype {dtype} (float32 or float64 only)")
     if not per_layer:
         raise NotImplementedError("torch_separable: the single-sigma approximation "
                                   "(per_layer=False) is not provided; use per_layer=True")
-    prec = precision or ("tf32" if allow_tf32 else DEFAULT_PRECISION)
+    prec = precision or DEFAULT_PRECISION
     t0 = time.perf_counter()
+    plan = DosePlan(problem, precision=prec, tables="problem", device=device)
     if layer_chunk:
-        _lib.call("pbd_set_schedule", int(layer_chunk), 0)
-    try:
-        plan = DosePlan(problem, precision=prec, tables="problem", device=device)
-        dose = plan.forward()
+        plan.schedule = (int(layer_chunk), 0)
+    if dtype == torch.float64:
+        dose = plan.forward_f64(np.ascontiguousarray(problem.lattice.ensure_weights(),
+                                                     dtype=np.float64))
         torch.cuda.synchronize(plan.device)
-    finally:
-        if layer_chunk:
-            _lib.call("pbd_set_schedule", 0, 0)
+    else:
+        dose = plan.forward()
+        plan.check("fwd")        # synchronises; raises if a device wait ran out
     t1 = time.perf_counter()
     return (dose, t1 - t0) if return_timing else dose

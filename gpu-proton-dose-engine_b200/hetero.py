@@ -62,7 +62,7 @@ class WedPlan:
         g, L = problem.grid, problem.lattice
         if L.energies is None:
             raise ValueError("the heterogeneous dose needs lattice.energies")
-        self.field = problem.field_descriptor()
+        self.field = _lib.field_of(problem)
         self.precision = _lib.precision_code(precision)
         self.spec = ph.lut_spec(g.nz, g.oz, g.dz, idd_model=idd_model, sigma_x0=sigma_x0)
         self.energies = torch.as_tensor(np.asarray(L.energies, dtype=np.float64), device=self.device)

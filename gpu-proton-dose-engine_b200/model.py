@@ -134,11 +134,9 @@ class PBProblem:
         return self.grid.nz
 
     def field_descriptor(self) -> _lib.Field:
-        """The C ABI's pbd_field for this problem."""
-        g, L = self.grid, self.lattice
-        return _lib.Field(nx=g.nx, ny=g.ny, nz=g.nz, dx=g.dx, dy=g.dy, dz=g.dz, ox=g.ox, oy=g.oy,
-                          oz=g.oz, n_sx=L.n_sx, n_sy=L.n_sy, n_layers=L.n_layers,
-                          dx_spot=L.dx_spot, dy_spot=L.dy_spot, x0=L.x0, y0=L.y0)
+        """The C ABI's pbd_field for this problem (``_lib.field_of``, which the engines use so
+        that the reference's own PBProblem, which has no such method, works too)."""
+        return _lib.field_of(self)
 
     def summary(self) -> str:
         g, L = self.grid, self.lattice

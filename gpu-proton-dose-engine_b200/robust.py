@@ -57,7 +57,7 @@ class ScenarioBatch:
                                     anchor_surface=True, device=self.device,
                                     fd_step=fd_step if with_grad else 0.0)
                 d = torch.empty((g.nz, g.ny, g.nx), dtype=torch.float32, device=self.device)
-                f = p.field_descriptor()
+                f = _lib.field_of(p)
                 f.x0 = L.x0 + s.dx
                 f.y0 = L.y0 + s.dy
                 self.jobs[k] = _lib.Job(field=f, w=_lib.ptr(w), idd=_lib.ptr(t.idd),

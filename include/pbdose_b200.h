@@ -112,9 +112,10 @@ PBD_API int pbd_version(void);
 /* Validates a field descriptor; replaces pb_problem_validate, pencil_beam.cu:717-730. */
 PBD_API int pbd_field_validate(const pbd_field *f);
 /* Work-item granularity of the calling host thread's subsequent calls (0 = built-in
- * default): energy layers per forward item, depth slices per adjoint item.  The
- * workspace queries use the same setting, so set it before sizing.  No counterpart in
- * the reference (it plays the role of engines.torch_separable's layer_chunk knob). */
+ * default): energy layers per forward item, depth slices per adjoint item.  The setting is
+ * per host thread (calls from other threads keep their own), and the workspace queries use
+ * it too, so set it before sizing.  No counterpart in the reference (it plays the role of
+ * engines.torch_separable's layer_chunk knob). */
 PBD_API int pbd_set_schedule(int fwd_layers_per_item, int adj_depths_per_item);
 /* Measurement utilities (no counterpart in the reference).  Between begin and end, the
  * calling thread's forward and adjoint calls record CUDA events around their main dose
@@ -124,6 +125,23 @@ PBD_API int pbd_profile_begin(void);
 PBD_API int pbd_profile_end(double *fwd_ms, int *n_fwd, double *adj_ms, int *n_adj);
 /* Number of kernels this library has launched from the calling thread so far. */
 PBD_API int pbd_launch_count(long long *n);
+
+/* Status of the last call that used `workspace` (no counterpart in the reference, whose
+ * kernels never wait on one another).  The kernels' waits on each other are bounded (2 s);
+ * a wait that runs out makes the call's results NaN and sets a status word at the start of
+ * its workspace.  This reads those words on `stream`, waits for the stream, and stores
+ * PBD_OK or PBD_ERR_TIMEOUT in *status.  Valid after pbd_forward, pbd_adjoint, pbd_loss_grad,
+ * pbd_forward_batch, pbd_loss_grad_batch, pbd_forward_wed(_curves) and pbd_adjoint_wed; not
+ * for use inside stream capture. */
+PBD_API int pbd_workspace_status(const void *workspace, size_t workspace_bytes, int *status,
+                                 void *stream);
+/* Test hook of the timeout path (no counterpart in the reference).  For the calling thread's
+ * later calls: wait_limit_ns bounds every device wait of the tensor-core forward and adjoint
+ * (0 = the default 2 s), and hold_schedulers = 1 makes their scheduler warps publish no work,
+ * so that every other warp's first wait runs out after wait_limit_ns (which must then be
+ * non-zero) -- no tensor-core instruction is issued, the kernels end, the outputs are NaN and
+ * pbd_workspace_status reports PBD_ERR_TIMEOUT.  pbd_test_hook(0, 0) restores the defaults. */
+PBD_API int pbd_test_hook(unsigned long long wait_limit_ns, int hold_schedulers);
 
 /* ---- depth-LUT builder (FP64, on the device) -------------------------------------
  * Replaces the per-layer host loop of model.py:225-233 (physics.idd_pristine with
@@ -148,6 +166,15 @@ PBD_API int pbd_forward(const pbd_field *f, const float *w, const double *idd, c
                 float *dose, int precision, void *workspace, size_t workspace_bytes,
                 void *stream);
 
+/* ---- forward dose in FP64 ----------------------------------------------------------
+ * Replaces engines.torch_separable(..., dtype=torch.float64) on CUDA, engines.py:223-224 and
+ * 230-274 (operands and both batched matmuls in float64).  The dose of pbd_forward with the
+ * weights, Gaussians, products and sums in float64 on the CUDA cores: w (L, nsy, nsx) and
+ * dose (nz, ny, nx) are float64.  No workspace: one block per (64 x 64 voxel tile, slice) sums
+ * every layer in layer order and writes its voxels once. */
+PBD_API int pbd_forward_f64(const pbd_field *f, const double *w, const double *idd,
+                            const double *sigma, double *dose, void *stream);
+
 /* ---- forward dose without any device allocation ----------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory: a
  * real-time adaptive-therapy loop that reserves its memory once at start-up and must not
@@ -158,7 +185,9 @@ PBD_API int pbd_forward(const pbd_field *f, const float *w, const double *idd, c
  * items must fit the 1 MiB (about 32,000 items); otherwise PBD_ERR_UNSUPPORTED or
  * PBD_ERR_WORKSPACE.  The first call on a device resolves the array's device address,
  * so make it before any stream capture.  Calls share the array: two calls that overlap
- * on the GPU race, so order them (same stream) or do not overlap them. */
+ * on the GPU race, so order them (same stream) or do not overlap them.  The resolved address
+ * belongs to the device's primary context: after cudaDeviceReset(), or from a context the
+ * caller created through the driver API, this entry point must not be used on that device. */
 PBD_API int pbd_forward_noalloc(const pbd_field *f, const float *w, const double *idd,
                                 const double *sigma, float *dose, int precision, void *stream);
 

@@ -189,3 +189,102 @@ def test_slab_plans_sum_to_full_field(pb, world):
     assert rel(dose.cpu().numpy(), full["dose"].cpu().numpy()) < 1e-6
     with pytest.raises(RuntimeError):
         parts[0].loss_grad(m, p)       # world > 1 without a process group
+
+
+# ------------------------------------------------------------- the full robust workload
+# 4 uneven fields (21x21x16, 33x33x28, 41x41x40, 51x41x48 spots x layers) x 25 scenarios on
+# 128^3 voxels: the batched forward (one persistent launch) and the batched loss gradient
+# (one forward + one adjoint launch for all 100 jobs), every job against the float64 oracle.
+# * Tables: every distinct (depth shift, range scaling) pair of every field, built on the
+#   device, against the oracle's scenario tables: 1e-9 of max.
+# * Dose: each job's dose on 8 depth slices (including the slice of its maximum) against the
+#   oracle's separable sum fed the job's own tables: 1e-6 of max (TF32x3).
+# * Gradients: each job's loss, dL/dW and dL/dR against float64 autograd through the
+#   oracle's torch engine: loss 1e-6 relative, dL/dW and dL/dR 1e-4 of max (split-BF16
+#   adjoint).
+CFG3_SLICES = (0, 17, 40, 63, 85, 100, 127)
+
+
+@pytest.fixture(scope="module")
+def cfg3(pb):
+    import torch
+    fields = pb.workloads.robust_fields()
+    scen = pb.workloads.robust_scenarios()
+    probs = pb.robust.robust_problems(fields)
+    b = pb.robust.ScenarioBatch(probs, scen, precision="tf32x3", with_grad=True)
+    b.run()
+    g = fields[0]["grid"]
+    m_np, p_np = pb.workloads.target_loss_arrays(g)
+    m = torch.as_tensor(m_np, device="cuda")
+    p = torch.as_tensor(p_np, device="cuda")
+    outs = b.loss_grad_all(m, p)
+    torch.cuda.synchronize()
+    doses = [d.cpu().numpy() for d in b.doses]
+    grads = [{k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in o.items()}
+             for o in outs]
+    return fields, scen, probs, b, doses, grads, m_np, p_np
+
+
+def test_cfg3_tables_vs_oracle(pb, cfg3):
+    fields, scen, probs, b, *_ = cfg3
+    seen = set()
+    for k in range(b.n_jobs):
+        fi, si = divmod(k, len(scen))
+        sx, sy, sz, sc = scen[si]
+        if (fi, sz, sc) in seen:
+            continue
+        seen.add((fi, sz, sc))
+        g = probs[fi].grid
+        en = probs[fi].lattice.energies
+        idd, sig = pr.scenario_luts(g.oz - sz, g.dz, g.nz, en, depth_scale=sc)
+        t = b.tables[k]
+        assert rel(t.idd.cpu().numpy(), idd) < 1e-9, (fi, sz, sc)
+        assert rel(t.sigma.cpu().numpy(), sig) < 1e-9, (fi, sz, sc)
+    assert len(seen) == 4 * 9
+
+
+def test_cfg3_doses_vs_oracle(pb, cfg3):
+    fields, scen, probs, b, doses, *_ = cfg3
+    worst = 0.0
+    for k in range(b.n_jobs):
+        fi, si = divmod(k, len(scen))
+        sx, sy, sz, sc = scen[si]
+        prob, t, d = probs[fi], b.tables[k], doses[k]
+        g, L = prob.grid, prob.lattice
+        zs = sorted(set(CFG3_SLICES) | {int(np.argmax(d.reshape(g.nz, -1).max(axis=1)))})
+        idd = t.idd.cpu().numpy()[:, zs]
+        sig = t.sigma.cpu().numpy()[:, zs]
+        ref = er.separable_f64(g.x, g.y, L.spot_x + sx, L.spot_y + sy, fields[fi]["weights"],
+                               idd, sig)
+        err = float(np.max(np.abs(d[zs] - ref)) / np.max(np.abs(ref)))
+        worst = max(worst, err)
+        assert err < DOSE_TOL["tf32x3"], (k, err)
+    print(f"cfg3: worst dose error over 100 jobs {worst:.2e}")
+
+
+def test_cfg3_gradients_vs_oracle(pb, cfg3):
+    import torch
+    fields, scen, probs, b, doses, grads, m_np, p_np = cfg3
+    mask = torch.as_tensor(m_np, dtype=torch.float64)
+    presc = torch.as_tensor(p_np, dtype=torch.float64)
+    worst = [0.0, 0.0, 0.0]
+    for k in range(b.n_jobs):
+        fi, si = divmod(k, len(scen))
+        sx, sy, sz, sc = scen[si]
+        prob, t, o = probs[fi], b.tables[k], grads[k]
+        g, L = prob.grid, prob.lattice
+        wt = torch.tensor(fields[fi]["weights"].astype(np.float64), requires_grad=True)
+        it = torch.tensor(t.idd.cpu().numpy(), requires_grad=True)
+        st = torch.tensor(t.sigma.cpu().numpy(), requires_grad=True)
+        d = er.separable_torch(g.x, g.y, L.spot_x + sx, L.spot_y + sy, wt, it, st)
+        loss = er.masked_quadratic_loss(d, mask, presc)
+        loss.backward()
+        gr = ((it.grad * t.didd_dr.cpu().double()).sum(1)
+              + (st.grad * t.dsigma_dr.cpu().double()).sum(1)).numpy()
+        e = (abs(float(o["loss"]) - float(loss)) / abs(float(loss)),
+             rel(o["grad_w"], wt.grad.numpy()), rel(o["grad_range"], gr))
+        worst = [max(a, c) for a, c in zip(worst, e)]
+        assert e[0] <= 1e-6, (k, e)
+        assert e[1] < 1e-4, (k, e)
+        assert e[2] < 1e-4, (k, e)
+    print(f"cfg3: worst loss / dL/dW / dL/dR errors over 100 jobs {worst}")

@@ -29,7 +29,7 @@ def _inputs(pb, torch, prob):
 
 
 def _with_workspace(pb, torch, lib, prob, prec):
-    f = prob.field_descriptor()
+    f = pb._lib.field_of(prob)
     w, idd, sig = _inputs(pb, torch, prob)
     out = torch.empty(prob.grid.shape, dtype=torch.float32, device="cuda")
     n = ctypes.c_size_t(0)
@@ -44,7 +44,7 @@ def _with_workspace(pb, torch, lib, prob, prec):
 
 
 def _without(pb, torch, lib, prob, prec):
-    f = prob.field_descriptor()
+    f = pb._lib.field_of(prob)
     w, idd, sig = _inputs(pb, torch, prob)
     out = torch.full(prob.grid.shape, 7.0, dtype=torch.float32, device="cuda")   # stale bytes
     rc = lib.pbd_forward_noalloc(ctypes.byref(f), w.data_ptr(), idd.data_ptr(), sig.data_ptr(),
@@ -69,6 +69,27 @@ def _fields(pb):
     return a, b
 
 
+def _deep_field(pb):
+    """64 layers (the entry point's limit: one item holds every layer of its slice) on a
+    128 x 96 grid, with slices that no layer reaches (all-zero depth-dose columns)."""
+    rng = np.random.default_rng(17)
+    M = pb.model
+    nl, nz = 64, 12
+    grid = M.DoseGrid(128, 96, nz, 0.2, 0.2, 0.25, -12.7, -9.5, 0.0)
+    w = rng.uniform(0.2, 1.2, (nl, 21, 25))
+    lat = M.SpotLattice(25, 21, nl, 0.5, 0.5, x0=0.1, y0=-0.05, weights=w)
+    idd = rng.uniform(0.1, 3.0, (nl, nz))
+    idd[rng.random((nl, nz)) < 0.2] = 0.0
+    idd[:, [3, 8]] = 0.0                        # slices no layer reaches
+    return M.PBProblem(grid, lat, idd, rng.uniform(0.3, 0.9, (nl, nz)))
+
+
+def _oracle(prob):
+    from oracle import engine_ref as er
+    g, L = prob.grid, prob.lattice
+    return er.separable_f64(g.x, g.y, L.spot_x, L.spot_y, L.weights, prob.idd, prob.sigma)
+
+
 @pytest.mark.parametrize("prec", [0, 1])   # FP32 and TF32x3
 def test_noalloc_matches_workspace_forward_two_calls(prec):
     import torch
@@ -81,6 +102,25 @@ def test_noalloc_matches_workspace_forward_two_calls(prec):
         ref = _with_workspace(pb, torch, lib, prob, prec)
         err = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
         assert err <= DOSE_TOL, err
+    # the ragged second field against the float64 oracle directly
+    ref64 = _oracle(second)
+    assert float(np.max(np.abs(got2 - ref64)) / np.max(np.abs(ref64))) <= DOSE_TOL
+
+
+@pytest.mark.parametrize("prec", [0, 1])   # FP32 and TF32x3
+def test_noalloc_64_layers_and_empty_slices(prec):
+    import torch
+    pb = load_pkg()
+    lib = pb._lib.load()
+    prob = _deep_field(pb)
+    got = _without(pb, torch, lib, prob, prec)
+    got_again = _without(pb, torch, lib, prob, prec)
+    ref = _with_workspace(pb, torch, lib, prob, prec)
+    ref64 = _oracle(prob)
+    for g in (got, got_again):
+        assert float(np.max(np.abs(g - ref)) / np.max(np.abs(ref))) <= DOSE_TOL
+        assert float(np.max(np.abs(g - ref64)) / np.max(np.abs(ref64))) <= DOSE_TOL
+        assert np.all(g[[3, 8]] == 0.0)          # stale bytes overwritten with zeros
 
 
 def test_noalloc_rejects_what_does_not_fit():
