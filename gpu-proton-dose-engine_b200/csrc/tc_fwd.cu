@@ -604,6 +604,16 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         const int nsx = cur.nsx, nsy = cur.nsy;
         const float a2 = cur.a2;
 
+        // With one Gy buffer (lattices too wide for two), the previous step's stage 2 reads the
+        // buffer this step's G overwrites: drain that step (its completion) first.
+        bool drained = false;
+        if (P.na2 == 1 && have_prev) {
+            drain();
+            if (!__all_sync(0xffffffffu, ok)) break;
+            if (prev.flags & kLast) output(prev);
+            drained = true;
+        }
+
         // ---- W_l loads, consumed after the Gaussian generation ----
         float wv[kWReg][EPC];
         {
@@ -744,7 +754,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         if (lane == 0) tc::mbar_arrive(ops1);
 
         // ---- DR: previous step's D; its unit's output when it was the unit's last step ----
-        if (have_prev) {
+        if (have_prev && !drained) {
             drain();
             if (!__all_sync(0xffffffffu, ok)) break;
             if (prev.flags & kLast) output(prev);

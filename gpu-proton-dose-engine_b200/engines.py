@@ -22,7 +22,17 @@ from . import physics as ph
 from .model import PBProblem
 
 INV_SQRT_2PI = 1.0 / np.sqrt(2.0 * np.pi)
-DEFAULT_PRECISION = "tf32x3"   # tcgen05 hi/lo split: within 1e-6 of FP64 and faster than FP32
+# "auto": the tensor cores' hi/lo split (TF32x3, within 1e-6 of FP64 and faster than FP32) for
+# lattices they take (<= 64 x 64 spots), else the FP32 kernel on the CUDA cores
+DEFAULT_PRECISION = "auto"
+
+
+def resolve_precision(precision, lattice) -> int:
+    """Library precision code of ``precision`` for a lattice ("auto": see DEFAULT_PRECISION)."""
+    if precision is None or str(precision).lower() == "auto":
+        wide = int(lattice.n_sx) > 64 or int(lattice.n_sy) > 64
+        return _lib.PREC["fp32" if wide else "tf32x3"]
+    return _lib.precision_code(precision)
 DEFAULT_FD_STEP = 0.005   # cm: central-difference step of the range-derivative tables
 
 
@@ -105,7 +115,7 @@ class DosePlan:
         self.problem = problem
         self.field = _lib.field_of(problem)
         _lib.call("pbd_field_validate", ctypes.byref(self.field))
-        self.precision = _lib.precision_code(precision)
+        self.precision = resolve_precision(precision, problem.lattice)
         self.fd_step = float(fd_step)
         g, L = problem.grid, problem.lattice
         self.shape = (g.nz, g.ny, g.nx)
@@ -391,8 +401,9 @@ def torch_separable(problem, device: str = "cuda", dtype=None, allow_tf32: bool 
     every call and synchronises before returning.
 
     * ``dtype``: None or torch.float32 give a float32 dose from the tensor cores (split
-      TF32, three products: within 1e-6 of FP64); torch.float64 gives a float64 dose
-      computed in FP64 on the CUDA cores (the reference's float64 mode, ~1e-15).
+      TF32, three products: within 1e-6 of FP64; lattices wider than 64 spots use the FP32
+      kernel on the CUDA cores); torch.float64 gives a float64 dose computed in FP64 on the
+      CUDA cores (the reference's float64 mode, ~1e-15).
     * ``allow_tf32``: the reference's flag for TF32 tensor cores; its run with the flag
       kept FP32 accuracy (1.51e-7, benchmark_full.json:68-81), so it maps to the split TF32
       form as well.  One-product TF32 (~1e-4) is available only as ``precision="tf32"``.

@@ -2,7 +2,8 @@
 
 Tolerances (written here, not tuned per run):
   * depth tables (FP64 device builder) vs the reference's NumPy: 1e-9 of the table max;
-  * dose, FP32 path: max |dD| / max D <= 1e-6 against the float64 oracle;
+  * dose, FP32 path (precision="fp32", the CUDA-core kernels; the tensor-core modes are in
+    test_gpu_tensorcore.py): max |dD| / max D <= 1e-6 against the float64 oracle;
   * gradients: dL/dW within 1e-4 (relative to max |g|) of float64 autograd through the
     oracle's separable engine; dL/dR within 1e-4 of float64 central differences.
 """
@@ -91,7 +92,7 @@ def test_forward_cfg0_vs_reference_dose(pb):
     wl = pb.workloads.build_workload(0)
     lut = golden("luts_cfg0.npz")
     prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
-    d = pb.engines.torch_separable(prob, "cuda")
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32")
     assert d.shape == (64, 32, 32) and str(d.dtype) == "torch.float32"
     assert rel(d.cpu().numpy(), golden("dose_cfg0.npz")["dose"]) < DOSE_TOL
 
@@ -102,7 +103,7 @@ def test_forward_engine_check_case(pb):
     grid = M.DoseGrid(24, 24, 32, 0.25, 0.25, 0.25, -3.0, -3.0, 0.0)
     lat = M.SpotLattice(3, 3, 3, 0.5, 0.5, energies=g["energies"], weights=g["w"])
     prob = M.PBProblem(grid, lat, g["idd"], g["sigma"])
-    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32").cpu().numpy()
     assert rel(d, g["dose_naive"]) < DOSE_TOL
     assert rel(d, g["dose_sep"]) < DOSE_TOL
 
@@ -112,7 +113,7 @@ def test_forward_cfg1_clinical(pb):
     wl = pb.workloads.build_workload(1)
     lut = golden("luts_cfg1.npz")
     prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
-    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32").cpu().numpy()
     ref = golden("dose_cfg1_slices.npz")
     assert rel(d[ref["k"]], ref["slices"]) <= DOSE_TOL * ref["dmax"] / np.max(np.abs(ref["slices"]))
     full = er.separable_torch(*axes(prob), wl["weights"], lut["idd"], lut["sigma"]).numpy()
@@ -133,7 +134,7 @@ def test_forward_ragged_and_chunked(pb, shape):
     idd[rng.random((nl, nz)) < 0.3] = 0.0     # inactive (layer, slice) pairs
     sig = rng.uniform(0.2, 0.8, (nl, nz))
     prob = M.PBProblem(grid, lat, idd, sig)
-    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32").cpu().numpy()
     ref = er.separable_f64(grid.x, grid.y, lat.spot_x, lat.spot_y, w, idd, sig)
     if np.max(np.abs(ref)) == 0:
         assert np.all(d == 0)
@@ -146,7 +147,7 @@ def test_forward_all_layers_inactive(pb):
     grid = M.DoseGrid(20, 20, 10, 0.2, 0.2, 0.2, -1.9, -1.9, 0.0)
     lat = M.SpotLattice(5, 5, 2, 0.5, 0.5, weights=np.ones((2, 5, 5)))
     prob = M.PBProblem(grid, lat, np.zeros((2, 10)), np.full((2, 10), 0.4))
-    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32").cpu().numpy()
     assert np.all(d == 0.0)
 
 
@@ -154,7 +155,7 @@ def test_device_tables_end_to_end_cfg0(pb):
     """Device LUT builder + kernel against the reference's own float64 dose."""
     wl = pb.workloads.build_workload(0)
     prob = pb.model.problem_from_workload(wl)
-    d = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    d = pb.engines.torch_separable(prob, "cuda", precision="fp32").cpu().numpy()
     assert rel(d, golden("dose_cfg0.npz")["dose"]) < DOSE_TOL
 
 
@@ -162,9 +163,9 @@ def test_layer_chunk_and_schedule_invariance(pb):
     wl = pb.workloads.build_workload(0)
     lut = golden("luts_cfg0.npz")
     prob = pb.model.problem_from_workload(wl, lut["energies"], lut["idd"], lut["sigma"])
-    base = pb.engines.torch_separable(prob, "cuda").cpu().numpy()
+    base = pb.engines.torch_separable(prob, "cuda", precision="fp32").cpu().numpy()
     for c in (1, 3, 8):
-        d = pb.engines.torch_separable(prob, "cuda", layer_chunk=c).cpu().numpy()
+        d = pb.engines.torch_separable(prob, "cuda", precision="fp32", layer_chunk=c).cpu().numpy()
         assert rel(d, base) < 1e-6
 
 
@@ -177,8 +178,10 @@ def test_api_errors(pb, torch):
     with pytest.raises(NotImplementedError):
         pb.engines.torch_separable(prob, "cuda", per_layer=False)
     with pytest.raises(NotImplementedError):
-        pb.engines.torch_separable(prob, "cuda", dtype=torch.float64)
-    d, t = pb.engines.torch_separable(prob, "cuda", return_timing=True)
+        pb.engines.torch_separable(prob, "cuda", dtype=torch.float16)
+    d64 = pb.engines.torch_separable(prob, "cuda", dtype=torch.float64)
+    assert d64.dtype == torch.float64
+    d, t = pb.engines.torch_separable(prob, "cuda", precision="fp32", return_timing=True)
     assert t > 0 and d.is_cuda
 
 
@@ -197,7 +200,7 @@ def test_loss_grad_cfg0_vs_autograd(pb, torch):
     wl = pb.workloads.build_workload(0)
     en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
     prob = pb.model.problem_from_workload(wl, energies=en)
-    plan = pb.engines.DosePlan(prob, tables="device")
+    plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
     mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
     presc = presc * 100.0
     out = plan.loss_grad(torch.as_tensor(mask, device="cuda"), torch.as_tensor(presc, device="cuda"))
@@ -216,7 +219,7 @@ def test_range_gradient_vs_fd_cfg0(pb, torch):
     wl = pb.workloads.build_workload(0)
     en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
     prob = pb.model.problem_from_workload(wl, energies=en)
-    plan = pb.engines.DosePlan(prob, tables="device")
+    plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
     mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
     presc = presc * 100.0
     out = plan.loss_grad(torch.as_tensor(mask, device="cuda"), torch.as_tensor(presc, device="cuda"))
@@ -239,7 +242,7 @@ def test_autograd_function(pb, torch):
     wl = pb.workloads.build_workload(0)
     en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
     prob = pb.model.problem_from_workload(wl, energies=en)
-    plan = pb.engines.DosePlan(prob, tables="device")
+    plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
     w = torch.tensor(wl["weights"], device="cuda", requires_grad=True)
     dr = torch.zeros(len(en), dtype=torch.float64, device="cuda", requires_grad=True)
     d = pb.engines.separable_dose(w, dr, plan)
@@ -261,7 +264,7 @@ def test_clinical_fd_checks_cfg2(pb, torch):
     lut = golden("luts_cfg1.npz")
     en = lut["energies"]
     prob = pb.model.problem_from_workload(wl, energies=en)
-    plan = pb.engines.DosePlan(prob, tables="device")
+    plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
     m = torch.as_tensor(wl["mask"], device="cuda")
     p = torch.as_tensor(wl["presc"], device="cuda")
     out = plan.loss_grad(m, p)
@@ -349,7 +352,7 @@ def test_plans_refuse_mis_sized_tensors(pb, torch):
     wl = pb.workloads.build_workload(0)
     en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
     prob = pb.model.problem_from_workload(wl, energies=en)
-    plan = pb.engines.DosePlan(prob, tables="device")
+    plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
     g = prob.grid
     shape = (g.nz, g.ny, g.nx)
     ok = plan.forward()
