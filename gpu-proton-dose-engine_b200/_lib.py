@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libpbdose_b200.so")
 
 PBD_OK = 0
 PBD_ERR_TIMEOUT = -8
-PREC = {"fp32": 0, "tf32x3": 1, "tf32": 2, "bf16x3": 3, "bf16": 4}
+PREC = {"fp32": 0, "tf32x3": 1, "tf32": 2, "bf16x3": 3, "bf16": 4, "fp16x3": 5}
 MAX_JOBS = 128
 
 

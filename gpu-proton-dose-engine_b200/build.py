@@ -29,6 +29,7 @@ SOURCES = {
     "fwd_f64.cu": [],
     "adj_simt.cu": [],
     "tc_fwd.cu": [],
+    "tc_fwd16.cu": [],
     "noalloc.cu": [],
     "adj_tc.cu": [],
     "optim.cu": [],

@@ -166,7 +166,7 @@ int choose_adj_chunk(const pbd_field* f) {
 bool finite_pos(double v) { return isfinite(v) && v > 0.0; }
 
 int check_precision(int p) {
-    if (p >= PBD_PREC_FP32 && p <= PBD_PREC_BF16) return PBD_OK;
+    if (p >= PBD_PREC_FP32 && p <= PBD_PREC_FP16X3) return PBD_OK;
     return PBD_ERR_BAD_VALUE;
 }
 
@@ -198,6 +198,8 @@ struct Ws {
     void* aitems;        // AdjItem (FP32 path) or FwdItem (tensor-core path), 32 B each
     int adj_tc;          // 1: tensor-core adjoint, (layer, slice) dL/dW slots
     int* anch;
+    void* pack;          // split-FP16 forward: packed spot maps
+    size_t pack_bytes;
     int* acnt;           // tensor-core adjoint: unit counter, error word, per-layer counters
     float* apart;
     float* dc;
@@ -222,12 +224,18 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
     w.aitems = nullptr; w.anch = nullptr; w.apart = nullptr; w.dc = nullptr; w.dsg = nullptr;
     w.acnt = nullptr;
     w.f_items = w.a_items = 0;
+    w.pack = nullptr;
+    w.pack_bytes = 0;
     if (fwd) {
         size_t pe = 0;
         PBD_TRY(fwd_plan_sizes(f, w.f_chunk, &pe, &w.f_items));
         w.fitems = c.take<FwdItem>(w.f_items);
         w.fnch = c.take<int>(f->nz);
         w.fpart = c.take<float>(pe);
+        if (precision == PBD_PREC_FP16X3) {
+            w.pack_bytes = tc16_pack_bytes(1, f->n_layers, f->n_sx, f->n_sy);
+            w.pack = c.take<char>(w.pack_bytes);
+        }
     }
     if (loss) w.loss_part = c.take<double>(w.n_loss_part);
     w.adj_tc = 0;
@@ -561,7 +569,8 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
-                          ws.status + kStatFwd, ws.f_chunk, 0, precision, 1, s);
+                          ws.status + kStatFwd, ws.f_chunk, 0, precision, 1, ws.pack,
+                          ws.pack_bytes, s);
 }
 
 // err: the adjoint's error word (the workspace's own status word unless a caller passes its
@@ -688,7 +697,8 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     PBD_LAUNCH_CHECK();
     count_launch(1);
     PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
-                           ws.status + kStatFwd, ws.f_chunk, 1, precision, 0, s));
+                           ws.status + kStatFwd, ws.f_chunk, 1, precision, 0, ws.pack,
+                           ws.pack_bytes, s));
     return run_adjoint(ws, precision, &A, with_range, 1, ws.adj_tc, ws.status + kStatAdj, s);
 }
 
@@ -699,7 +709,7 @@ constexpr int kBatchAdjChunk = 8;
 
 struct GradPlan {
     int chunk, direct, with_range, max_l;
-    size_t arr, fpart, lpart, apart, dcs;
+    size_t arr, fpart, lpart, apart, dcs, pack;
 };
 
 static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, GradPlan* gp) {
@@ -708,7 +718,7 @@ static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, 
     if (n_jobs > PBD_MAX_JOBS) return PBD_ERR_TOO_MANY;
     PBD_TRY(check_precision(precision));
     if (precision == PBD_PREC_FP32) return PBD_ERR_UNSUPPORTED;
-    int max_l = 0, chunk = kMaxChunkCost;
+    int max_l = 0, chunk = kMaxChunkCost, max_sx = 1, max_sy = 1;
     gp->with_range = jobs[0].grad_range != nullptr;
     for (int k = 0; k < n_jobs; ++k) {
         const pbd_field* f = &jobs[k].field;
@@ -719,10 +729,13 @@ static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, 
         PBD_TRY(tc_adjoint_dims(precision, f, &n1));
         if ((jobs[k].grad_range != nullptr) != (gp->with_range != 0)) return PBD_ERR_BAD_VALUE;
         max_l = max_l > f->n_layers ? max_l : f->n_layers;
+        max_sx = max_sx > f->n_sx ? max_sx : f->n_sx;
+        max_sy = max_sy > f->n_sy ? max_sy : f->n_sy;
         const int ch = choose_fwd_chunk(f, precision);
         chunk = ch < chunk ? ch : chunk;
     }
     gp->max_l = max_l;
+    gp->pack = precision == PBD_PREC_FP16X3 ? tc16_pack_bytes(n_jobs, max_l, max_sx, max_sy) : 0;
     gp->direct = (max_l <= kMaxChunkCost && g_fwd_chunk == 0) ? 1 : 0;
     gp->chunk = gp->direct ? max_l : chunk;
     gp->arr = gp->fpart = gp->lpart = gp->apart = gp->dcs = 0;
@@ -743,6 +756,7 @@ static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, 
 
 struct GradCarve {
     int* status;
+    void* pack;
     JobDev *fwd, *adj;
     int *fcnt, *acnt;
     float* fpart;
@@ -762,6 +776,7 @@ static size_t carve_grad(void* base, int n_jobs, const GradPlan& gp, GradCarve& 
     g.apart = c.take<float>(gp.apart);
     g.dcs = c.take<float>(gp.dcs);
     g.dsgs = c.take<float>(gp.dcs);
+    g.pack = c.take<char>(gp.pack);
     return c.used + 256;
 }
 
@@ -771,7 +786,7 @@ static size_t carve_grad(void* base, int n_jobs, const GradPlan& gp, GradCarve& 
 // grid balanced).  Otherwise items hold `chunk` layers and partial slices are summed.
 struct BatchPlan {
     int chunk, direct, items;
-    size_t nch, part, arr;
+    size_t nch, part, arr, pack;
 };
 
 static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan* bp) {
@@ -779,11 +794,13 @@ static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan*
     if (n_jobs <= 0) return PBD_ERR_BAD_DIM;
     if (n_jobs > PBD_MAX_JOBS) return PBD_ERR_TOO_MANY;
     PBD_TRY(check_precision(precision));
-    int max_l = 0, chunk = kMaxChunkCost;
+    int max_l = 0, chunk = kMaxChunkCost, max_sx = 1, max_sy = 1;
     for (int k = 0; k < n_jobs; ++k) {
         PBD_TRY(host_validate_field(&jobs[k].field));
         PBD_TRY(check_field_precision(&jobs[k].field, precision));
         max_l = max_l > jobs[k].field.n_layers ? max_l : jobs[k].field.n_layers;
+        max_sx = max_sx > jobs[k].field.n_sx ? max_sx : jobs[k].field.n_sx;
+        max_sy = max_sy > jobs[k].field.n_sy ? max_sy : jobs[k].field.n_sy;
         const int ch = choose_fwd_chunk(&jobs[k].field, precision);
         chunk = ch < chunk ? ch : chunk;
     }
@@ -806,6 +823,7 @@ static int plan_batch(const pbd_job* jobs, int n_jobs, int precision, BatchPlan*
     }
     if (items > (size_t)1 << 30) return PBD_ERR_UNSUPPORTED;
     bp->items = (int)items;
+    bp->pack = precision == PBD_PREC_FP16X3 ? tc16_pack_bytes(n_jobs, max_l, max_sx, max_sy) : 0;
     return PBD_OK;
 }
 
@@ -820,6 +838,7 @@ int pbd_forward_batch_workspace(const pbd_job* jobs, int n_jobs, int precision, 
     c.take<FwdItem>(bp.items);
     c.take<int>(bp.nch);
     c.take<float>(bp.part);
+    c.take<char>(bp.pack);
     *bytes = c.used + 256;
     return PBD_OK;
 }
@@ -870,13 +889,14 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
     FwdItem* items = c.take<FwdItem>(item_base);
     int* nchb = c.take<int>(nch_off);
     float* partb = c.take<float>(part_off);
+    void* packb = c.take<char>(bp.pack);
     cudaStream_t s = (cudaStream_t)stream;
     install_table_kernel<<<(n_jobs + 31) / 32, 32, 0, s>>>(t, jd, partb, nchb, counter + 2,
                                                              status);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return launch_forward(jd, host_view, n_jobs, items, item_base, counter, 2 + arr_off,
-                          status + kStatFwd, bp.chunk, 0, precision, 1, s);
+                          status + kStatFwd, bp.chunk, 0, precision, 1, packb, bp.pack, s);
 }
 
 // ---- heterogeneous media ------------------------------------------------------------
@@ -933,7 +953,7 @@ static int forward_layer_maps(const pbd_field* f, const float* w, const double* 
     count_launch(1);
     // no poison pass here: the combine's poison pass reads this error word too
     return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount, err,
-                          ws.f_chunk, 0, precision, 0, s);
+                          ws.f_chunk, 0, precision, 0, nullptr, 0, s);
 }
 
 // Activity table, the per-layer lateral maps, then the combine.
@@ -1144,7 +1164,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
         count_launch(1);
     }
     PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr,
-                           g.status + kStatFwd, gp.chunk, 1, precision, 0, s));
+                           g.status + kStatFwd, gp.chunk, 1, precision, 0, g.pack, gp.pack, s));
     return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, g.status + kStatAdj, a_chunk,
                              gp.with_range, 1, 1, s);
 }

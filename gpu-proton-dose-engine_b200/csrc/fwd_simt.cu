@@ -290,9 +290,13 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
                    int total_items, int* counter, size_t n_counter_ints, int* err, int chunk,
-                   int with_loss, int precision, int poison, cudaStream_t s) {
+                   int with_loss, int precision, int poison, void* pack, size_t pack_bytes,
+                   cudaStream_t s) {
     if (precision != PBD_PREC_FP32) {
         PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, n_counter_ints * sizeof(int), s)));
+        if (precision == PBD_PREC_FP16X3 && jobs_host[0].layer_stride == 0)
+            return launch_forward_tc16(jobs_dev, jobs_host, n_jobs, counter, err, chunk,
+                                       with_loss, poison, pack, pack_bytes, s);
         return launch_forward_tc(precision, jobs_dev, jobs_host, n_jobs, counter, err, chunk,
                                  with_loss, poison, s);
     }

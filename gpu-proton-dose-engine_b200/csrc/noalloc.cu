@@ -72,7 +72,8 @@ extern "C" int pbd_forward_noalloc(const pbd_field* f, const float* w, const dou
                                    const double* sigma, float* dose, int precision,
                                    void* stream) {
     PBD_TRY(host_validate_field(f));
-    if (precision < PBD_PREC_FP32 || precision > PBD_PREC_BF16) return PBD_ERR_BAD_VALUE;
+    if (precision < PBD_PREC_FP32 || precision > PBD_PREC_FP16X3) return PBD_ERR_BAD_VALUE;
+    if (precision == PBD_PREC_FP16X3) return PBD_ERR_UNSUPPORTED;   // its spot maps need scratch
     if (precision != PBD_PREC_FP32) {
         int k1 = 0, n1 = 0;
         PBD_TRY(tc_operand_dims(precision, f->n_sx, f->n_sy, &k1, &n1));
@@ -113,5 +114,5 @@ extern "C" int pbd_forward_noalloc(const pbd_field* f, const float* w, const dou
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return launch_forward(jd, &J, 1, it, items, counters, 2, counters + 1, chunk, 0, precision, 1,
-                          s);
+                          nullptr, 0, s);
 }

@@ -167,7 +167,8 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 // contiguously by the caller).
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
                    int total_items, int* counter, size_t n_counter_ints, int* err, int chunk,
-                   int with_loss, int precision, int poison, cudaStream_t s);
+                   int with_loss, int precision, int poison, void* pack, size_t pack_bytes,
+                   cudaStream_t s);
 
 // (slice, tile, layer-chunk) work items sorted longest-first, one CTA per job.
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
@@ -203,6 +204,13 @@ int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
 // over all layers, writing the dose directly (no scratch).
 int launch_forward_f64(const pbd_field* f, const double* w, const double* idd,
                        const double* sigma, double* dose, cudaStream_t s);
+
+// forward (tcgen05, split FP16) -- tc_fwd16.cu.  Same units, counters and outputs as
+// launch_forward_tc; `pack` (tc16_pack_bytes) receives the packed spot maps of every job.
+size_t tc16_pack_bytes(int n_jobs, int max_layers, int nsx, int nsy);
+int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, int* counter,
+                        int* err, int chunk, int with_loss, int poison, void* pack,
+                        size_t pack_bytes, cudaStream_t s);
 
 // adjoint (FP32 SIMT) -- adj_simt.cu
 int adj_chunk_depths(const pbd_field* f);

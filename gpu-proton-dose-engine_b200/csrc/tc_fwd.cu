@@ -932,7 +932,8 @@ int launch_mode(const Params& P0, cudaStream_t s) {
 }  // namespace
 
 int tc_operand_dims(int precision, int nsx, int nsy, int* K1, int* N1) {
-    const int kstep = (precision == PBD_PREC_BF16X3 || precision == PBD_PREC_BF16) ? 16 : 8;
+    const int kstep = (precision == PBD_PREC_BF16X3 || precision == PBD_PREC_BF16 ||
+                       precision == PBD_PREC_FP16X3) ? 16 : 8;
     *K1 = (nsx + kstep - 1) / kstep * kstep;
     *N1 = (nsy + 15) / 16 * 16;
     if (*K1 > 64 || *N1 > 64) return PBD_ERR_UNSUPPORTED;
@@ -978,6 +979,8 @@ int launch_forward_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     for (int j = 1; j < n_jobs; ++j)
         if ((jobs_host[j].layer_stride != 0) != maps) return PBD_ERR_UNSUPPORTED;
     if (maps && with_loss) return PBD_ERR_UNSUPPORTED;
+    // the split-FP16 kernel has no per-layer-maps mode: its accuracy class is TF32x3's
+    if (precision == PBD_PREC_FP16X3) precision = PBD_PREC_TF32X3;
     int rc = PBD_ERR_BAD_VALUE;
     switch (precision) {
         case PBD_PREC_TF32X3:

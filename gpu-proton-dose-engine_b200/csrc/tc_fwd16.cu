@@ -1,0 +1,960 @@
+// tc_fwd16.cu -- forward dose on the 5th-generation tensor cores in split FP16 (hi + lo halves,
+// three products, FP32 accumulation): PBD_PREC_FP16X3.
+//
+// For every active (layer l, slice z) and 128 x 128 lateral tile ("step"):
+//
+//   stage 1   U[x, n]  = sum_i Gx[x, i] [Wh; Wl][n, i]     M = 128 (x), N = 2 N1, K = K1
+//             U[x, N1 + j] += sum_i Gxl[x, i] Wh[j, i]      M = 128, N = N1 (cross products)
+//   stage 2   Db[y, x]  = sum_j Gyh[y, j] sUh[x, j]         M = N = 128, K = N1 (hi * hi, per step)
+//             Dc[y, x] += sum_j Gyh sUl + Gyl sUh           (cross products, per unit)
+//
+// with unnormalised Gaussians exp(-d^2 / (2 s^2)) generated on the chip, s U = IDD / (2 pi s^2)
+// (U big + U cross), and every operand split a = hi + lo, hi = fp16(a), lo = fp16(a - hi)
+// (11 + 11 significant bits; the dropped lo * lo term is ~2^-22 of a product).  FP16 has a 5-bit
+// exponent, so every operand is scaled by a power of two into [2^-14, 2^15]: the Gaussians by
+// 2^14 (folded into the exponent), each layer's W by 2^e_l (its largest |W| lands in
+// [2^14, 2^15)), and s U by 2^k with k chosen per unit from a bound on |s U|
+// (max|W_l| (1 + sqrt(2 pi) s / dx_spot) s); the drain divides by the unit's power of two
+// exactly.  Values that still fall below the FP16 normal range are at most 2^-38 of the
+// operand's scale.  kind::f16 takes K = 16 per MMA (twice TF32's 8) at twice the TF32 rate.
+//
+// CTA = 8 math warps, 1 scheduler / producer warp, 3 MMA warps; one CTA per SM (persistent).
+//  * Scheduler warp: units (slice z, chunk c of <= C active layers, tile) from an atomic
+//    counter in z-major order; per unit the scale exponent; one step per active layer into an
+//    8-deep ring.  As producer it also brings each step's spot map into a shared-memory ring
+//    with one bulk copy (cp.async.bulk, mbarrier transaction count): the maps are packed once
+//    per call by pack_w16_kernel into the exact operand image (hi rows then lo rows, K-major
+//    8 x 16-byte core matrices), so the math warps never load W.
+//  * Math warps, software-pipelined by one step: G(n+1) (Gy, Gx of the next step into
+//    double-buffered shared memory, from per-thread squared-distance tables formed in FP64 at
+//    a unit's first step), then E1(n) (U from TMEM, scaled, split into stage 2's B operand),
+//    then DR(n-1) (the hi * hi product of the step before from TMEM into FP32 registers, and
+//    at a unit's end its cross products and the output).
+//  * MMA warps: stage 1 (waits for the spot map, Gx and a free U), stage 2 hi * hi into one of
+//    two D accumulators, stage 2 cross products into the unit's accumulator; each commits to
+//    the barriers that release its operands and publish its result.
+//
+// Accumulation as in the TF32 forward: the large products of a step go to a fresh accumulator
+// that the math warps add in FP32 registers (the tensor core truncates when it accumulates),
+// the cross products (~2^-11 of them) stay in one accumulator per unit.
+//
+// Output (per math warp: 32 rows x 64 columns of the tile) as in the TF32 forward: a unit that
+// holds every active layer of its slice writes its dose rows; otherwise partial rows, summed in
+// chunk order by the warp that completes the slice; with the loss, dL/dD and an FP64 partial
+// of the loss.  Every wait is bounded (2 s of %globaltimer, or the test limit): a warp whose
+// wait runs out sets the error word and leaves, after the MMAs and bulk copies it issued have
+// completed (bounded), and the callers turn the results into NaN.
+#include <algorithm>
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include "pbd_internal.cuh"
+#include "tc_common.cuh"
+
+namespace pbd {
+namespace {
+using namespace tcc;
+
+constexpr int kMathWarps = kTcFwdWarps;
+constexpr int kMath = 32 * kMathWarps;     // 256 math threads: warpgroups 0 and 1
+constexpr int kSchedWarp = kMathWarps;     // warpgroup 2: scheduler / producer, then 3 MMA warps
+constexpr int kS1Warp = kMathWarps + 1;
+constexpr int kS2Warp = kMathWarps + 2;
+constexpr int kS3Warp = kMathWarps + 3;
+constexpr int kThreads = kMath + 128;
+constexpr int kMathRegs = 208, kCtrlRegs = 80;
+constexpr int kLaunchRegsNeeded = (kMath * kMathRegs + 128 * kCtrlRegs + kThreads - 1) / kThreads;
+constexpr int kRing = 8;                   // step slots
+constexpr uint32_t kCols = 512;
+// TMEM columns: D big [0,128) and [128,256) (alternating steps), D cross [256,384), U [384, +2 N1)
+constexpr uint32_t kColDb = 0, kColDc = 256, kColU = 384;
+constexpr float kGScale = 14.0f;           // log2 of the Gaussians' scale
+constexpr int kGExp = 14;
+
+enum : int { kFirst = 1, kLast = 2, kEnd = 4, kZero = 8, kTab = 16 };
+
+struct Step {
+    int job, z, tile, l;
+    int chunk, nch, flags, kd;   // kd: D = accumulator * 2^-kd
+    float a2, f1;                // exponent scale (log2 e / (2 s^2)); U -> s U factor
+    const uint8_t* wimg;         // packed spot map of (job, layer)
+};
+
+struct Params {
+    const JobDev* jobs;
+    int n_jobs, chunk, cmax, tmax, n_units;
+    int* counter;                // [0] unit counter
+    int* err;                    // error word
+    unsigned long long wait_ns;
+    int hold;
+    int with_loss;
+    int K1, N1;
+    int nR, nA1, nB2;            // spot-map ring slots, Gx buffers, sU buffers (Gy: always 2)
+    uint32_t img;                // bytes of one packed spot map (= ring slot)
+    uint32_t oW, oA1, oA2, oB2, oTab;   // shared-memory offsets
+    int ty4, tx4;                // float4 groups of the per-thread distance table
+    const uint8_t* wpack;        // (n_jobs, lmax) packed spot maps
+    const float* wmax;           // (n_jobs, lmax) max |W_l|
+    const int* wexp;             // (n_jobs, lmax) e_l
+    int lmax;
+};
+
+__device__ __forceinline__ uint32_t h2bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+
+// a = hi + lo for two adjacent K elements (already scaled into FP16's range), packed as
+// {element 0 in the low half, element 1 in the high half}.
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 hf = __half22float2(h);
+    hi = h2bits(h);
+    lo = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
+}
+
+__device__ __forceinline__ void split8(const float* v, uint4& hi, uint4& lo) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) split2(v[2 * q], v[2 * q + 1], h[q], l[q]);
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+        : "memory");
+}
+
+// ------------------------------------------------------------------------------------------
+// Spot maps -> packed FP16 operand images, one block per (layer, job).  Image of layer l:
+// K1 / 8 planes of 2 N1 rows x 16 bytes (8 halves of K); rows j < N1 hold hi(W[j, i] 2^e),
+// rows N1 + j hold lo; zero outside the lattice.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) pack_w16_kernel(const JobDev* __restrict__ jobs, int K1,
+                                                       int N1, int lmax, uint32_t img,
+                                                       uint8_t* wpack, float* wmax, int* wexp) {
+    const JobDev& J = jobs[blockIdx.y];
+    const int l = blockIdx.x;
+    if (l >= J.nl) return;
+    const int nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;
+    const float* w = J.w + (size_t)l * per;
+    __shared__ float red[8];
+    float m = 0.f;
+    bool nonfinite = false;
+    for (int e = threadIdx.x; e < per; e += blockDim.x) {
+        const float a = fabsf(__ldg(w + e));
+        if (!(a <= 3.0e38f)) nonfinite = true;   // NaN or inf: leave the layer unscaled
+        m = fmaxf(m, a);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    nonfinite = __syncthreads_or(nonfinite);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = red[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) m = fmaxf(m, red[k]);
+    int q = 0;
+    (void)frexpf(m, &q);                        // m = f 2^q, f in [0.5, 1)
+    const int e = (m > 0.f && !nonfinite) ? 15 - q : 0;   // m 2^e in [2^14, 2^15)
+    uint8_t* out = wpack + ((size_t)blockIdx.y * lmax + l) * img;
+    const int rows = 2 * N1, items = (K1 / 8) * rows;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int g = it / rows, r = it % rows;
+        const int j = r < N1 ? r : r - N1;
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = 8 * g + k;
+            v[k] = (i < nsx && j < nsy) ? ldexpf(__ldg(w + (size_t)j * nsx + i), e) : 0.f;
+        }
+        uint4 hi, lo;
+        split8(v, hi, lo);
+        *reinterpret_cast<uint4*>(out + (size_t)g * rows * 16 + (size_t)r * 16) = r < N1 ? hi : lo;
+    }
+    if (threadIdx.x == 0) {
+        wmax[(size_t)blockIdx.y * lmax + l] = m;
+        wexp[(size_t)blockIdx.y * lmax + l] = e;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Scheduler / producer warp.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, Step* ring,
+                                               uint64_t* full, uint64_t* empty, uint64_t* wfull,
+                                               uint64_t* wempty) {
+    const int lane = threadIdx.x & 31;
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t sW = tc::smem_u32(smem) + P.oW;
+    int k = 0, n = 0;          // ring pushes; steps with a spot map (bulk copies issued)
+    bool ok = true;
+
+    auto push = [&](int src, const Step& st) -> bool {
+        const int slot = k % kRing, u = k / kRing;
+        bool w = wait_bar(&empty[slot], (uint32_t)((u & 1) ^ 1), P.wait_ns);
+        const bool mapped = !(st.flags & (kZero | kEnd));
+        if (mapped && n >= P.nR) {   // the ring slot of the spot map is free again
+            const int ws = n % P.nR;
+            w = w && wait_bar(&wempty[ws], (uint32_t)(((n / P.nR) - 1) & 1), P.wait_ns);
+        }
+        if (!__all_sync(FULL, w)) return false;
+        if (lane == src) {
+            if (mapped) bulk_copy(sW + (uint32_t)(n % P.nR) * P.img, st.wimg, P.img, &wfull[n % P.nR]);
+            ring[slot] = st;
+            tc::mbar_arrive(&full[slot]);
+        }
+        __syncwarp();
+        ++k;
+        if (__shfl_sync(FULL, mapped ? 1 : 0, src)) ++n;
+        return true;
+    };
+
+    if (!P.hold) {
+        for (;;) {
+            int u = 0;
+            if (lane == 0) u = atomicAdd(P.counter, 1);
+            u = __shfl_sync(FULL, u, 0);
+            if (u >= P.n_units) break;
+            int v = u;
+            const int tile = v % P.tmax; v /= P.tmax;
+            const int job = v % P.n_jobs; v /= P.n_jobs;
+            const int c = v % P.cmax;
+            const int z = v / P.cmax;
+            const JobDev& J = P.jobs[job];
+            const int nz = J.nz, nl = J.nl;
+            if (z >= nz || tile >= J.ntx * J.nty) continue;
+            const double* idd = J.idd;
+            int tot = 0;
+            for (int b = 0; b < nl; b += 32) {
+                const int l = b + lane;
+                const bool a = l < nl && idd[(size_t)l * nz + z] != 0.0;
+                tot += __popc(__ballot_sync(FULL, a));
+            }
+            if (tot == 0) {
+                if (c == 0) {
+                    Step st{};
+                    st.job = job; st.z = z; st.tile = tile;
+                    st.nch = 1; st.flags = kFirst | kLast | kZero;
+                    if (!push(0, st)) { ok = false; break; }
+                }
+                continue;
+            }
+            const int nch = (tot + P.chunk - 1) / P.chunk;
+            if (c >= nch) continue;
+            const int r0 = c * P.chunk, r1 = min(tot, r0 + P.chunk);
+            // pass 1: the unit's scale exponent, the smallest over its layers of
+            // 14 - ceil(log2(bound on |s U|)), so that every s U of the unit fits FP16
+            int ks = 127;
+            {
+                int rank = 0;
+                for (int b = 0; b < nl && rank < r1; b += 32) {
+                    const int l = b + lane;
+                    const double iv = l < nl ? idd[(size_t)l * nz + z] : 0.0;
+                    const unsigned bal = __ballot_sync(FULL, iv != 0.0);
+                    const int my = rank + __popc(bal & ((1u << lane) - 1u));
+                    if (iv != 0.0 && my >= r0 && my < r1) {
+                        const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
+                        const double sv = fabs(iv) * kInv2Pi / (s * s);
+                        const double wm = (double)P.wmax[(size_t)job * P.lmax + l];
+                        const double bnd = sv * wm * (1.0 + 2.5066282746310002 * s / J.dsx);
+                        int q = 0;
+                        if (bnd > 0.0 && bnd < 1e300) {
+                            (void)frexp(bnd, &q);          // bnd < 2^q
+                            ks = min(ks, 14 - q);
+                        }
+                    }
+                    rank += __popc(bal);
+                }
+                ks = __reduce_min_sync(FULL, ks);
+                ks = ks > 100 ? 100 : (ks < -100 ? -100 : ks);
+            }
+            int rank = 0;
+            for (int b = 0; b < nl && rank < r1 && ok; b += 32) {
+                const int l = b + lane;
+                const double iv = l < nl ? idd[(size_t)l * nz + z] : 0.0;
+                const bool a = iv != 0.0;
+                const unsigned bal = __ballot_sync(FULL, a);
+                const int my = rank + __popc(bal & ((1u << lane) - 1u));
+                const bool mine = a && my >= r0 && my < r1;
+                Step st{};
+                if (mine) {
+                    const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
+                    const int ew = P.wexp[(size_t)job * P.lmax + l];
+                    st.job = job; st.z = z; st.tile = tile; st.l = l;
+                    st.chunk = c; st.nch = nch;
+                    st.flags = (my == r0 ? kFirst | kTab : 0) | (my == r1 - 1 ? kLast : 0);
+                    // U = 2^(14 + e_l) U_true; s U enters stage 2 as 2^ks s U_true, so
+                    // D = 2^(14 + ks) D_true
+                    st.kd = kGExp + ks;
+                    st.a2 = (float)(kLog2e / (2.0 * s * s));
+                    st.f1 = (float)ldexp(iv * kInv2Pi / (s * s), ks - ew - kGExp);
+                    st.wimg = P.wpack + ((size_t)job * P.lmax + l) * P.img;
+                }
+                unsigned emit = __ballot_sync(FULL, mine);
+                while (emit) {
+                    const int src = __ffs(emit) - 1;
+                    emit &= emit - 1u;
+                    Step sb;
+                    // every lane passes the emitting lane's step (push reads its flags)
+                    sb.flags = __shfl_sync(FULL, st.flags, src);
+                    if (lane == src) sb = st;
+                    if (!push(src, sb)) { ok = false; break; }
+                }
+                rank += __popc(bal);
+            }
+            if (!ok) break;
+        }
+        if (ok) {
+            Step st{};
+            st.flags = kEnd;
+            (void)push(0, st);
+        }
+    }
+    // the spot-map copies still in flight land before the block exits
+    const int first = n > P.nR ? n - P.nR : 0;
+    for (int m = first; m < n; ++m)
+        (void)wait_bar(&wfull[m % P.nR], (uint32_t)((m / P.nR) & 1), P.wait_ns);
+    if (!ok && lane == 0) atomicExch(P.err, 1);
+}
+
+// ------------------------------------------------------------------------------------------
+// MMA warps.  role 1: stage 1; role 2: stage 2 hi * hi; role 3: stage 2 cross products.
+// bars: [0,4) wfull, [4,8) wempty (ring slots), then
+//   a1r[2], a1f[2], a2r[2], a2f[2], b2r[2], b2f[2], uf (U full), uu (U free),
+//   df[2] (D big full), du[2] (D big free), cf (cross full), cu (cross free)
+// ------------------------------------------------------------------------------------------
+struct Bars {
+    uint64_t *wfull, *wempty, *a1r, *a1f, *a2r, *a2f, *b2r, *b2f, *uf, *uu, *df, *du, *cf, *cu;
+};
+
+__device__ __forceinline__ Bars make_bars(uint64_t* b) {
+    Bars B;
+    B.wfull = b; B.wempty = b + 4;
+    B.a1r = b + 8; B.a1f = b + 10; B.a2r = b + 12; B.a2f = b + 14; B.b2r = b + 16; B.b2f = b + 18;
+    B.uf = b + 20; B.uu = b + 21; B.df = b + 22; B.du = b + 24; B.cf = b + 26; B.cu = b + 27;
+    return B;
+}
+constexpr int kNumBars = 28;
+
+__device__ __forceinline__ void mma_warp(const Params& P, uint32_t sbase, uint32_t tb, int role,
+                                         const Step* ring, uint64_t* full, uint64_t* empty,
+                                         const Bars& B) {
+    const int lane = threadIdx.x & 31;
+    const int K1 = P.K1, N1 = P.N1;
+    const uint32_t plA = 128u * 16u;                 // plane of a 128-row operand
+    const uint32_t plW = 2u * (uint32_t)N1 * 16u;    // plane of the spot map (2 N1 rows)
+    const uint32_t aBytes1 = (uint32_t)K1 * 256u;    // one half (hi or lo) of a Gx buffer
+    const uint32_t aBytes2 = (uint32_t)N1 * 256u;    // one half of a Gy / sU buffer
+    const uint32_t id1w = tc::instr_desc(128, 2 * N1, 0u);
+    const uint32_t id1n = tc::instr_desc(128, N1, 0u);
+    const uint32_t id2 = tc::instr_desc(128, 128, 0u);
+    int k = 0, n = 0, seg = 0;
+    bool ok = true;
+    for (;;) {
+        const int slot = k % kRing;
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
+        const int flags = ring[slot].flags;
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[slot]);
+        ++k;
+        if (!__all_sync(0xffffffffu, ok)) break;
+        if (flags & kEnd) break;
+        if (flags & kZero) continue;
+        if (role == 1) {
+            const int ws = n % P.nR, ia = n % P.nA1;
+            ok = wait_bar(&B.wfull[ws], (uint32_t)((n / P.nR) & 1), P.wait_ns);
+            ok = ok && wait_bar(&B.a1r[ia], (uint32_t)((n / P.nA1) & 1), P.wait_ns);
+            if (n > 0) ok = ok && wait_bar(B.uu, (uint32_t)((n - 1) & 1), P.wait_ns);
+            if (!__all_sync(0xffffffffu, ok)) break;
+            tc::fence_after_sync();
+            if (lane == 0) {
+                const uint32_t a = sbase + P.oA1 + (uint32_t)ia * 2u * aBytes1;
+                const uint32_t w = sbase + P.oW + (uint32_t)ws * P.img;
+                for (int st = 0; st < K1 / 16; ++st) {
+                    const uint32_t oa = (uint32_t)st * 2u * plA, ow = (uint32_t)st * 2u * plW;
+                    tc::mma_bf16(tb + kColU, tc::smem_desc(a + oa, plA, 128),
+                                 tc::smem_desc(w + ow, plW, 128), id1w, st > 0 ? 1u : 0u);
+                    tc::mma_bf16(tb + kColU + (uint32_t)N1, tc::smem_desc(a + aBytes1 + oa, plA, 128),
+                                 tc::smem_desc(w + ow, plW, 128), id1n, 1u);
+                }
+                tc::commit(B.uf);
+                tc::commit(&B.a1f[ia]);
+                tc::commit(&B.wempty[ws]);
+            }
+            __syncwarp();
+        } else {
+            const int ia = n & 1, ib = n % P.nB2, db = n & 1;
+            ok = wait_bar(&B.a2r[ia], (uint32_t)((n >> 1) & 1), P.wait_ns);
+            ok = ok && wait_bar(&B.b2r[ib], (uint32_t)((n / P.nB2) & 1), P.wait_ns);
+            const bool first = (flags & kFirst) != 0;
+            if (role == 2 && n >= 2)
+                ok = ok && wait_bar(&B.du[db], (uint32_t)(((n >> 1) - 1) & 1), P.wait_ns);
+            if (role == 3 && first && seg > 0)
+                ok = ok && wait_bar(B.cu, (uint32_t)((seg - 1) & 1), P.wait_ns);
+            if (!__all_sync(0xffffffffu, ok)) break;
+            tc::fence_after_sync();
+            if (lane == 0) {
+                const uint32_t a = sbase + P.oA2 + (uint32_t)ia * 2u * aBytes2;
+                const uint32_t b = sbase + P.oB2 + (uint32_t)ib * 2u * aBytes2;
+                for (int st = 0; st < N1 / 16; ++st) {
+                    const uint32_t o = (uint32_t)st * 2u * plA;
+                    if (role == 2) {
+                        tc::mma_bf16(tb + kColDb + (uint32_t)db * 128u, tc::smem_desc(a + o, plA, 128),
+                                     tc::smem_desc(b + o, plA, 128), id2, st > 0 ? 1u : 0u);
+                    } else {
+                        tc::mma_bf16(tb + kColDc, tc::smem_desc(a + o, plA, 128),
+                                     tc::smem_desc(b + aBytes2 + o, plA, 128), id2,
+                                     (first && st == 0) ? 0u : 1u);
+                        tc::mma_bf16(tb + kColDc, tc::smem_desc(a + aBytes2 + o, plA, 128),
+                                     tc::smem_desc(b + o, plA, 128), id2, 1u);
+                    }
+                }
+                if (role == 2) tc::commit(&B.df[db]);
+                tc::commit(&B.a2f[ia]);
+                tc::commit(&B.b2f[ib]);
+                if (role == 3 && (flags & kLast)) tc::commit(B.cf);
+            }
+            __syncwarp();
+            if (role == 3 && (flags & kLast)) ++seg;
+        }
+        ++n;
+    }
+    if (!ok && lane == 0) atomicExch(P.err, 1);
+    // this warp's last MMAs are complete before the block frees its TMEM
+    if (n > 0) {
+        const int m = n - 1;
+        if (role == 1) (void)wait_bar(&B.a1f[m % P.nA1], (uint32_t)((m / P.nA1) & 1), P.wait_ns);
+        else (void)wait_bar(&B.b2f[m % P.nB2], (uint32_t)((m / P.nB2) & 1), P.wait_ns);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Math warps.
+// ------------------------------------------------------------------------------------------
+// Dose (and loss) of 64 voxels of row y from column xb (v = null: zeros); returns the FP64
+// sum of m (D - P)^2.
+__device__ __forceinline__ double write_final(const JobDev& J, int z, int y, int xb,
+                                              const float* v, int with_loss) {
+    double lsum = 0.0;
+    if (y >= J.ny) return lsum;
+    const size_t o = ((size_t)z * J.ny + y) * J.nx + xb;
+    float* d = J.dose + o;
+    const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
+#pragma unroll
+    for (int q = 0; q < 64; q += 4) {
+        float x4[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) x4[r] = v ? v[q + r] : 0.f;
+        if (!with_loss) {
+            if (vec) {
+                *reinterpret_cast<float4*>(d + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (xb + q + r < J.nx) d[q + r] = x4[r];
+            }
+            continue;
+        }
+        float m4[4], p4[4];
+        if (vec) {
+            const float4 a = *reinterpret_cast<const float4*>(J.mask + o + q);
+            const float4 b = *reinterpret_cast<const float4*>(J.presc + o + q);
+            m4[0] = a.x; m4[1] = a.y; m4[2] = a.z; m4[3] = a.w;
+            p4[0] = b.x; p4[1] = b.y; p4[2] = b.z; p4[3] = b.w;
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const bool in = xb + q + r < J.nx;
+                m4[r] = in ? J.mask[o + q + r] : 0.f;
+                p4[r] = in ? J.presc[o + q + r] : 0.f;
+            }
+        }
+        float r4[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            r4[r] = x4[r] - p4[r];
+            lsum += (double)m4[r] * (double)r4[r] * (double)r4[r];
+        }
+        float* g = J.grad_dose + o;
+        if (vec) {
+            *reinterpret_cast<float4*>(d + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
+            *reinterpret_cast<float4*>(g + q) = make_float4(2.f * m4[0] * r4[0], 2.f * m4[1] * r4[1],
+                                                            2.f * m4[2] * r4[2], 2.f * m4[3] * r4[3]);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (xb + q + r < J.nx) {
+                    d[q + r] = x4[r];
+                    g[q + r] = 2.f * m4[r] * r4[r];
+                }
+        }
+    }
+    return lsum;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint32_t tb,
+                                           const Step* ring, uint64_t* full, uint64_t* empty,
+                                           const Bars& B) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int K1 = P.K1, N1 = P.N1;
+    const int sp = warp & 3, half = warp >> 2;
+    const uint32_t lane_base = (uint32_t)(32 * sp) << 16;
+    const int trow = 32 * sp + lane;                 // TMEM lane = tile row of this thread
+    const int grow = tid & 127, ghalf = tid >> 7;    // operand row and chunk parity generated
+    const uint32_t aBytes1 = (uint32_t)K1 * 256u, aBytes2 = (uint32_t)N1 * 256u;
+    float4* tab = reinterpret_cast<float4*>(smem + P.oTab);
+    constexpr int kMaxR = 64 / 16;                   // chunk pairs per thread (K <= 64)
+
+    float dsum[64];
+#pragma unroll
+    for (int q = 0; q < 64; ++q) dsum[q] = 0.f;
+    bool ok = true;
+    int k = 0;         // ring reads
+    int ng = 0;        // steps generated (G done)
+    int useg = 0;      // units whose cross accumulator was drained
+    Step s1{}, s2{};   // step ng - 1 (awaiting E1) and ng - 2 (awaiting DR)
+
+    // Output of this warp's rows of a finished unit (dsum = its dose), then dsum = 0; or, for a
+    // slice no layer reaches, zeros (dsum, which may hold a unit in progress, untouched).
+    auto output = [&](const Step& st, bool zero) {
+        const JobDev& J = P.jobs[st.job];
+        const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
+        const int y = ty * kTile + trow, xb = tx * kTile + half * 64;
+        const int slot = (st.z * (J.ntx * J.nty) + st.tile) * kMathWarps + warp;
+        if (zero || st.nch == 1) {
+            const double ls = warp_sum(write_final(J, st.z, y, xb, zero ? nullptr : dsum, P.with_loss));
+            if (P.with_loss && lane == 0) J.loss_part[slot] = ls;
+        } else {
+            const size_t n3 = (size_t)J.nz * J.ny * J.nx;
+            const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
+            if (y < J.ny) {
+                float* o = J.partial + (size_t)st.chunk * n3 + ((size_t)st.z * J.ny + y) * J.nx + xb;
+#pragma unroll
+                for (int q = 0; q < 64; q += 4) {
+                    if (vec) {
+                        *reinterpret_cast<float4*>(o + q) =
+                            make_float4(dsum[q], dsum[q + 1], dsum[q + 2], dsum[q + 3]);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (xb + q + r < J.nx) o[q + r] = dsum[q + r];
+                    }
+                }
+            }
+            __threadfence();
+            __syncwarp();
+            int last = 0;
+            if (lane == 0) last = atomicAdd(&J.arrive[slot], 1) == st.nch - 1;
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+#pragma unroll
+                for (int q = 0; q < 64; ++q) dsum[q] = 0.f;
+                if (y < J.ny) {
+                    const float* base = J.partial + ((size_t)st.z * J.ny + y) * J.nx + xb;
+                    for (int c = 0; c < st.nch; ++c) {
+                        const float* pc = base + (size_t)c * n3;
+#pragma unroll
+                        for (int q = 0; q < 64; q += 4) {
+                            if (vec) {
+                                const float4 a = __ldcg(reinterpret_cast<const float4*>(pc + q));
+                                dsum[q] += a.x; dsum[q + 1] += a.y; dsum[q + 2] += a.z; dsum[q + 3] += a.w;
+                            } else {
+#pragma unroll
+                                for (int r = 0; r < 4; ++r)
+                                    if (xb + q + r < J.nx) dsum[q + r] += __ldcg(pc + q + r);
+                            }
+                        }
+                    }
+                }
+                const double ls = warp_sum(write_final(J, st.z, y, xb, dsum, P.with_loss));
+                if (P.with_loss && lane == 0) J.loss_part[slot] = ls;
+            }
+        }
+        if (!zero) {
+#pragma unroll
+            for (int q = 0; q < 64; ++q) dsum[q] = 0.f;
+        }
+    };
+
+    // G: the Gaussian operands of step m (= ng) into buffers A1[m % nA1], A2[m & 1].
+    auto gen = [&](const Step& st, int m) -> bool {
+        const int ia = m % P.nA1, ia2 = m & 1;
+        bool w = true;
+        if (m >= P.nA1) w = wait_bar(&B.a1f[ia], (uint32_t)(((m / P.nA1) - 1) & 1), P.wait_ns);
+        if (m >= 2) w = w && wait_bar(&B.a2f[ia2], (uint32_t)(((m >> 1) - 1) & 1), P.wait_ns);
+        if (!__all_sync(0xffffffffu, w)) return false;
+        const JobDev& J = P.jobs[st.job];
+        if (st.flags & kTab) {
+            // this thread's squared distances (FP64 differences), +inf outside the lattice
+            const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
+            const double cx = 0.5 * (double)(J.nsx - 1), cy = 0.5 * (double)(J.nsy - 1);
+            const double yv = J.oy + (double)(ty * kTile + grow) * J.dy;
+            const double xv = J.ox + (double)(tx * kTile + grow) * J.dx;
+#pragma unroll
+            for (int r = 0; r < kMaxR; ++r) {
+                const int g = ghalf + 2 * r;
+                if (r < N1 / 16) {
+                    float d2[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int j = 8 * g + q;
+                        const float d = (float)(yv - (J.sy0 + ((double)j - cy) * J.dsy));
+                        d2[q] = j < J.nsy ? d * d : INFINITY;
+                    }
+                    tab[(2 * r) * kMath + tid] = make_float4(d2[0], d2[1], d2[2], d2[3]);
+                    tab[(2 * r + 1) * kMath + tid] = make_float4(d2[4], d2[5], d2[6], d2[7]);
+                }
+                if (r < K1 / 16) {
+                    float d2[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int i = 8 * g + q;
+                        const float d = (float)(xv - (J.sx0 + ((double)i - cx) * J.dsx));
+                        d2[q] = i < J.nsx ? d * d : INFINITY;
+                    }
+                    tab[(P.ty4 + 2 * r) * kMath + tid] = make_float4(d2[0], d2[1], d2[2], d2[3]);
+                    tab[(P.ty4 + 2 * r + 1) * kMath + tid] = make_float4(d2[4], d2[5], d2[6], d2[7]);
+                }
+            }
+        }
+        const float a2 = st.a2;
+        uint8_t* a2h = smem + P.oA2 + (uint32_t)ia2 * 2u * aBytes2;
+        uint8_t* a1h = smem + P.oA1 + (uint32_t)ia * 2u * aBytes1;
+#pragma unroll
+        for (int r = 0; r < kMaxR; ++r) {
+            const int g = ghalf + 2 * r;
+            if (r < N1 / 16) {
+                const float4 p = tab[(2 * r) * kMath + tid], q4 = tab[(2 * r + 1) * kMath + tid];
+                float v[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+                for (int e = 0; e < 8; ++e) v[e] = ex2_approx(fmaf(-v[e], a2, kGScale));
+                uint4 hi, lo;
+                split8(v, hi, lo);
+                const uint32_t off = (uint32_t)g * 2048u + (uint32_t)grow * 16u;
+                *reinterpret_cast<uint4*>(a2h + off) = hi;
+                *reinterpret_cast<uint4*>(a2h + aBytes2 + off) = lo;
+            }
+            if (r < K1 / 16) {
+                const float4 p = tab[(P.ty4 + 2 * r) * kMath + tid];
+                const float4 q4 = tab[(P.ty4 + 2 * r + 1) * kMath + tid];
+                float v[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
+#pragma unroll
+                for (int e = 0; e < 8; ++e) v[e] = ex2_approx(fmaf(-v[e], a2, kGScale));
+                uint4 hi, lo;
+                split8(v, hi, lo);
+                const uint32_t off = (uint32_t)g * 2048u + (uint32_t)grow * 16u;
+                *reinterpret_cast<uint4*>(a1h + off) = hi;
+                *reinterpret_cast<uint4*>(a1h + aBytes1 + off) = lo;
+            }
+        }
+        tc::fence_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+            tc::mbar_arrive(&B.a1r[ia]);
+            tc::mbar_arrive(&B.a2r[ia2]);
+        }
+        return true;
+    };
+
+    // E1: U of step m from TMEM, times f1, split -> B2[m % nB2] (x rows, K = j).
+    auto e1 = [&](const Step& st, int m) -> bool {
+        bool w = wait_bar(B.uf, (uint32_t)(m & 1), P.wait_ns);
+        if (!__all_sync(0xffffffffu, w)) return false;
+        tc::fence_after_sync();
+        const int ncol = N1 / 2, c0 = half * ncol;   // this warp's columns j: multiple of 8
+        uint32_t rb[4][8], rc[4][8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q * 8 < ncol) {
+                tc::tmem_ld8(tb + kColU + lane_base + (uint32_t)(c0 + 8 * q), rb[q]);
+                tc::tmem_ld8(tb + kColU + lane_base + (uint32_t)(N1 + c0 + 8 * q), rc[q]);
+            }
+        }
+        tc::tmem_wait_ld();
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(B.uu);
+        const int ib = m % P.nB2;
+        if (m >= P.nB2) w = wait_bar(&B.b2f[ib], (uint32_t)(((m / P.nB2) - 1) & 1), P.wait_ns);
+        if (!__all_sync(0xffffffffu, w)) return false;
+        uint8_t* bh = smem + P.oB2 + (uint32_t)ib * 2u * aBytes2;
+        const float f1 = st.f1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q * 8 < ncol) {
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    v[e] = (__uint_as_float(rb[q][e]) + __uint_as_float(rc[q][e])) * f1;
+                uint4 hi, lo;
+                split8(v, hi, lo);
+                const uint32_t off = (uint32_t)((c0 >> 3) + q) * 2048u + (uint32_t)trow * 16u;
+                *reinterpret_cast<uint4*>(bh + off) = hi;
+                *reinterpret_cast<uint4*>(bh + aBytes2 + off) = lo;
+            }
+        }
+        tc::fence_async_smem();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&B.b2r[ib]);
+        return true;
+    };
+
+    // DR: step m's hi * hi product into dsum; at its unit's end the cross products and output.
+    auto dr = [&](const Step& st, int m) -> bool {
+        const int db = m & 1;
+        bool w = wait_bar(&B.df[db], (uint32_t)((m >> 1) & 1), P.wait_ns);
+        if (!__all_sync(0xffffffffu, w)) return false;
+        tc::fence_after_sync();
+        const float sc = __int_as_float((127 - st.kd) << 23);   // 2^-kd, exact (|kd| <= 114)
+        uint32_t r[4][16];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            tc::tmem_ld16(tb + kColDb + (uint32_t)db * 128u + lane_base + (uint32_t)(half * 64 + c * 16), r[c]);
+        tc::tmem_wait_ld();
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&B.du[db]);
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int q = 0; q < 16; ++q) dsum[c * 16 + q] = fmaf(__uint_as_float(r[c][q]), sc, dsum[c * 16 + q]);
+        if (st.flags & kLast) {
+            w = wait_bar(B.cf, (uint32_t)(useg & 1), P.wait_ns);
+            if (!__all_sync(0xffffffffu, w)) return false;
+            tc::fence_after_sync();
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                tc::tmem_ld16(tb + kColDc + lane_base + (uint32_t)(half * 64 + c * 16), r[c]);
+            tc::tmem_wait_ld();
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(B.cu);
+            ++useg;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int q = 0; q < 16; ++q) dsum[c * 16 + q] = fmaf(__uint_as_float(r[c][q]), sc, dsum[c * 16 + q]);
+            output(st, false);
+        }
+        return true;
+    };
+
+    for (;;) {
+        const int slot = k % kRing;
+        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
+        const Step cur = ring[slot];
+        if (cur.flags != kEnd && (cur.job < 0 || cur.job >= P.n_jobs)) ok = false;
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[slot]);
+        ++k;
+        if (!__all_sync(0xffffffffu, ok)) break;
+        if (cur.flags & kEnd) break;
+        if (cur.flags & kZero) {        // a slice no layer reaches: zeros (and the loss)
+            output(cur, true);
+            continue;
+        }
+        // G(ng), E1(ng - 1), DR(ng - 2)
+        ok = gen(cur, ng);
+        if (!ok) break;
+        if (ng >= 1) {
+            ok = e1(s1, ng - 1);
+            if (!ok) break;
+        }
+        if (ng >= 2) {
+            ok = dr(s2, ng - 2);
+            if (!ok) break;
+        }
+        s2 = s1;
+        s1 = cur;
+        ++ng;
+    }
+    if (ok && ng >= 1) {
+        ok = e1(s1, ng - 1);
+        if (ok && ng >= 2) ok = dr(s2, ng - 2);
+        if (ok) ok = dr(s1, ng - 1);
+    }
+    if (!ok && lane == 0) atomicExch(P.err, 1);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) fwd_tc16_kernel(Params P) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[kRing];
+    __shared__ __align__(8) uint64_t empty[kRing];
+    __shared__ __align__(8) uint64_t bars[kNumBars];
+    __shared__ Step ring[kRing];
+    __shared__ uint32_t tmem_base_s;
+
+    const int warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base_s, kCols);
+        tc::tmem_relinquish();
+    }
+    const Bars B = make_bars(bars);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; ++i) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], kMathWarps + 3);   // math warps + the three MMA warps
+        }
+        for (int i = 0; i < 4; ++i) {
+            tc::mbar_init(&B.wfull[i], 1);             // producer's expect_tx arrival + bytes
+            tc::mbar_init(&B.wempty[i], 1);            // stage-1 commit
+        }
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&B.a1r[i], kMathWarps);
+            tc::mbar_init(&B.a1f[i], 1);
+            tc::mbar_init(&B.a2r[i], kMathWarps);
+            tc::mbar_init(&B.a2f[i], 2);               // both stage-2 warps
+            tc::mbar_init(&B.b2r[i], kMathWarps);
+            tc::mbar_init(&B.b2f[i], 2);
+            tc::mbar_init(&B.df[i], 1);
+            tc::mbar_init(&B.du[i], kMathWarps);
+        }
+        tc::mbar_init(B.uf, 1);
+        tc::mbar_init(B.uu, kMathWarps);
+        tc::mbar_init(B.cf, 1);
+        tc::mbar_init(B.cu, kMathWarps);
+        tc::fence_mbar_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    // the spot maps are packed by the kernel before this one (a programmatic dependent launch:
+    // everything above overlaps its end)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+
+    if (warp >= kMathWarps) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
+        if (warp == kSchedWarp)
+            scheduler_warp(P, smem, ring, full, empty, B.wfull, B.wempty);
+        else
+            mma_warp(P, tc::smem_u32(smem), tmem_base_s, warp - kSchedWarp, ring, full, empty, B);
+    } else {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kMathRegs));
+        math_warps(P, smem, tmem_base_s, ring, full, empty, B);
+    }
+
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_dealloc(tmem_base_s, kCols);
+}
+
+__global__ void fwd16_poison_kernel(const JobDev* __restrict__ jobs, int n_jobs, const int* err) {
+    if (*err == 0) return;
+    for (int j = 0; j < n_jobs; ++j) {
+        const JobDev& J = jobs[j];
+        const size_t n = (size_t)J.nx * J.ny * J.nz;
+        for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+             v += (size_t)gridDim.x * blockDim.x)
+            J.dose[v] = __int_as_float(0x7fc00000);
+    }
+}
+
+// Shared-memory plan: buffer counts (largest first that fit) and offsets.
+struct Plan16 {
+    int nR, nA1, nB2;
+    uint32_t img, oW, oA1, oA2, oB2, oTab, total;
+    int ty4, tx4;
+};
+
+bool plan16(int K1, int N1, int max_dyn, Plan16* p) {
+    p->img = 4u * (uint32_t)K1 * (uint32_t)N1;
+    p->ty4 = N1 / 8;
+    p->tx4 = K1 / 8;
+    const uint32_t a1 = 2u * (uint32_t)K1 * 256u, a2 = 2u * (uint32_t)N1 * 256u;
+    const uint32_t tab = (uint32_t)(p->ty4 + p->tx4) * (uint32_t)kMath * 16u;
+    static const int cand[][3] = {{3, 2, 2}, {2, 2, 2}, {2, 2, 1}, {2, 1, 1}};
+    for (const auto& c : cand) {
+        p->nR = c[0]; p->nA1 = c[1]; p->nB2 = c[2];
+        p->oW = 0;
+        p->oA1 = p->oW + (uint32_t)p->nR * p->img;
+        p->oA2 = p->oA1 + (uint32_t)p->nA1 * a1;
+        p->oB2 = p->oA2 + 2u * a2;
+        p->oTab = p->oB2 + (uint32_t)p->nB2 * a2;
+        p->total = p->oTab + tab;
+        if ((int)p->total <= max_dyn) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+size_t tc16_pack_bytes(int n_jobs, int max_layers, int nsx, int nsy) {
+    const size_t K1 = (size_t)(nsx + 15) / 16 * 16, N1 = (size_t)(nsy + 15) / 16 * 16;
+    return (size_t)n_jobs * (size_t)max_layers * (4u * K1 * N1 + 8u);
+}
+
+int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, int* counter,
+                        int* err, int chunk, int with_loss, int poison, void* pack,
+                        size_t pack_bytes, cudaStream_t s) {
+    Params P{};
+    P.jobs = jobs_dev;
+    P.n_jobs = n_jobs;
+    P.chunk = chunk;
+    P.counter = counter;
+    P.err = err;
+    P.wait_ns = wait_limit_ns();
+    P.hold = test_hold();
+    P.with_loss = with_loss;
+    int lmax = 1, nsx = 1, nsy = 1;
+    for (int j = 0; j < n_jobs; ++j) {
+        int k1 = 0, n1 = 0;
+        PBD_TRY(tc_operand_dims(PBD_PREC_BF16X3, jobs_host[j].nsx, jobs_host[j].nsy, &k1, &n1));
+        P.K1 = std::max(P.K1, k1);
+        P.N1 = std::max(P.N1, n1);
+        lmax = std::max(lmax, jobs_host[j].nl);
+        nsx = std::max(nsx, jobs_host[j].nsx);
+        nsy = std::max(nsy, jobs_host[j].nsy);
+    }
+    if (jobs_host[0].layer_stride != 0) return PBD_ERR_UNSUPPORTED;   // per-layer maps: TF32 kernel
+    PBD_TRY(tc_forward_units(jobs_host, n_jobs, chunk, &P.cmax, &P.tmax, &P.n_units));
+    const size_t need = tc16_pack_bytes(n_jobs, lmax, P.K1, P.N1);
+    if (!pack || pack_bytes < need) return PBD_ERR_WORKSPACE;
+    P.lmax = lmax;
+    P.img = 4u * (uint32_t)P.K1 * (uint32_t)P.N1;
+    uint8_t* base = static_cast<uint8_t*>(pack);
+    P.wpack = base;
+    float* wmax = reinterpret_cast<float*>(base + (size_t)n_jobs * lmax * P.img);
+    int* wexp = reinterpret_cast<int*>(wmax + (size_t)n_jobs * lmax);
+    P.wmax = wmax;
+    P.wexp = wexp;
+    int max_dyn = 0;
+    PBD_TRY(smem_optin((const void*)fwd_tc16_kernel, -1, kLaunchRegsNeeded, &max_dyn));
+    Plan16 pl;
+    if (!plan16(P.K1, P.N1, max_dyn, &pl)) return PBD_ERR_NO_SMEM;
+    P.nR = pl.nR; P.nA1 = pl.nA1; P.nB2 = pl.nB2;
+    P.oW = pl.oW; P.oA1 = pl.oA1; P.oA2 = pl.oA2; P.oB2 = pl.oB2; P.oTab = pl.oTab;
+    P.ty4 = pl.ty4; P.tx4 = pl.tx4;
+    // >= 116 KiB: one CTA (and its 512 TMEM columns) per SM
+    const size_t smem = std::max<size_t>(pl.total, 116u * 1024u);
+    if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
+    pack_w16_kernel<<<dim3(lmax, n_jobs), 256, 0, s>>>(jobs_dev, P.K1, P.N1, lmax, P.img,
+                                                       const_cast<uint8_t*>(P.wpack), wmax, wexp);
+    PBD_LAUNCH_CHECK();
+    const int grid = std::max(1, std::min(P.n_units, num_sms()));
+    prof_mark(kProfFwd, 0, s);
+    PBD_TRY(launch_dependent(fwd_tc16_kernel, dim3(grid), dim3(kThreads), smem, s, P));
+    prof_mark(kProfFwd, 1, s);
+    count_launch(2);
+    if (poison) {
+        fwd16_poison_kernel<<<num_sms(), 256, 0, s>>>(jobs_dev, n_jobs, err);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    }
+    return PBD_OK;
+}
+
+}  // namespace pbd

@@ -58,6 +58,8 @@ extern "C" {
 #define PBD_PREC_TF32    2   /* tcgen05 TF32, one product */
 #define PBD_PREC_BF16X3  3   /* tcgen05 BF16, hi/lo split, three products */
 #define PBD_PREC_BF16    4   /* tcgen05 BF16, one product */
+#define PBD_PREC_FP16X3  5   /* tcgen05 FP16, hi/lo split, three products; operands scaled by
+                                powers of two into FP16's range */
 
 #define PBD_MAX_JOBS 128     /* jobs (fields x scenarios) per batched launch */
 

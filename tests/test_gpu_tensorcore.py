@@ -1,7 +1,7 @@
 """Tensor-core (tcgen05) forward against the float64 oracle, every precision mode.
 
 Tolerances (max |dD| / max D against float64):
-  tf32x3 (default):  1e-6   -- the north-star bound for the split forms
+  tf32x3, fp16x3:    1e-6   -- the north-star bound for the split forms
   bf16x3:            5e-5   -- reported; the split with bf16 parts keeps ~16 mantissa bits
   tf32:              5e-3   -- one TF32 product (10-bit mantissa)
   bf16:              5e-2   -- one BF16 product (7-bit mantissa)
@@ -15,7 +15,7 @@ from oracle import physics_ref as pr
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")]
 
-TOL = {"tf32x3": 1e-6, "bf16x3": 5e-5, "tf32": 5e-3, "bf16": 5e-2}
+TOL = {"tf32x3": 1e-6, "fp16x3": 1e-6, "bf16x3": 5e-5, "tf32": 5e-3, "bf16": 5e-2}
 
 
 def rel(a, b):
@@ -29,7 +29,7 @@ def pb():
     return load_pkg()
 
 
-@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "tf32", "bf16"])
+@pytest.mark.parametrize("prec", ["tf32x3", "fp16x3", "bf16x3", "tf32", "bf16"])
 def test_tc_forward_cfg0(pb, prec):
     wl = pb.workloads.build_workload(0)
     lut = golden("luts_cfg0.npz")
@@ -40,7 +40,7 @@ def test_tc_forward_cfg0(pb, prec):
     assert err < TOL[prec]
 
 
-@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "tf32", "bf16"])
+@pytest.mark.parametrize("prec", ["tf32x3", "fp16x3", "bf16x3", "tf32", "bf16"])
 def test_tc_forward_cfg1(pb, prec):
     wl = pb.workloads.build_workload(1)
     lut = golden("luts_cfg1.npz")
@@ -53,9 +53,11 @@ def test_tc_forward_cfg1(pb, prec):
     assert err < TOL[prec]
 
 
+@pytest.mark.parametrize("prec", ["tf32x3", "fp16x3"])
 @pytest.mark.parametrize("shape", [(1, 1, 1, 1, 1, 1), (150, 70, 33, 61, 13, 5),
-                                   (37, 129, 9, 5, 64, 3), (200, 200, 3, 61, 61, 2)])
-def test_tc_forward_ragged(pb, shape):
+                                   (37, 129, 9, 5, 64, 3), (200, 200, 3, 61, 61, 2),
+                                   (128, 96, 12, 51, 41, 70)])
+def test_tc_forward_ragged(pb, shape, prec):
     nx, ny, nz, nsx, nsy, nl = shape
     rng = np.random.default_rng(sum(shape) + 1)
     M = pb.model
@@ -66,12 +68,12 @@ def test_tc_forward_ragged(pb, shape):
     idd[rng.random((nl, nz)) < 0.3] = 0.0
     sig = rng.uniform(0.2, 0.8, (nl, nz))
     prob = M.PBProblem(grid, lat, idd, sig)
-    d = pb.engines.torch_separable(prob, "cuda", precision="tf32x3").cpu().numpy()
+    d = pb.engines.torch_separable(prob, "cuda", precision=prec).cpu().numpy()
     ref = er.separable_f64(grid.x, grid.y, lat.spot_x, lat.spot_y, w, idd, sig)
     if np.max(np.abs(ref)) == 0:
         assert np.all(d == 0)
     else:
-        assert rel(d, ref) < TOL["tf32x3"]
+        assert rel(d, ref) < TOL[prec]
 
 
 def test_tc_rejects_large_lattice(pb):
@@ -85,13 +87,14 @@ def test_tc_rejects_large_lattice(pb):
     assert d.shape == (4, 16, 16)
 
 
-def test_tc_loss_grad_and_batch(pb):
+@pytest.mark.parametrize("prec", ["tf32x3", "fp16x3"])
+def test_tc_loss_grad_and_batch(pb, prec):
     import torch
     wl = pb.workloads.build_workload(0)
     en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
     prob = pb.model.problem_from_workload(wl, energies=en)
     ref_plan = pb.engines.DosePlan(prob, tables="device", precision="fp32")
-    tc_plan = pb.engines.DosePlan(prob, tables="device", precision="tf32x3")
+    tc_plan = pb.engines.DosePlan(prob, tables="device", precision=prec)
     mask, presc = pb.workloads.target_loss_arrays(wl["grid"], half=1.0, shell=1.0, depth=5.0)
     m = torch.as_tensor(mask, device="cuda")
     p = torch.as_tensor(presc * 100.0, device="cuda")
@@ -101,7 +104,7 @@ def test_tc_loss_grad_and_batch(pb):
     assert rel(b["grad_w"].cpu().numpy(), a["grad_w"].cpu().numpy()) < 1e-5
     scen = [(0, 0, 0, 1.0), (0.3, -0.3, 0.3, 1.035)]
     b32 = pb.robust.ScenarioBatch([prob], scen, precision="fp32")
-    btc = pb.robust.ScenarioBatch([prob], scen, precision="tf32x3")
+    btc = pb.robust.ScenarioBatch([prob], scen, precision=prec)
     b32.run()
     btc.run()
     torch.cuda.synchronize()
@@ -215,7 +218,8 @@ def test_loss_grad_graph_replay_matches_eager(pb):
 # against the float64 oracle fed the reference's own tables (luts_cfg4.npz).  Bounds: FP32
 # and TF32x3 at the north-star 1e-6 of max; the reduced modes pinned at ~5x their measured
 # error (BF16x3 2.0e-6, TF32 2.7e-4, BF16 2.1e-3); the FP64 kernel at 1e-12.
-CFG4_TOL = {"fp32": 1e-6, "tf32x3": 1e-6, "bf16x3": 1e-5, "tf32": 1e-3, "bf16": 1e-2}
+CFG4_TOL = {"fp32": 1e-6, "tf32x3": 1e-6, "fp16x3": 1e-6, "bf16x3": 1e-5, "tf32": 1e-3,
+            "bf16": 1e-2}
 
 
 @pytest.fixture(scope="module")
@@ -229,7 +233,7 @@ def cfg4(pb):
     return prob, ref
 
 
-@pytest.mark.parametrize("prec", ["fp32", "tf32x3", "bf16x3", "tf32", "bf16"])
+@pytest.mark.parametrize("prec", ["fp32", "tf32x3", "fp16x3", "bf16x3", "tf32", "bf16"])
 def test_precision_study_cfg4(pb, cfg4, prec):
     prob, ref = cfg4
     d = pb.engines.torch_separable(prob, "cuda", precision=prec).cpu().numpy()
