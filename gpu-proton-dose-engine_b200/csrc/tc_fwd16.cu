@@ -71,7 +71,9 @@ constexpr uint32_t kColDb = 0, kColDc = 256, kColU = 384;
 constexpr float kGScale = 14.0f;           // log2 of the Gaussians' scale
 constexpr int kGExp = 14;
 
-enum : int { kFirst = 1, kLast = 2, kEnd = 4, kZero = 8, kTab = 16 };
+// kSym: Gx == Gy bit for bit (same grid and lattice along x and y, a diagonal tile): G writes
+// Gy only and stage 1 reads it as its A operand
+enum : int { kFirst = 1, kLast = 2, kEnd = 4, kZero = 8, kTab = 16, kSym = 32 };
 
 struct Step {
     int job, z, tile, l;
@@ -88,8 +90,9 @@ struct Params {
     unsigned long long wait_ns;
     int hold;
     int with_loss;
+    int sym;                     // every job symmetric in x and y (see kSym)
     int K1, N1;
-    int nR, nA1, nB2;            // spot-map ring slots, Gx buffers, sU buffers (Gy: always 2)
+    int nR, nA1, nA2, nB2;       // buffers: spot-map ring slots, Gx, Gy (>= 2), sU
     uint32_t img;                // bytes of one packed spot map (= ring slot)
     uint32_t oW, oA1, oA2, oB2, oTab;   // shared-memory offsets
     int ty4, tx4;                // float4 groups of the per-thread distance table
@@ -102,12 +105,17 @@ struct Params {
 __device__ __forceinline__ uint32_t h2bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
 // a = hi + lo for two adjacent K elements (already scaled into FP16's range), packed as
-// {element 0 in the low half, element 1 in the high half}.
+// {element 0 in the low half, element 1 in the high half}.  hi = a rounded to 11 significant
+// bits in FP32 with integer operations (half an ulp added to the magnitude, low 13 bits
+// cleared), so a - hi is exact and hi converts to FP16 exactly (in FP16's normal range; below it
+// the conversion's rounding is at most 2^-25 of the operand's scale); lo = fp16(a - hi).
+__device__ __forceinline__ float round11(float a) {
+    return __uint_as_float((__float_as_uint(a) + 0x1000u) & 0xFFFFE000u);
+}
 __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
-    const __half2 h = __floats2half2_rn(a, b);
-    const float2 hf = __half22float2(h);
-    hi = h2bits(h);
-    lo = h2bits(__floats2half2_rn(a - hf.x, b - hf.y));
+    const float ha = round11(a), hb = round11(b);
+    hi = h2bits(__floats2half2_rn(ha, hb));
+    lo = h2bits(__floats2half2_rn(a - ha, b - hb));
 }
 
 __device__ __forceinline__ void split8(const float* v, uint4& hi, uint4& lo) {
@@ -216,6 +224,11 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
     };
 
     if (!P.hold) {
+        // The unit's data (depth dose, width, spot-map scale of each of its slice's layers) is
+        // loaded in one batch per 32 layers: every load of a unit in flight together.
+        constexpr int kG = 2;                       // layer groups kept in registers (<= 64 layers)
+        // A unit is claimed once the one before is pushed (dynamic balance); its loads then
+        // overlap the steps still queued in the rings.
         for (;;) {
             int u = 0;
             if (lane == 0) u = atomicAdd(P.counter, 1);
@@ -230,11 +243,38 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
             const int nz = J.nz, nl = J.nl;
             if (z >= nz || tile >= J.ntx * J.nty) continue;
             const double* idd = J.idd;
+            double ivg[kG], sg[kG];
+            float wmg[kG];
+            int ewg[kG];
+            auto load = [&](int b, double& iv, double& sv, float& wm, int& ew) {
+                const int l = b + lane;
+                const bool in = l < nl;
+                iv = in ? idd[(size_t)l * nz + z] : 0.0;
+                sv = in ? J.sigma[(size_t)l * nz + z] : 1.0;
+                wm = in ? P.wmax[(size_t)job * P.lmax + l] : 0.f;
+                ew = in ? P.wexp[(size_t)job * P.lmax + l] : 0;
+            };
+            const bool cached = nl <= 32 * kG;
+            if (cached) {
+#pragma unroll
+                for (int g = 0; g < kG; ++g) load(32 * g, ivg[g], sg[g], wmg[g], ewg[g]);
+            }
+            auto group = [&](int b, double& iv, double& sv, float& wm, int& ew) {
+                if (cached) {
+                    const int g = b >> 5;
+                    iv = g == 0 ? ivg[0] : ivg[1];
+                    sv = g == 0 ? sg[0] : sg[1];
+                    wm = g == 0 ? wmg[0] : wmg[1];
+                    ew = g == 0 ? ewg[0] : ewg[1];
+                } else {
+                    load(b, iv, sv, wm, ew);
+                }
+            };
             int tot = 0;
             for (int b = 0; b < nl; b += 32) {
-                const int l = b + lane;
-                const bool a = l < nl && idd[(size_t)l * nz + z] != 0.0;
-                tot += __popc(__ballot_sync(FULL, a));
+                double iv, sv; float wm; int ew;
+                group(b, iv, sv, wm, ew);
+                tot += __popc(__ballot_sync(FULL, iv != 0.0));
             }
             if (tot == 0) {
                 if (c == 0) {
@@ -248,21 +288,20 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
             const int nch = (tot + P.chunk - 1) / P.chunk;
             if (c >= nch) continue;
             const int r0 = c * P.chunk, r1 = min(tot, r0 + P.chunk);
-            // pass 1: the unit's scale exponent, the smallest over its layers of
+            // the unit's scale exponent: the smallest over its layers of
             // 14 - ceil(log2(bound on |s U|)), so that every s U of the unit fits FP16
             int ks = 127;
             {
                 int rank = 0;
                 for (int b = 0; b < nl && rank < r1; b += 32) {
-                    const int l = b + lane;
-                    const double iv = l < nl ? idd[(size_t)l * nz + z] : 0.0;
+                    double iv, sv; float wm; int ew;
+                    group(b, iv, sv, wm, ew);
                     const unsigned bal = __ballot_sync(FULL, iv != 0.0);
                     const int my = rank + __popc(bal & ((1u << lane) - 1u));
                     if (iv != 0.0 && my >= r0 && my < r1) {
-                        const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
-                        const double sv = fabs(iv) * kInv2Pi / (s * s);
-                        const double wm = (double)P.wmax[(size_t)job * P.lmax + l];
-                        const double bnd = sv * wm * (1.0 + 2.5066282746310002 * s / J.dsx);
+                        const double s = fmax(sv, 1e-9);
+                        const double bnd = fabs(iv) * kInv2Pi / (s * s) * (double)wm *
+                                           (1.0 + 2.5066282746310002 * s / J.dsx);
                         int q = 0;
                         if (bnd > 0.0 && bnd < 1e300) {
                             (void)frexp(bnd, &q);          // bnd < 2^q
@@ -274,21 +313,23 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
                 ks = __reduce_min_sync(FULL, ks);
                 ks = ks > 100 ? 100 : (ks < -100 ? -100 : ks);
             }
+            const int tyy = tile / J.ntx, txx = tile % J.ntx;
+            const int sym = (P.sym && tyy == txx) ? kSym : 0;
             int rank = 0;
             for (int b = 0; b < nl && rank < r1 && ok; b += 32) {
-                const int l = b + lane;
-                const double iv = l < nl ? idd[(size_t)l * nz + z] : 0.0;
+                double iv, sv; float wm; int ew;
+                group(b, iv, sv, wm, ew);
                 const bool a = iv != 0.0;
                 const unsigned bal = __ballot_sync(FULL, a);
                 const int my = rank + __popc(bal & ((1u << lane) - 1u));
                 const bool mine = a && my >= r0 && my < r1;
                 Step st{};
                 if (mine) {
-                    const double s = fmax(J.sigma[(size_t)l * nz + z], 1e-9);
-                    const int ew = P.wexp[(size_t)job * P.lmax + l];
+                    const int l = b + lane;
+                    const double s = fmax(sv, 1e-9);
                     st.job = job; st.z = z; st.tile = tile; st.l = l;
                     st.chunk = c; st.nch = nch;
-                    st.flags = (my == r0 ? kFirst | kTab : 0) | (my == r1 - 1 ? kLast : 0);
+                    st.flags = (my == r0 ? kFirst | kTab : 0) | (my == r1 - 1 ? kLast : 0) | sym;
                     // U = 2^(14 + e_l) U_true; s U enters stage 2 as 2^ks s U_true, so
                     // D = 2^(14 + ks) D_true
                     st.kd = kGExp + ks;
@@ -326,7 +367,7 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
 // ------------------------------------------------------------------------------------------
 // MMA warps.  role 1: stage 1; role 2: stage 2 hi * hi; role 3: stage 2 cross products.
 // bars: [0,4) wfull, [4,8) wempty (ring slots), then
-//   a1r[2], a1f[2], a2r[2], a2f[2], b2r[2], b2f[2], uf (U full), uu (U free),
+//   a1r[2], a1f[2], a2r[3], a2f[3], b2r[2], b2f[2], uf (U full), uu (U free),
 //   df[2] (D big full), du[2] (D big free), cf (cross full), cu (cross free)
 // ------------------------------------------------------------------------------------------
 struct Bars {
@@ -336,11 +377,11 @@ struct Bars {
 __device__ __forceinline__ Bars make_bars(uint64_t* b) {
     Bars B;
     B.wfull = b; B.wempty = b + 4;
-    B.a1r = b + 8; B.a1f = b + 10; B.a2r = b + 12; B.a2f = b + 14; B.b2r = b + 16; B.b2f = b + 18;
-    B.uf = b + 20; B.uu = b + 21; B.df = b + 22; B.du = b + 24; B.cf = b + 26; B.cu = b + 27;
+    B.a1r = b + 8; B.a1f = b + 10; B.a2r = b + 12; B.a2f = b + 15; B.b2r = b + 18; B.b2f = b + 20;
+    B.uf = b + 22; B.uu = b + 23; B.df = b + 24; B.du = b + 26; B.cf = b + 28; B.cu = b + 29;
     return B;
 }
-constexpr int kNumBars = 28;
+constexpr int kNumBars = 30;
 
 __device__ __forceinline__ void mma_warp(const Params& P, uint32_t sbase, uint32_t tb, int role,
                                          const Step* ring, uint64_t* full, uint64_t* empty,
@@ -367,30 +408,35 @@ __device__ __forceinline__ void mma_warp(const Params& P, uint32_t sbase, uint32
         if (flags & kEnd) break;
         if (flags & kZero) continue;
         if (role == 1) {
-            const int ws = n % P.nR, ia = n % P.nA1;
+            const int ws = n % P.nR, ia = n % P.nA1, ia2 = n % P.nA2;
             ok = wait_bar(&B.wfull[ws], (uint32_t)((n / P.nR) & 1), P.wait_ns);
             ok = ok && wait_bar(&B.a1r[ia], (uint32_t)((n / P.nA1) & 1), P.wait_ns);
             if (n > 0) ok = ok && wait_bar(B.uu, (uint32_t)((n - 1) & 1), P.wait_ns);
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::fence_after_sync();
             if (lane == 0) {
-                const uint32_t a = sbase + P.oA1 + (uint32_t)ia * 2u * aBytes1;
+                // symmetric step: Gx is the Gy buffer (same bits, same layout; K1 == N1)
+                const bool sym = (flags & kSym) != 0;
+                const uint32_t a = sym ? sbase + P.oA2 + (uint32_t)ia2 * 2u * aBytes2
+                                       : sbase + P.oA1 + (uint32_t)ia * 2u * aBytes1;
+                const uint32_t alo = sym ? aBytes2 : aBytes1;
                 const uint32_t w = sbase + P.oW + (uint32_t)ws * P.img;
                 for (int st = 0; st < K1 / 16; ++st) {
                     const uint32_t oa = (uint32_t)st * 2u * plA, ow = (uint32_t)st * 2u * plW;
                     tc::mma_bf16(tb + kColU, tc::smem_desc(a + oa, plA, 128),
                                  tc::smem_desc(w + ow, plW, 128), id1w, st > 0 ? 1u : 0u);
-                    tc::mma_bf16(tb + kColU + (uint32_t)N1, tc::smem_desc(a + aBytes1 + oa, plA, 128),
+                    tc::mma_bf16(tb + kColU + (uint32_t)N1, tc::smem_desc(a + alo + oa, plA, 128),
                                  tc::smem_desc(w + ow, plW, 128), id1n, 1u);
                 }
                 tc::commit(B.uf);
                 tc::commit(&B.a1f[ia]);
                 tc::commit(&B.wempty[ws]);
+                tc::commit(&B.a2f[ia2]);   // Gy buffers are released by stage 1 as well
             }
             __syncwarp();
         } else {
-            const int ia = n & 1, ib = n % P.nB2, db = n & 1;
-            ok = wait_bar(&B.a2r[ia], (uint32_t)((n >> 1) & 1), P.wait_ns);
+            const int ia = n % P.nA2, ib = n % P.nB2, db = n & 1;
+            ok = wait_bar(&B.a2r[ia], (uint32_t)((n / P.nA2) & 1), P.wait_ns);
             ok = ok && wait_bar(&B.b2r[ib], (uint32_t)((n / P.nB2) & 1), P.wait_ns);
             const bool first = (flags & kFirst) != 0;
             if (role == 2 && n >= 2)
@@ -589,12 +635,15 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
         }
     };
 
-    // G: the Gaussian operands of step m (= ng) into buffers A1[m % nA1], A2[m & 1].
+    // G: the Gaussian operands of step m (= ng) into buffers A1[m % nA1], A2[m % nA2].  Stage 2
+    // of step m - 2 becomes ready only in this iteration (E1 of step m - 1 precedes it), so with
+    // three Gy buffers G never waits for it.
     auto gen = [&](const Step& st, int m) -> bool {
-        const int ia = m % P.nA1, ia2 = m & 1;
+        const int ia = m % P.nA1, ia2 = m % P.nA2;
         bool w = true;
         if (m >= P.nA1) w = wait_bar(&B.a1f[ia], (uint32_t)(((m / P.nA1) - 1) & 1), P.wait_ns);
-        if (m >= 2) w = w && wait_bar(&B.a2f[ia2], (uint32_t)(((m >> 1) - 1) & 1), P.wait_ns);
+        if (m >= P.nA2)
+            w = w && wait_bar(&B.a2f[ia2], (uint32_t)(((m / P.nA2) - 1) & 1), P.wait_ns);
         if (!__all_sync(0xffffffffu, w)) return false;
         const JobDev& J = P.jobs[st.job];
         if (st.flags & kTab) {
@@ -633,33 +682,25 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
         const float a2 = st.a2;
         uint8_t* a2h = smem + P.oA2 + (uint32_t)ia2 * 2u * aBytes2;
         uint8_t* a1h = smem + P.oA1 + (uint32_t)ia * 2u * aBytes1;
+        auto operand = [&](int tab0, int nc, uint8_t* dst, uint32_t lo_off) {
 #pragma unroll
-        for (int r = 0; r < kMaxR; ++r) {
-            const int g = ghalf + 2 * r;
-            if (r < N1 / 16) {
-                const float4 p = tab[(2 * r) * kMath + tid], q4 = tab[(2 * r + 1) * kMath + tid];
-                float v[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
+            for (int r = 0; r < kMaxR; ++r) {
+                if (r < nc) {
+                    const float4 p = tab[(tab0 + 2 * r) * kMath + tid];
+                    const float4 q4 = tab[(tab0 + 2 * r + 1) * kMath + tid];
+                    float v[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
 #pragma unroll
-                for (int e = 0; e < 8; ++e) v[e] = ex2_approx(fmaf(-v[e], a2, kGScale));
-                uint4 hi, lo;
-                split8(v, hi, lo);
-                const uint32_t off = (uint32_t)g * 2048u + (uint32_t)grow * 16u;
-                *reinterpret_cast<uint4*>(a2h + off) = hi;
-                *reinterpret_cast<uint4*>(a2h + aBytes2 + off) = lo;
+                    for (int e = 0; e < 8; ++e) v[e] = ex2_approx(fmaf(-v[e], a2, kGScale));
+                    uint4 hi, lo;
+                    split8(v, hi, lo);
+                    const uint32_t off = (uint32_t)(ghalf + 2 * r) * 2048u + (uint32_t)grow * 16u;
+                    *reinterpret_cast<uint4*>(dst + off) = hi;
+                    *reinterpret_cast<uint4*>(dst + lo_off + off) = lo;
+                }
             }
-            if (r < K1 / 16) {
-                const float4 p = tab[(P.ty4 + 2 * r) * kMath + tid];
-                const float4 q4 = tab[(P.ty4 + 2 * r + 1) * kMath + tid];
-                float v[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
-#pragma unroll
-                for (int e = 0; e < 8; ++e) v[e] = ex2_approx(fmaf(-v[e], a2, kGScale));
-                uint4 hi, lo;
-                split8(v, hi, lo);
-                const uint32_t off = (uint32_t)g * 2048u + (uint32_t)grow * 16u;
-                *reinterpret_cast<uint4*>(a1h + off) = hi;
-                *reinterpret_cast<uint4*>(a1h + aBytes1 + off) = lo;
-            }
-        }
+        };
+        operand(0, N1 / 16, a2h, aBytes2);
+        if (!(st.flags & kSym)) operand(P.ty4, K1 / 16, a1h, aBytes1);
         tc::fence_async_smem();
         __syncwarp();
         if (lane == 0) {
@@ -812,11 +853,13 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc16_kernel(Params P) {
             tc::mbar_init(&B.wfull[i], 1);             // producer's expect_tx arrival + bytes
             tc::mbar_init(&B.wempty[i], 1);            // stage-1 commit
         }
+        for (int i = 0; i < 3; ++i) {
+            tc::mbar_init(&B.a2r[i], kMathWarps);
+            tc::mbar_init(&B.a2f[i], 3);               // stage 1 and both stage-2 warps
+        }
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&B.a1r[i], kMathWarps);
             tc::mbar_init(&B.a1f[i], 1);
-            tc::mbar_init(&B.a2r[i], kMathWarps);
-            tc::mbar_init(&B.a2f[i], 2);               // both stage-2 warps
             tc::mbar_init(&B.b2r[i], kMathWarps);
             tc::mbar_init(&B.b2f[i], 2);
             tc::mbar_init(&B.df[i], 1);
@@ -865,7 +908,7 @@ __global__ void fwd16_poison_kernel(const JobDev* __restrict__ jobs, int n_jobs,
 
 // Shared-memory plan: buffer counts (largest first that fit) and offsets.
 struct Plan16 {
-    int nR, nA1, nB2;
+    int nR, nA1, nA2, nB2;
     uint32_t img, oW, oA1, oA2, oB2, oTab, total;
     int ty4, tx4;
 };
@@ -876,13 +919,16 @@ bool plan16(int K1, int N1, int max_dyn, Plan16* p) {
     p->tx4 = K1 / 8;
     const uint32_t a1 = 2u * (uint32_t)K1 * 256u, a2 = 2u * (uint32_t)N1 * 256u;
     const uint32_t tab = (uint32_t)(p->ty4 + p->tx4) * (uint32_t)kMath * 16u;
-    static const int cand[][3] = {{3, 2, 2}, {2, 2, 2}, {2, 2, 1}, {2, 1, 1}};
+    // (ring, Gx, Gy, sU) buffers, deepest first; Gy needs at least two (G of step m + 1 runs
+    // before E1 of step m, which stage 2 of step m waits for)
+    static const int cand[][4] = {{3, 2, 3, 1}, {2, 2, 3, 1}, {2, 1, 3, 1}, {2, 2, 2, 1},
+                                  {2, 1, 2, 1}};
     for (const auto& c : cand) {
-        p->nR = c[0]; p->nA1 = c[1]; p->nB2 = c[2];
+        p->nR = c[0]; p->nA1 = c[1]; p->nA2 = c[2]; p->nB2 = c[3];
         p->oW = 0;
         p->oA1 = p->oW + (uint32_t)p->nR * p->img;
         p->oA2 = p->oA1 + (uint32_t)p->nA1 * a1;
-        p->oB2 = p->oA2 + 2u * a2;
+        p->oB2 = p->oA2 + (uint32_t)p->nA2 * a2;
         p->oTab = p->oB2 + (uint32_t)p->nB2 * a2;
         p->total = p->oTab + tab;
         if ((int)p->total <= max_dyn) return true;
@@ -920,6 +966,13 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
         nsy = std::max(nsy, jobs_host[j].nsy);
     }
     if (jobs_host[0].layer_stride != 0) return PBD_ERR_UNSUPPORTED;   // per-layer maps: TF32 kernel
+    P.sym = 1;
+    for (int j = 0; j < n_jobs; ++j) {
+        const JobDev& J = jobs_host[j];
+        if (!(J.nx == J.ny && J.ox == J.oy && J.dx == J.dy && J.nsx == J.nsy && J.sx0 == J.sy0 &&
+              J.dsx == J.dsy))
+            P.sym = 0;
+    }
     PBD_TRY(tc_forward_units(jobs_host, n_jobs, chunk, &P.cmax, &P.tmax, &P.n_units));
     const size_t need = tc16_pack_bytes(n_jobs, lmax, P.K1, P.N1);
     if (!pack || pack_bytes < need) return PBD_ERR_WORKSPACE;
@@ -935,7 +988,7 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
     PBD_TRY(smem_optin((const void*)fwd_tc16_kernel, -1, kLaunchRegsNeeded, &max_dyn));
     Plan16 pl;
     if (!plan16(P.K1, P.N1, max_dyn, &pl)) return PBD_ERR_NO_SMEM;
-    P.nR = pl.nR; P.nA1 = pl.nA1; P.nB2 = pl.nB2;
+    P.nR = pl.nR; P.nA1 = pl.nA1; P.nA2 = pl.nA2; P.nB2 = pl.nB2;
     P.oW = pl.oW; P.oA1 = pl.oA1; P.oA2 = pl.oA2; P.oB2 = pl.oB2; P.oTab = pl.oTab;
     P.ty4 = pl.ty4; P.tx4 = pl.tx4;
     // >= 116 KiB: one CTA (and its 512 TMEM columns) per SM
