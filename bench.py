@@ -43,8 +43,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None,
-                    help="fp32 | tf32x3 | bf16x3 | tf32 | bf16; the clinical workload defaults "
-                    "to tf32x3 (tcgen05, <= 1e-6 of max against FP64)")
+                    help="fp32 | fp16x3 | tf32x3 | bf16x3 | tf32 | bf16; the clinical workload "
+                    "defaults to fp16x3 (tcgen05, <= 1e-6 of max against FP64)")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-side-legs", action="store_true",
@@ -285,7 +285,7 @@ def robust_bench(args):
     pb = importlib.import_module("gpu-proton-dose-engine_b200")
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    prec = args.precision or "tf32x3"
+    prec = args.precision or "fp16x3"
     fields = pb.workloads.robust_fields()
     scen = pb.workloads.robust_scenarios()
     probs = pb.robust.robust_problems(fields)
@@ -358,7 +358,7 @@ def optimize_bench(args):
     pb, wl = workload_arrays()
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    prec = args.precision or "tf32x3"
+    prec = args.precision or "fp16x3"
     K, W = args.steps, max(args.warmup, 3)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     prob = pb.model.problem_from_workload(wl)
@@ -651,7 +651,7 @@ def precision_bench(args):
     clocks = ClockSampler(0)
     clocks.start()
     modes = {}
-    for mode in ("fp32", "tf32x3", "bf16x3", "tf32", "bf16"):
+    for mode in ("fp32", "fp16x3", "tf32x3", "bf16x3", "tf32", "bf16"):
         plan = base if mode == "fp32" else pb.engines.DosePlan(prob, tables="device",
                                                                 precision=mode, device=dev)
         plan.idd, plan.sigma = base.idd, base.sigma
@@ -752,13 +752,13 @@ def gpu_baseline_leg(torch, dev, pb, wl, plan, flush, steps, ours_fwd_ms, ours_g
 
 
 def robust_leg(torch, dev, pb, flush, steps, warmup):
-    """The 4-field x 25-scenario batch (100 doses of 128^3): the batched forward in one
-    persistent launch replayed from a CUDA graph, against loops of one pbd_forward per job in
-    plain FP32 and in TF32x3, and the batched loss gradient of all 100 jobs."""
+    """The 4-field x 25-scenario batch (100 doses of 128^3): the batched forward (FP16x3) in
+    one persistent launch replayed from a CUDA graph, against loops of one pbd_forward per job
+    in plain FP32 and in FP16x3, and the batched loss gradient of all 100 jobs."""
     fields = pb.workloads.robust_fields()
     scen = pb.workloads.robust_scenarios()
     probs = pb.robust.robust_problems(fields)
-    sb = pb.robust.ScenarioBatch(probs, scen, precision="tf32x3", device=dev, with_grad=True)
+    sb = pb.robust.ScenarioBatch(probs, scen, precision="fp16x3", device=dev, with_grad=True)
     m_np, p_np = pb.workloads.target_loss_arrays(fields[0]["grid"])
     m = torch.as_tensor(m_np, device=dev)
     p = torch.as_tensor(p_np, device=dev)
@@ -766,8 +766,8 @@ def robust_leg(torch, dev, pb, flush, steps, warmup):
         sb.loop_forward("fp32")
     t_fp32 = _timed(torch, dev, lambda: sb.loop_forward("fp32"), steps, flush)
     for _ in range(warmup):
-        sb.loop_forward("tf32x3")
-    t_tc = _timed(torch, dev, lambda: sb.loop_forward("tf32x3"), steps, flush)
+        sb.loop_forward("fp16x3")
+    t_tc = _timed(torch, dev, lambda: sb.loop_forward("fp16x3"), steps, flush)
     loop_doses = [d.clone() for d in sb._loop_doses]
     sb.capture()
     for _ in range(warmup):
@@ -784,10 +784,11 @@ def robust_leg(torch, dev, pb, flush, steps, warmup):
     return {"workload": "4 fields (21x21x16, 33x33x28, 41x41x40, 51x41x48 spots x layers) x 25 "
                         "scenarios (setup shifts +-3 mm, range x0.965/1.035, 4 corners), 128^3",
             "jobs": n, "batched_forward_ms": t_batch, "doses_per_s": n * 1e3 / t_batch,
-            "loop_fp32_forward_ms": t_fp32, "loop_tf32x3_forward_ms": t_tc,
-            "speedup_vs_fp32_loop": t_fp32 / t_batch, "speedup_vs_tf32x3_loop": t_tc / t_batch,
+            "precision": "fp16x3 (batch and second loop)",
+            "loop_fp32_forward_ms": t_fp32, "loop_fp16x3_forward_ms": t_tc,
+            "speedup_vs_fp32_loop": t_fp32 / t_batch, "speedup_vs_fp16x3_loop": t_tc / t_batch,
             "batched_loss_grad_ms": t_grad, "grad_evals_per_s": n * 1e3 / t_grad,
-            "batched_vs_tf32x3_loop_max_rel": worst, "l2": "flushed between steps"}
+            "batched_vs_fp16x3_loop_max_rel": worst, "l2": "flushed between steps"}
 
 
 def precision_leg(torch, dev, pb, flush, steps, warmup):
@@ -807,7 +808,7 @@ def precision_leg(torch, dev, pb, flush, steps, warmup):
     ref_max = float(d64.abs().max())
     modes = {"fp64": {"ms": t64, "tflops_credited": flop / (t64 * 1e-3) / 1e12,
                       "max_rel_err": 0.0}}
-    for mode in ("fp32", "tf32x3", "bf16x3", "tf32", "bf16"):
+    for mode in ("fp32", "fp16x3", "tf32x3", "bf16x3", "tf32", "bf16"):
         plan = base if mode == "fp32" else pb.engines.DosePlan(prob, tables="device",
                                                                 precision=mode, device=dev)
         plan.idd, plan.sigma = base.idd, base.sigma
@@ -853,7 +854,7 @@ def main():
                                 device_id=dev)
     pb, wl = workload_arrays()
     lib = pb._lib
-    prec = args.precision or "tf32x3"
+    prec = args.precision or "fp16x3"
     prob = pb.model.problem_from_workload(wl)
     plan = pb.engines.DosePlan(prob, tables="device", precision=prec, device=dev)
     active = plan.active_pairs()
@@ -971,8 +972,8 @@ def main():
         kname = "fwd_simt_kernel" if prec == "fp32" else "fwd_tc_kernel"
     # the split forms' own ceiling: TF32 runs at half the BF16 rate, three products per MAC
     # (BF16x3: the BF16 rate, three products); credited FLOPs count one product
-    split_ceiling = {"tf32x3": peak / 6.0, "bf16x3": peak / 3.0, "tf32": peak / 2.0,
-                     "bf16": peak}.get(prec if dom == "forward" else "bf16x3")
+    split_ceiling = {"fp16x3": peak / 3.0, "tf32x3": peak / 6.0, "bf16x3": peak / 3.0,
+                     "tf32": peak / 2.0, "bf16": peak}.get(prec if dom == "forward" else "bf16x3")
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": read_traffic(kname), "kernel": kname,
             "kernel_ms_per_launch": dom_ms, "flop_per_launch": per_launch_flop,
@@ -985,8 +986,8 @@ def main():
             "fwd_ms_per_launch": prof["fwd_ms"] / max(prof["n_fwd"], 1),
             "adj_ms_per_launch": prof["adj_ms"] / max(prof["n_adj"], 1)}
 
-    adj_mode = {"tf32x3": "bf16x3", "tf32": "bf16x3", "bf16x3": "bf16x3", "bf16": "bf16",
-                "fp32": "fp32"}[prec]
+    adj_mode = {"fp16x3": "bf16x3", "tf32x3": "bf16x3", "tf32": "bf16x3", "bf16x3": "bf16x3",
+                "bf16": "bf16", "fp32": "fp32"}[prec]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": max(args.warmup, 3), "ms_per_step": t_ms / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"{prec} fwd / {adj_mode} adj",

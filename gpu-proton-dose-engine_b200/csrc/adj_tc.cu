@@ -88,6 +88,9 @@ struct Params {
     unsigned long long wait_ns;   // limit of every bounded wait
     int hold;            // test of the timeout path: the scheduler publishes no step
     int N1;              // x-lattice padded to 16
+    int stage;           // 1: each unit's dL/dD slice arrives by bulk copy into a staging buffer
+                         //    (every job's slice is contiguous, 16-byte aligned, nx ny % 4 == 0)
+    uint32_t o_stage;    // its shared-memory offset
 };
 
 struct Layout {
@@ -129,10 +132,11 @@ __device__ __forceinline__ void split8(const float* v, uint4& hi, uint4& lo) {
 // Scheduler warp: units (z, chunk) -> one step per active layer.
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint64_t* full,
-                                               uint64_t* empty) {
+                                               uint64_t* empty, uint8_t* smem, uint64_t* sfull,
+                                               uint64_t* sfree) {
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
-    int k = 0;
+    int k = 0, nu = 0;       // ring pushes; units whose slice was copied into the staging buffer
     bool ok = true;
     auto push = [&](int src, const Step& st) -> bool {
         const int slot = k % kRing, n = k / kRing;
@@ -170,6 +174,27 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
         const int r0 = c * P.chunk;
         if (r0 >= tot) continue;   // no chunk c here (slices no layer reaches carry no gradient)
         const int r1 = min(tot, r0 + P.chunk);
+        if (P.stage) {
+            // the unit's dL/dD slice into the staging buffer, once the math warps have converted
+            // the previous unit's copy
+            bool w = true;
+            if (nu > 0) w = wait_bar(sfree, (uint32_t)((nu - 1) & 1), P.wait_ns);
+            if (!__all_sync(FULL, w)) { ok = false; break; }
+            if (lane == 0) {
+                const uint32_t bytes = (uint32_t)J.nx * (uint32_t)J.ny * 4u;
+                const uint32_t dst = tc::smem_u32(smem) + P.o_stage;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                                 tc::smem_u32(sfull)), "r"(bytes)
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                    "[%3];" ::"r"(dst),
+                    "l"(J.grad_dose + (size_t)z * J.ny * J.nx), "r"(bytes), "r"(tc::smem_u32(sfull))
+                    : "memory");
+            }
+            __syncwarp();
+            ++nu;
+        }
         int rank = 0;
         for (int b = 0; b < nl && rank < r1 && ok; b += 32) {
             const int l = b + lane;
@@ -203,6 +228,9 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
         st.flags = kEnd;
         (void)push(0, st);
     }
+    // the last staging copy lands before the block exits
+    if (nu > 0) (void)wait_bar(sfull, (uint32_t)((nu - 1) & 1), P.wait_ns);
+    if (!ok && lane == 0) atomicExch(P.err, 1);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -274,7 +302,8 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
 template <int MODE>
 __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uint8_t* smem,
                                            uint32_t tb, const Step* ring, uint64_t* full,
-                                           uint64_t* empty, uint64_t* bars) {
+                                           uint64_t* empty, uint64_t* bars, uint64_t* sfull,
+                                           uint64_t* sfree) {
     using Pr = Prec<MODE>;
     constexpr int NARR = Pr::NPROD == 3 ? 2 : 1;
     uint64_t* ops1 = bars + 0;
@@ -294,7 +323,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
     bool ok = true;
     Step prev{};
     bool have_prev = false;
-    int k = 0, n = 0;
+    int k = 0, n = 0, nu = 0;
     float ybase = 0.f;                     // (y0 of this thread's columns) - ys_j, per unit
 
     for (;;) {
@@ -314,7 +343,14 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
 
         // ---- unit start: G^T of the slice (rows x, K = y; zero outside the grid) ----
         if (cur.flags & kFirst) {
+            // the slice from the staging buffer (bulk copy issued by the scheduler when it
+            // claimed the unit) or, for slices that cannot be bulk copied, from global memory
             const float* g = J.grad_dose + (size_t)cur.z * ny * nx;
+            if (P.stage) {
+                ok = wait_bar(sfull, (uint32_t)(nu & 1), P.wait_ns);
+                if (!__all_sync(0xffffffffu, ok)) break;
+                g = reinterpret_cast<const float*>(smem + P.o_stage);
+            }
 #pragma unroll 2
             for (int r = 0; r < 8; ++r) {
                 const int e = tid + r * kMath;
@@ -331,6 +367,11 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
                 *reinterpret_cast<uint4*>(smem + L.gth + off) = hi;
                 if (NARR == 2) *reinterpret_cast<uint4*>(smem + L.gtl + off) = lo;
             }
+            if (P.stage) {
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(sfree);   // the staging buffer is free again
+                ++nu;
+            }
             const double cy = 0.5 * (double)(nsy - 1);
             ybase = (float)((J.oy + (double)(64 * half) * J.dy) - (J.sy0 + ((double)jrow - cy) * J.dsy));
         }
@@ -339,7 +380,10 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         // The j lane evaluates the exponentials of columns c < 32 of the two rows, the j'
         // lane those of columns 32 + c; a shuffle swaps them.  Each column's value is the
         // same FP32 computation as evaluating it in place.
-        {
+        // a warp whose 32 TMEM rows are all padding (m >= 2 nsy) skips G and E1: those rows of
+        // every product only ever feed rows of Q that are never read
+        const bool pad_warp = 32 * sp >= 2 * nsy;
+        if (!pad_warp) {
             const float dyf = (float)J.dy;
             const bool valid = jrow < nsy;
             const float cself = deriv ? 32.f : 0.f;   // first column of this lane's exponentials
@@ -457,7 +501,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         if (ok) ph1 ^= 1;
         if (!__all_sync(0xffffffffu, ok)) break;
         tc::fence_after_sync();
-        {
+        if (!pad_warp) {
             uint32_t r[4][16];
 #pragma unroll
             for (int c = 0; c < 4; ++c)
@@ -537,6 +581,7 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     __shared__ __align__(8) uint64_t full[kRing];
     __shared__ __align__(8) uint64_t empty[kRing];
     __shared__ __align__(8) uint64_t bars[4];   // ops1, ops2, mma1, mma2
+    __shared__ __align__(8) uint64_t sbars[2];  // staging buffer full, free
     __shared__ Step ring[kRing];
     __shared__ uint32_t tmem_base_s;
 
@@ -550,6 +595,8 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
             tc::mbar_init(&full[i], 1);
             tc::mbar_init(&empty[i], kMathWarps + 2);   // math warps + both MMA warps
         }
+        tc::mbar_init(&sbars[0], 1);                    // the scheduler's expect_tx + bytes
+        tc::mbar_init(&sbars[1], kMathWarps);
         tc::mbar_init(&bars[0], kMathWarps);
         tc::mbar_init(&bars[1], kMathWarps);
         tc::mbar_init(&bars[2], 1);
@@ -567,7 +614,7 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     if (warp >= kMathWarps) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
         if (warp == kSchedWarp) {
-            scheduler_warp(P, ring, full, empty);
+            scheduler_warp(P, ring, full, empty, smem, &sbars[0], &sbars[1]);
         } else if (warp == kS1Warp || warp == kS2Warp) {
             const Layout L = make_layout<NARR>(P.N1);
             mma_warp<MODE>(P, L, tc::smem_u32(smem), tmem_base_s, warp == kS1Warp ? 1 : 2, ring,
@@ -576,7 +623,7 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     } else {
         asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kMathRegs));
         const Layout L = make_layout<NARR>(P.N1);
-        math_warps<MODE>(P, L, smem, tmem_base_s, ring, full, empty, bars);
+        math_warps<MODE>(P, L, smem, tmem_base_s, ring, full, empty, bars, &sbars[0], &sbars[1]);
     }
 
     tc::fence_before_sync();
@@ -746,8 +793,12 @@ int launch_mode(const Params& P0, cudaStream_t s) {
     // the setmaxnreg split needs the full launch allotment, or its increase never returns
     int max_dyn = 0;
     PBD_TRY(smem_optin((const void*)adj_tc_kernel<MODE>, -1, kLaunchRegsNeeded, &max_dyn));
-    const Params P = P0;
+    Params P = P0;
     size_t smem = adj_smem_bytes<MODE>(P.N1);
+    // the staging buffer (one 128 x 128 FP32 slice) after the operands, when it fits
+    P.o_stage = (uint32_t)align_up(smem, 1024);
+    if (P.stage && P.o_stage + 65536u > (size_t)max_dyn) P.stage = 0;
+    if (P.stage) smem = P.o_stage + 65536u;
     // >= 116 KiB: one CTA, and its 512 TMEM columns, per SM
     smem = std::max<size_t>(smem, 116u * 1024u);
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
@@ -788,6 +839,14 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     P.err = err;
     P.wait_ns = wait_limit_ns();
     P.hold = test_hold();
+    // bulk copies of the dL/dD slices need them contiguous and 16-byte aligned
+    P.stage = 1;
+    for (int j = 0; j < n_jobs; ++j) {
+        const JobDev& J = jobs_host[j];
+        if (((size_t)J.nx * J.ny) % 4 != 0 ||
+            (reinterpret_cast<uintptr_t>(J.grad_dose) & 15u) != 0)
+            P.stage = 0;
+    }
     int cm = 1, nzm = 1, max_l = 1, max_per = 1;
     for (int j = 0; j < n_jobs; ++j) {
         pbd_field f{};

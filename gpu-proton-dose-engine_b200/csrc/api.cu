@@ -1153,6 +1153,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
             fview[k].max_chunks = a.max_chunks_f;
             aview[k] = fview[k];
             aview[k].max_chunks = a.max_chunks_a;
+            aview[k].grad_dose = j.grad_dose;   // the adjoint checks its alignment
             arr += (size_t)f->nz * tiles * kTcFwdWarps;
             fpart += gp.direct ? 0 : pe;
             lpart += (size_t)a.n_loss_part;

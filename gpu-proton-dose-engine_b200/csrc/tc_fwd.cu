@@ -358,63 +358,76 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
 // ------------------------------------------------------------------------------------------
 // Math warps.
 // ------------------------------------------------------------------------------------------
-// Dose (and loss) of 64 voxels of row y from column xb; returns the FP64 sum of m (D - P)^2.
+// Dose (and loss) of 64 voxels of row y from column xb (v = null: zeros); returns the FP64
+// sum of m (D - P)^2.  The mask and prescription are loaded four float4s at a time before any
+// store, so their round trips overlap (the stores could alias the loads otherwise).
 __device__ __forceinline__ double write_final(const JobDev& J, int z, int y, int xb,
                                               const float* v, int with_loss) {
     double lsum = 0.0;
     if (y >= J.ny) return lsum;
     const size_t o = ((size_t)z * J.ny + y) * J.nx + xb;
-    float* d = J.dose + o;
+    float* __restrict__ d = J.dose + o;
     const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
     if (!with_loss) {
 #pragma unroll
         for (int q = 0; q < 64; q += 4) {
+            float x4[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) x4[r] = v ? v[q + r] : 0.f;
             if (vec) {
-                *reinterpret_cast<float4*>(d + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+                *reinterpret_cast<float4*>(d + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
             } else {
 #pragma unroll
                 for (int r = 0; r < 4; ++r)
-                    if (xb + q + r < J.nx) d[q + r] = v[q + r];
+                    if (xb + q + r < J.nx) d[q + r] = x4[r];
             }
         }
         return lsum;
     }
-    const float* mk = J.mask + o;
-    const float* pr = J.presc + o;
-    float* g = J.grad_dose + o;
+    const float* __restrict__ mk = J.mask + o;
+    const float* __restrict__ pr = J.presc + o;
+    float* __restrict__ g = J.grad_dose + o;
 #pragma unroll
-    for (int q = 0; q < 64; q += 4) {
-        float m4[4], p4[4];
-        if (vec) {
-            const float4 a = *reinterpret_cast<const float4*>(mk + q);
-            const float4 b = *reinterpret_cast<const float4*>(pr + q);
-            m4[0] = a.x; m4[1] = a.y; m4[2] = a.z; m4[3] = a.w;
-            p4[0] = b.x; p4[1] = b.y; p4[2] = b.z; p4[3] = b.w;
-        } else {
+    for (int h = 0; h < 64; h += 16) {
+        float m8[16], p8[16];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const bool in = xb + q + r < J.nx;
-                m4[r] = in ? mk[q + r] : 0.f;
-                p4[r] = in ? pr[q + r] : 0.f;
+        for (int q = 0; q < 16; q += 4) {
+            if (vec) {
+                const float4 a = __ldg(reinterpret_cast<const float4*>(mk + h + q));
+                const float4 b = __ldg(reinterpret_cast<const float4*>(pr + h + q));
+                m8[q] = a.x; m8[q + 1] = a.y; m8[q + 2] = a.z; m8[q + 3] = a.w;
+                p8[q] = b.x; p8[q + 1] = b.y; p8[q + 2] = b.z; p8[q + 3] = b.w;
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const bool in = xb + h + q + r < J.nx;
+                    m8[q + r] = in ? mk[h + q + r] : 0.f;
+                    p8[q + r] = in ? pr[h + q + r] : 0.f;
+                }
             }
         }
-        float r4[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            r4[r] = v[q + r] - p4[r];
-            lsum += (double)m4[r] * (double)r4[r] * (double)r4[r];
-        }
-        if (vec) {
-            *reinterpret_cast<float4*>(d + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-            *reinterpret_cast<float4*>(g + q) = make_float4(2.f * m4[0] * r4[0], 2.f * m4[1] * r4[1],
-                                                            2.f * m4[2] * r4[2], 2.f * m4[3] * r4[3]);
-        } else {
+        for (int q = 0; q < 16; q += 4) {
+            float x4[4], r4[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (xb + q + r < J.nx) {
-                    d[q + r] = v[q + r];
-                    g[q + r] = 2.f * m4[r] * r4[r];
-                }
+            for (int r = 0; r < 4; ++r) {
+                x4[r] = v ? v[h + q + r] : 0.f;
+                r4[r] = x4[r] - p8[q + r];
+                lsum += (double)m8[q + r] * (double)r4[r] * (double)r4[r];
+            }
+            if (vec) {
+                *reinterpret_cast<float4*>(d + h + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
+                *reinterpret_cast<float4*>(g + h + q) =
+                    make_float4(2.f * m8[q] * r4[0], 2.f * m8[q + 1] * r4[1], 2.f * m8[q + 2] * r4[2],
+                                2.f * m8[q + 3] * r4[3]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (xb + h + q + r < J.nx) {
+                        d[h + q + r] = x4[r];
+                        g[h + q + r] = 2.f * m8[q + r] * r4[r];
+                    }
+            }
         }
     }
     return lsum;
@@ -626,6 +639,20 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
                     const int i = g * EPC + q;
                     wv[r][q] = (wrg[r] >= 0 && row < nsy && i < nsx) ? __ldg(wl + (size_t)row * nsx + i) : 0.f;
                 }
+            }
+        }
+        // ---- unit start: the mask and prescription of this warp's output rows into L2 ahead
+        // of the unit's output (two 128-byte lines of each) ----
+        if ((cur.flags & kFirst) && P.with_loss) {
+            const int ty = cur.tile / J.ntx, tx = cur.tile % J.ntx;
+            const int y = ty * kTile + trow, xb = tx * kTile + half * 64;
+            if (y < J.ny && xb < J.nx) {
+                const size_t o = ((size_t)cur.z * J.ny + y) * J.nx + xb;
+                const int last = min(63, J.nx - 1 - xb);
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.mask + o));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.mask + o + last));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.presc + o));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.presc + o + last));
             }
         }
         // ---- unit start: this thread's squared distances (FP64 differences) ----

@@ -484,20 +484,21 @@ __device__ __forceinline__ void mma_warp(const Params& P, uint32_t sbase, uint32
 // Math warps.
 // ------------------------------------------------------------------------------------------
 // Dose (and loss) of 64 voxels of row y from column xb (v = null: zeros); returns the FP64
-// sum of m (D - P)^2.
+// sum of m (D - P)^2.  The mask and prescription are loaded four float4s at a time before any
+// store, so their round trips overlap (the stores could alias the loads otherwise).
 __device__ __forceinline__ double write_final(const JobDev& J, int z, int y, int xb,
                                               const float* v, int with_loss) {
     double lsum = 0.0;
     if (y >= J.ny) return lsum;
     const size_t o = ((size_t)z * J.ny + y) * J.nx + xb;
-    float* d = J.dose + o;
+    float* __restrict__ d = J.dose + o;
     const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
+    if (!with_loss) {
 #pragma unroll
-    for (int q = 0; q < 64; q += 4) {
-        float x4[4];
+        for (int q = 0; q < 64; q += 4) {
+            float x4[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) x4[r] = v ? v[q + r] : 0.f;
-        if (!with_loss) {
+            for (int r = 0; r < 4; ++r) x4[r] = v ? v[q + r] : 0.f;
             if (vec) {
                 *reinterpret_cast<float4*>(d + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
             } else {
@@ -505,40 +506,53 @@ __device__ __forceinline__ double write_final(const JobDev& J, int z, int y, int
                 for (int r = 0; r < 4; ++r)
                     if (xb + q + r < J.nx) d[q + r] = x4[r];
             }
-            continue;
         }
-        float m4[4], p4[4];
-        if (vec) {
-            const float4 a = *reinterpret_cast<const float4*>(J.mask + o + q);
-            const float4 b = *reinterpret_cast<const float4*>(J.presc + o + q);
-            m4[0] = a.x; m4[1] = a.y; m4[2] = a.z; m4[3] = a.w;
-            p4[0] = b.x; p4[1] = b.y; p4[2] = b.z; p4[3] = b.w;
-        } else {
+        return lsum;
+    }
+    const float* __restrict__ mk = J.mask + o;
+    const float* __restrict__ pr = J.presc + o;
+    float* __restrict__ g = J.grad_dose + o;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const bool in = xb + q + r < J.nx;
-                m4[r] = in ? J.mask[o + q + r] : 0.f;
-                p4[r] = in ? J.presc[o + q + r] : 0.f;
+    for (int h = 0; h < 64; h += 16) {
+        float m8[16], p8[16];
+#pragma unroll
+        for (int q = 0; q < 16; q += 4) {
+            if (vec) {
+                const float4 a = __ldg(reinterpret_cast<const float4*>(mk + h + q));
+                const float4 b = __ldg(reinterpret_cast<const float4*>(pr + h + q));
+                m8[q] = a.x; m8[q + 1] = a.y; m8[q + 2] = a.z; m8[q + 3] = a.w;
+                p8[q] = b.x; p8[q + 1] = b.y; p8[q + 2] = b.z; p8[q + 3] = b.w;
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const bool in = xb + h + q + r < J.nx;
+                    m8[q + r] = in ? mk[h + q + r] : 0.f;
+                    p8[q + r] = in ? pr[h + q + r] : 0.f;
+                }
             }
         }
-        float r4[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            r4[r] = x4[r] - p4[r];
-            lsum += (double)m4[r] * (double)r4[r] * (double)r4[r];
-        }
-        float* g = J.grad_dose + o;
-        if (vec) {
-            *reinterpret_cast<float4*>(d + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
-            *reinterpret_cast<float4*>(g + q) = make_float4(2.f * m4[0] * r4[0], 2.f * m4[1] * r4[1],
-                                                            2.f * m4[2] * r4[2], 2.f * m4[3] * r4[3]);
-        } else {
+        for (int q = 0; q < 16; q += 4) {
+            float x4[4], r4[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (xb + q + r < J.nx) {
-                    d[q + r] = x4[r];
-                    g[q + r] = 2.f * m4[r] * r4[r];
-                }
+            for (int r = 0; r < 4; ++r) {
+                x4[r] = v ? v[h + q + r] : 0.f;
+                r4[r] = x4[r] - p8[q + r];
+                lsum += (double)m8[q + r] * (double)r4[r] * (double)r4[r];
+            }
+            if (vec) {
+                *reinterpret_cast<float4*>(d + h + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
+                *reinterpret_cast<float4*>(g + h + q) =
+                    make_float4(2.f * m8[q] * r4[0], 2.f * m8[q + 1] * r4[1], 2.f * m8[q + 2] * r4[2],
+                                2.f * m8[q + 3] * r4[3]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (xb + h + q + r < J.nx) {
+                        d[h + q + r] = x4[r];
+                        g[h + q + r] = 2.f * m8[q + r] * r4[r];
+                    }
+            }
         }
     }
     return lsum;
@@ -570,7 +584,7 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
     int k = 0;         // ring reads
     int ng = 0;        // steps generated (G done)
     int useg = 0;      // units whose cross accumulator was drained
-    Step s1{}, s2{};   // step ng - 1 (awaiting E1) and ng - 2 (awaiting DR)
+    Step s1{}, s2{};   // step ng - 1 (awaiting E1) and ng - 2 (awaiting DR), when pending
 
     // Output of this warp's rows of a finished unit (dsum = its dose), then dsum = 0; or, for a
     // slice no layer reaches, zeros (dsum, which may hold a unit in progress, untouched).
@@ -646,6 +660,20 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
             w = w && wait_bar(&B.a2f[ia2], (uint32_t)(((m / P.nA2) - 1) & 1), P.wait_ns);
         if (!__all_sync(0xffffffffu, w)) return false;
         const JobDev& J = P.jobs[st.job];
+        if ((st.flags & kFirst) && P.with_loss) {
+            // the mask and prescription of this warp's output rows, into L2 ahead of the unit's
+            // output (two 128-byte lines of each)
+            const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
+            const int y = ty * kTile + trow, xb = tx * kTile + half * 64;
+            if (y < J.ny && xb < J.nx) {
+                const size_t o = ((size_t)st.z * J.ny + y) * J.nx + xb;
+                const int last = min(63, J.nx - 1 - xb);
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.mask + o));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.mask + o + last));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.presc + o));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.presc + o + last));
+            }
+        }
         if (st.flags & kTab) {
             // this thread's squared distances (FP64 differences), +inf outside the lattice
             const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
@@ -793,39 +821,59 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
         return true;
     };
 
+    // Each iteration: G of the step read (if it has work), E1 of the step before, DR of the one
+    // before that -- one call site each.  A slice no layer reaches, or the end, is handled after
+    // the pending steps are finished (iterations without G): E1 of a step otherwise waits for
+    // the next step with work, which a run of such slices could keep out of the ring.
+    bool p1 = false, p2 = false;   // s1 pending (awaiting E1), s2 pending (awaiting DR)
+    int i1 = 0, i2 = 0;            // their step indices
+    bool flushing = false, at_end = false, zero_pending = false;
+    Step zs{};
     for (;;) {
-        const int slot = k % kRing;
-        ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
-        const Step cur = ring[slot];
-        if (cur.flags != kEnd && (cur.job < 0 || cur.job >= P.n_jobs)) ok = false;
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&empty[slot]);
-        ++k;
-        if (!__all_sync(0xffffffffu, ok)) break;
-        if (cur.flags & kEnd) break;
-        if (cur.flags & kZero) {        // a slice no layer reaches: zeros (and the loss)
-            output(cur, true);
-            continue;
+        Step cur{};
+        bool have = false;
+        if (!flushing) {
+            const int slot = k % kRing;
+            ok = wait_bar(&full[slot], (uint32_t)((k / kRing) & 1), P.wait_ns);
+            cur = ring[slot];
+            if (cur.flags != kEnd && (cur.job < 0 || cur.job >= P.n_jobs)) ok = false;
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&empty[slot]);
+            ++k;
+            if (!__all_sync(0xffffffffu, ok)) break;
+            if (cur.flags & kEnd) {
+                flushing = at_end = true;
+            } else if (cur.flags & kZero) {
+                flushing = zero_pending = true;
+                zs = cur;
+            } else {
+                have = true;
+            }
         }
-        // G(ng), E1(ng - 1), DR(ng - 2)
-        ok = gen(cur, ng);
-        if (!ok) break;
-        if (ng >= 1) {
-            ok = e1(s1, ng - 1);
+        if (have) {
+            ok = gen(cur, ng);
             if (!ok) break;
         }
-        if (ng >= 2) {
-            ok = dr(s2, ng - 2);
+        if (p1) {
+            ok = e1(s1, i1);
             if (!ok) break;
         }
-        s2 = s1;
-        s1 = cur;
-        ++ng;
-    }
-    if (ok && ng >= 1) {
-        ok = e1(s1, ng - 1);
-        if (ok && ng >= 2) ok = dr(s2, ng - 2);
-        if (ok) ok = dr(s1, ng - 1);
+        if (p2) {
+            ok = dr(s2, i2);
+            if (!ok) break;
+        }
+        s2 = s1; i2 = i1; p2 = p1;
+        if (have) {
+            s1 = cur; i1 = ng; p1 = true;
+            ++ng;
+        } else {
+            p1 = false;
+        }
+        if (flushing && !p1 && !p2) {
+            if (zero_pending) output(zs, true);   // zeros (and the loss)
+            zero_pending = flushing = false;
+            if (at_end) break;
+        }
     }
     if (!ok && lane == 0) atomicExch(P.err, 1);
 }

@@ -22,8 +22,9 @@ from . import physics as ph
 from .model import PBProblem
 
 INV_SQRT_2PI = 1.0 / np.sqrt(2.0 * np.pi)
-# "auto": the tensor cores' hi/lo split (TF32x3, within 1e-6 of FP64 and faster than FP32) for
-# lattices they take (<= 64 x 64 spots), else the FP32 kernel on the CUDA cores
+# "auto": the tensor cores' hi/lo split in FP16 (FP16x3: within 1e-6 of FP64 -- 4e-7 on the
+# clinical field -- and the fastest mode that meets it) for lattices they take (<= 64 x 64
+# spots), else the FP32 kernel on the CUDA cores
 DEFAULT_PRECISION = "auto"
 
 
@@ -31,7 +32,7 @@ def resolve_precision(precision, lattice) -> int:
     """Library precision code of ``precision`` for a lattice ("auto": see DEFAULT_PRECISION)."""
     if precision is None or str(precision).lower() == "auto":
         wide = int(lattice.n_sx) > 64 or int(lattice.n_sy) > 64
-        return _lib.PREC["fp32" if wide else "tf32x3"]
+        return _lib.PREC["fp32" if wide else "fp16x3"]
     return _lib.precision_code(precision)
 DEFAULT_FD_STEP = 0.005   # cm: central-difference step of the range-derivative tables
 
@@ -401,13 +402,15 @@ def torch_separable(problem, device: str = "cuda", dtype=None, allow_tf32: bool 
     every call and synchronises before returning.
 
     * ``dtype``: None or torch.float32 give a float32 dose from the tensor cores (split
-      TF32, three products: within 1e-6 of FP64; lattices wider than 64 spots use the FP32
-      kernel on the CUDA cores); torch.float64 gives a float64 dose computed in FP64 on the
-      CUDA cores (the reference's float64 mode, ~1e-15).
+      FP16, three products with power-of-two scaling: within 1e-6 of FP64; lattices wider
+      than 64 spots use the FP32 kernel on the CUDA cores); torch.float64 gives a float64
+      dose computed in FP64 on the CUDA cores (the reference's float64 mode, ~1e-15).
     * ``allow_tf32``: the reference's flag for TF32 tensor cores; its run with the flag
-      kept FP32 accuracy (1.51e-7, benchmark_full.json:68-81), so it maps to the split TF32
-      form as well.  One-product TF32 (~1e-4) is available only as ``precision="tf32"``.
-    * ``precision``: any mode explicitly ("fp32", "tf32x3", "bf16x3", "tf32", "bf16").
+      kept FP32 accuracy (1.51e-7, benchmark_full.json:68-81), so it keeps the default
+      split form, within 1e-6.  One-product TF32 (~1e-4) is available only as
+      ``precision="tf32"``.
+    * ``precision``: any mode explicitly ("fp32", "fp16x3", "tf32x3", "bf16x3", "tf32",
+      "bf16").
     * ``layer_chunk``: active layers per forward work item, for this call only (the
       reference used it to bound memory; here it only sets the work granularity).
 
