@@ -64,6 +64,7 @@ __global__ void install_table_kernel(JobTable t, JobDev* dst, float* partial_bas
     J.sx0 = a.sx0; J.sy0 = a.sy0; J.dsx = a.dsx; J.dsy = a.dsy;
     J.w = a.w; J.idd = a.idd; J.sigma = a.sigma; J.dose = a.dose;
     J.partial = a.direct ? a.dose : partial_base + a.partial_off;
+    J.direct = a.direct;
     J.nchunks = nchunk_base + a.nchunk_off;
     J.arrive = arrive_base + a.arrive_off;
     dst[k] = J;
@@ -120,6 +121,7 @@ __global__ void install_grad_kernel(GradTable t, GradBufs b) {
     JobDev F = J, A = J;
     F.max_chunks = a.max_chunks_f;
     F.partial = a.direct ? a.dose : b.fpart + a.fpart_off;
+    F.direct = a.direct;
     F.arrive = b.farr + a.arrive_off;
     A.max_chunks = a.max_chunks_a;
     A.partial = b.apart + a.slot_off;
@@ -217,7 +219,7 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
     w.counters = c.take<int>(8 + narr);
     w.farr = w.counters ? w.counters + 8 : nullptr;
     w.n_fcount = 8 + narr;
-    w.n_loss_part = precision == PBD_PREC_FP32 ? kLossBlocks : f->nz * tiles * kTcFwdWarps;
+    w.n_loss_part = loss_partials(f, precision);
     w.f_chunk = choose_fwd_chunk(f, precision);
     w.a_chunk = choose_adj_chunk(f);
     w.fitems = nullptr; w.fnch = nullptr; w.fpart = nullptr; w.loss_part = nullptr;
@@ -338,6 +340,12 @@ int host_validate_field(const pbd_field* f) {
         !isfinite(f->y0))
         return PBD_ERR_BAD_VALUE;
     return PBD_OK;
+}
+
+int loss_partials(const pbd_field* f, int precision) {
+    const int tiles = ((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile);
+    if (precision == PBD_PREC_FP32 || precision == PBD_PREC_FP16X3) return kLossBlocks;
+    return f->nz * tiles * kTcFwdWarps;
 }
 
 int fill_job(const pbd_field* f, JobDev* J) {
@@ -709,6 +717,7 @@ constexpr int kBatchAdjChunk = 8;
 
 struct GradPlan {
     int chunk, direct, with_range, max_l;
+    int fprec;           // the forward's precision (split FP16 needs direct mode here)
     size_t arr, fpart, lpart, apart, dcs, pack;
 };
 
@@ -735,8 +744,11 @@ static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, 
         chunk = ch < chunk ? ch : chunk;
     }
     gp->max_l = max_l;
-    gp->pack = precision == PBD_PREC_FP16X3 ? tc16_pack_bytes(n_jobs, max_l, max_sx, max_sy) : 0;
     gp->direct = (max_l <= kMaxChunkCost && g_fwd_chunk == 0) ? 1 : 0;
+    // the split-FP16 forward's partial slices need per-slice chunk counts, which this path
+    // keeps only in direct mode; otherwise its forward runs split TF32 (same accuracy class)
+    gp->fprec = (precision == PBD_PREC_FP16X3 && !gp->direct) ? PBD_PREC_TF32X3 : precision;
+    gp->pack = gp->fprec == PBD_PREC_FP16X3 ? tc16_pack_bytes(n_jobs, max_l, max_sx, max_sy) : 0;
     gp->chunk = gp->direct ? max_l : chunk;
     gp->arr = gp->fpart = gp->lpart = gp->apart = gp->dcs = 0;
     for (int k = 0; k < n_jobs; ++k) {
@@ -747,7 +759,7 @@ static int plan_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, 
         PBD_TRY(fwd_plan_sizes(&f, gp->chunk, &pe, &it));
         gp->arr += (size_t)f.nz * tiles * kTcFwdWarps;
         gp->fpart += gp->direct ? 0 : pe;
-        gp->lpart += (size_t)f.nz * tiles * kTcFwdWarps;
+        gp->lpart += (size_t)loss_partials(&f, gp->fprec);
         gp->apart += tc_adjoint_slot_elems(&f);
         gp->dcs += (size_t)f.n_layers * f.nz;
     }
@@ -876,6 +888,7 @@ int pbd_forward_batch(const pbd_job* jobs, int n_jobs, int precision, void* work
         a.w = jobs[k].w; a.idd = jobs[k].idd; a.sigma = jobs[k].sigma; a.dose = jobs[k].dose;
         a.partial_off = part_off; a.nchunk_off = nch_off; a.arrive_off = arr_off;
         fill_job(f, &host_view[k]);
+        host_view[k].direct = bp.direct;
         item_base += it;
         nch_off += f->nz;
         arr_off += (size_t)f->nz * ((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile) *
@@ -1141,7 +1154,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
             a.max_chunks_f = gp.direct ? 1 : (f->n_layers + gp.chunk - 1) / gp.chunk;
             a.max_chunks_a = (f->n_layers + a_chunk - 1) / a_chunk;
             a.direct = gp.direct;
-            a.n_loss_part = (int)((size_t)f->nz * tiles * kTcFwdWarps);
+            a.n_loss_part = loss_partials(f, gp.fprec);
             a.ox = f->ox; a.oy = f->oy; a.dx = f->dx; a.dy = f->dy;
             a.sx0 = f->x0; a.sy0 = f->y0; a.dsx = f->dx_spot; a.dsy = f->dy_spot;
             a.w = j.w; a.idd = j.idd; a.sigma = j.sigma; a.didd = j.didd_dr; a.dsig = j.dsigma_dr;
@@ -1151,6 +1164,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
             a.dcs_off = dcs;
             fill_job(f, &fview[k]);
             fview[k].max_chunks = a.max_chunks_f;
+            fview[k].direct = a.direct;
             aview[k] = fview[k];
             aview[k].max_chunks = a.max_chunks_a;
             aview[k].grad_dose = j.grad_dose;   // the adjoint checks its alignment
@@ -1165,7 +1179,7 @@ int pbd_loss_grad_batch(const pbd_grad_job* jobs, int n_jobs, int precision, voi
         count_launch(1);
     }
     PBD_TRY(launch_forward(g.fwd, fview, n_jobs, nullptr, 0, g.fcnt, 2 + gp.arr,
-                           g.status + kStatFwd, gp.chunk, 1, precision, 0, g.pack, gp.pack, s));
+                           g.status + kStatFwd, gp.chunk, 1, gp.fprec, 0, g.pack, gp.pack, s));
     return launch_adjoint_tc(precision, g.adj, aview, n_jobs, g.acnt, g.status + kStatAdj, a_chunk,
                              gp.with_range, 1, 1, s);
 }

@@ -108,6 +108,7 @@ extern "C" int pbd_forward_noalloc(const pbd_field* f, const float* w, const dou
     J.item_base = 0;
     J.max_items = items;
     J.partial = dose;     // chunk 0 of every slice is the output itself
+    J.direct = 1;
     J.nchunks = nch;
     cudaStream_t s = (cudaStream_t)stream;
     noalloc_install_kernel<<<1, 32, 0, s>>>(J, jd, counters + 1);

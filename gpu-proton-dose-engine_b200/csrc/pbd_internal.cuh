@@ -47,6 +47,8 @@ struct JobDev {
     size_t layer_stride;          // tensor-core forward: > 0 writes each layer's own dose
                                   // (its lateral map times idd) to dose + l * layer_stride
                                   // instead of the sum over layers; 0 = the dose
+    int direct;                   // forward: partial == dose (one work item per slice writes
+                                  // the dose itself)
 };
 
 struct FwdItem { int job, z, ty, tx, lb, le, chunk, cost; };
@@ -127,6 +129,11 @@ struct JobPlan {
 };
 
 int fill_job(const pbd_field* f, JobDev* j);
+
+// Loss partial sums the forward of `precision` writes for one field (summed in index order by
+// the adjoint's reduce): per (slice, tile, math warp) for the tensor-core forward that forms the
+// loss in its output, per finalize block (kLossBlocks) for the paths with a finalize pass.
+int loss_partials(const pbd_field* f, int precision);
 
 // Status header: the first sub-array of every workspace whose kernels run bounded waits
 // (kStatusInts ints at the workspace's first 256-byte boundary).  Word kStatFwd is the

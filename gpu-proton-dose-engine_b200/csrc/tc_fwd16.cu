@@ -38,12 +38,14 @@
 // that the math warps add in FP32 registers (the tensor core truncates when it accumulates),
 // the cross products (~2^-11 of them) stay in one accumulator per unit.
 //
-// Output (per math warp: 32 rows x 64 columns of the tile) as in the TF32 forward: a unit that
-// holds every active layer of its slice writes its dose rows; otherwise partial rows, summed in
-// chunk order by the warp that completes the slice; with the loss, dL/dD and an FP64 partial
-// of the loss.  Every wait is bounded (2 s of %globaltimer, or the test limit): a warp whose
-// wait runs out sets the error word and leaves, after the MMAs and bulk copies it issued have
-// completed (bounded), and the callers turn the results into NaN.
+// Output (per math warp: 32 rows x 64 columns of the tile): plain stores of the unit's partial
+// slice (or, where every unit holds all layers of its slice, of the dose itself); a finalize
+// pass then sums each voxel's partials in chunk order -- deterministic -- and, with the loss,
+// forms dL/dD = 2 m (D - P) and FP64 partial sums of the loss: the persistent kernel never
+// waits on memory for its outputs.  Every wait is bounded (2 s of %globaltimer, or the test
+// limit): a warp whose wait runs out sets the error word and leaves, after the MMAs and bulk
+// copies it issued have completed (bounded), and the finalize (or poison) pass turns the
+// results into NaN.
 #include <algorithm>
 #include <cuda_fp16.h>
 #include <math.h>
@@ -276,8 +278,14 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
                 group(b, iv, sv, wm, ew);
                 tot += __popc(__ballot_sync(FULL, iv != 0.0));
             }
+            const int nch = (tot + P.chunk - 1) / P.chunk;
+            // the finalize pass sums nch partial slices of slice z (every unit of the slice
+            // writes the same count)
+            if (!J.direct && c == 0 && tile == 0 && lane == 0) J.nchunks[z] = nch;
             if (tot == 0) {
-                if (c == 0) {
+                // a slice no layer reaches: zeros written here when the output is the dose
+                // itself, else by the finalize pass (zero partial slices)
+                if (c == 0 && J.direct) {
                     Step st{};
                     st.job = job; st.z = z; st.tile = tile;
                     st.nch = 1; st.flags = kFirst | kLast | kZero;
@@ -285,7 +293,6 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
                 }
                 continue;
             }
-            const int nch = (tot + P.chunk - 1) / P.chunk;
             if (c >= nch) continue;
             const int r0 = c * P.chunk, r1 = min(tot, r0 + P.chunk);
             // the unit's scale exponent: the smallest over its layers of
@@ -483,87 +490,6 @@ __device__ __forceinline__ void mma_warp(const Params& P, uint32_t sbase, uint32
 // ------------------------------------------------------------------------------------------
 // Math warps.
 // ------------------------------------------------------------------------------------------
-// Dose (and loss) of 64 voxels of row y from column xb (v = null: zeros); returns the FP64
-// sum of m (D - P)^2.  The mask and prescription are loaded four float4s at a time before any
-// store, so their round trips overlap (the stores could alias the loads otherwise).
-__device__ __forceinline__ double write_final(const JobDev& J, int z, int y, int xb,
-                                              const float* v, int with_loss) {
-    double lsum = 0.0;
-    if (y >= J.ny) return lsum;
-    const size_t o = ((size_t)z * J.ny + y) * J.nx + xb;
-    float* __restrict__ d = J.dose + o;
-    const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
-    if (!with_loss) {
-#pragma unroll
-        for (int q = 0; q < 64; q += 4) {
-            float x4[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) x4[r] = v ? v[q + r] : 0.f;
-            if (vec) {
-                *reinterpret_cast<float4*>(d + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
-            } else {
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    if (xb + q + r < J.nx) d[q + r] = x4[r];
-            }
-        }
-        return lsum;
-    }
-    const float* __restrict__ mk = J.mask + o;
-    const float* __restrict__ pr = J.presc + o;
-    float* __restrict__ g = J.grad_dose + o;
-#pragma unroll
-    for (int h = 0; h < 64; h += 16) {
-        float m8[16], p8[16];
-#pragma unroll
-        for (int q = 0; q < 16; q += 4) {
-            if (vec) {
-                const float4 a = __ldg(reinterpret_cast<const float4*>(mk + h + q));
-                const float4 b = __ldg(reinterpret_cast<const float4*>(pr + h + q));
-                m8[q] = a.x; m8[q + 1] = a.y; m8[q + 2] = a.z; m8[q + 3] = a.w;
-                p8[q] = b.x; p8[q + 1] = b.y; p8[q + 2] = b.z; p8[q + 3] = b.w;
-            } else {
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const bool in = xb + h + q + r < J.nx;
-                    m8[q + r] = in ? mk[h + q + r] : 0.f;
-                    p8[q + r] = in ? pr[h + q + r] : 0.f;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q += 4) {
-            float x4[4], r4[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                x4[r] = v ? v[h + q + r] : 0.f;
-                r4[r] = x4[r] - p8[q + r];
-                lsum += (double)m8[q + r] * (double)r4[r] * (double)r4[r];
-            }
-            if (vec) {
-                *reinterpret_cast<float4*>(d + h + q) = make_float4(x4[0], x4[1], x4[2], x4[3]);
-                *reinterpret_cast<float4*>(g + h + q) =
-                    make_float4(2.f * m8[q] * r4[0], 2.f * m8[q + 1] * r4[1], 2.f * m8[q + 2] * r4[2],
-                                2.f * m8[q + 3] * r4[3]);
-            } else {
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    if (xb + h + q + r < J.nx) {
-                        d[h + q + r] = x4[r];
-                        g[h + q + r] = 2.f * m8[q + r] * r4[r];
-                    }
-            }
-        }
-    }
-    return lsum;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
 __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint32_t tb,
                                            const Step* ring, uint64_t* full, uint64_t* empty,
                                            const Bars& B) {
@@ -586,21 +512,23 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
     int useg = 0;      // units whose cross accumulator was drained
     Step s1{}, s2{};   // step ng - 1 (awaiting E1) and ng - 2 (awaiting DR), when pending
 
-    // Output of this warp's rows of a finished unit (dsum = its dose), then dsum = 0; or, for a
-    // slice no layer reaches, zeros (dsum, which may hold a unit in progress, untouched).
+    // Output of this warp's rows of a finished unit: its dose rows when the unit holds every
+    // layer of a slice whose output is the dose itself (or zeros, for a slice no layer
+    // reaches), else its partial slice (chunk); the finalize pass sums the partials in chunk
+    // order and forms the loss.  Plain stores: nothing here waits.
     auto output = [&](const Step& st, bool zero) {
         const JobDev& J = P.jobs[st.job];
         const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
         const int y = ty * kTile + trow, xb = tx * kTile + half * 64;
-        const int slot = (st.z * (J.ntx * J.nty) + st.tile) * kMathWarps + warp;
-        if (zero || st.nch == 1) {
-            const double ls = warp_sum(write_final(J, st.z, y, xb, zero ? nullptr : dsum, P.with_loss));
-            if (P.with_loss && lane == 0) J.loss_part[slot] = ls;
-        } else {
+        if (y < J.ny) {
             const size_t n3 = (size_t)J.nz * J.ny * J.nx;
+            float* o = (J.direct ? J.dose : J.partial + (size_t)st.chunk * n3) +
+                       ((size_t)st.z * J.ny + y) * J.nx + xb;
             const bool vec = xb + 64 <= J.nx && (J.nx & 3) == 0;
-            if (y < J.ny) {
-                float* o = J.partial + (size_t)st.chunk * n3 + ((size_t)st.z * J.ny + y) * J.nx + xb;
+            if (zero) {
+                for (int q = 0; q < 64; ++q)
+                    if (xb + q < J.nx) o[q] = 0.f;
+            } else {
 #pragma unroll
                 for (int q = 0; q < 64; q += 4) {
                     if (vec) {
@@ -612,35 +540,6 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
                             if (xb + q + r < J.nx) o[q + r] = dsum[q + r];
                     }
                 }
-            }
-            __threadfence();
-            __syncwarp();
-            int last = 0;
-            if (lane == 0) last = atomicAdd(&J.arrive[slot], 1) == st.nch - 1;
-            last = __shfl_sync(0xffffffffu, last, 0);
-            if (last) {
-                __threadfence();
-#pragma unroll
-                for (int q = 0; q < 64; ++q) dsum[q] = 0.f;
-                if (y < J.ny) {
-                    const float* base = J.partial + ((size_t)st.z * J.ny + y) * J.nx + xb;
-                    for (int c = 0; c < st.nch; ++c) {
-                        const float* pc = base + (size_t)c * n3;
-#pragma unroll
-                        for (int q = 0; q < 64; q += 4) {
-                            if (vec) {
-                                const float4 a = __ldcg(reinterpret_cast<const float4*>(pc + q));
-                                dsum[q] += a.x; dsum[q + 1] += a.y; dsum[q + 2] += a.z; dsum[q + 3] += a.w;
-                            } else {
-#pragma unroll
-                                for (int r = 0; r < 4; ++r)
-                                    if (xb + q + r < J.nx) dsum[q + r] += __ldcg(pc + q + r);
-                            }
-                        }
-                    }
-                }
-                const double ls = warp_sum(write_final(J, st.z, y, xb, dsum, P.with_loss));
-                if (P.with_loss && lane == 0) J.loss_part[slot] = ls;
             }
         }
         if (!zero) {
@@ -660,20 +559,6 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
             w = w && wait_bar(&B.a2f[ia2], (uint32_t)(((m / P.nA2) - 1) & 1), P.wait_ns);
         if (!__all_sync(0xffffffffu, w)) return false;
         const JobDev& J = P.jobs[st.job];
-        if ((st.flags & kFirst) && P.with_loss) {
-            // the mask and prescription of this warp's output rows, into L2 ahead of the unit's
-            // output (two 128-byte lines of each)
-            const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
-            const int y = ty * kTile + trow, xb = tx * kTile + half * 64;
-            if (y < J.ny && xb < J.nx) {
-                const size_t o = ((size_t)st.z * J.ny + y) * J.nx + xb;
-                const int last = min(63, J.nx - 1 - xb);
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.mask + o));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.mask + o + last));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.presc + o));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(J.presc + o + last));
-            }
-        }
         if (st.flags & kTab) {
             // this thread's squared distances (FP64 differences), +inf outside the lattice
             const int ty = st.tile / J.ntx, tx = st.tile % J.ntx;
@@ -943,6 +828,79 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc16_kernel(Params P) {
     if (warp == 0) tc::tmem_dealloc(tmem_base_s, kCols);
 }
 
+// Finalize pass (grid (kLossBlocks or more, jobs)): each voxel's dose as the sum of its slice's
+// partial slices in chunk order (or the dose itself, direct), NaN when a wait of the forward ran
+// out; with the loss, dL/dD = 2 m (D - P) and per-block FP64 partial sums of m (D - P)^2 in a
+// fixed order.  Four voxels per thread per step when every slice plane is a multiple of four.
+__global__ void __launch_bounds__(256) fwd16_finalize_kernel(const JobDev* __restrict__ jobs,
+                                                             int with_loss,
+                                                             const int* __restrict__ err) {
+    const JobDev& J = jobs[blockIdx.y];
+    const size_t plane = (size_t)J.nx * J.ny, n = plane * J.nz;
+    const bool bad = *err != 0;
+    const float nan = __int_as_float(0x7fc00000);
+    double lsum = 0.0;
+    auto voxel4 = [&](size_t v, int cnt) {      // voxels v .. v + cnt - 1 of one slice
+        const int z = (int)(v / plane);
+        const int nch = J.direct ? 1 : J.nchunks[z];
+        const float* src = J.direct ? J.dose : J.partial;
+        float s4[4] = {0.f, 0.f, 0.f, 0.f};
+        if (cnt == 4) {
+            for (int k = 0; k < nch; ++k) {
+                const float4 a = __ldcs(reinterpret_cast<const float4*>(src + (size_t)k * n + v));
+                s4[0] += a.x; s4[1] += a.y; s4[2] += a.z; s4[3] += a.w;
+            }
+        } else {
+            for (int k = 0; k < nch; ++k)
+                for (int r = 0; r < cnt; ++r) s4[r] += __ldcs(src + (size_t)k * n + v + r);
+        }
+        if (bad)
+            for (int r = 0; r < 4; ++r) s4[r] = nan;
+        if (!J.direct || bad) {
+            if (cnt == 4) *reinterpret_cast<float4*>(J.dose + v) = make_float4(s4[0], s4[1], s4[2], s4[3]);
+            else for (int r = 0; r < cnt; ++r) J.dose[v + r] = s4[r];
+        }
+        if (with_loss) {
+            float m4[4], p4[4], g4[4];
+            if (cnt == 4) {
+                const float4 a = __ldcs(reinterpret_cast<const float4*>(J.mask + v));
+                const float4 b = __ldcs(reinterpret_cast<const float4*>(J.presc + v));
+                m4[0] = a.x; m4[1] = a.y; m4[2] = a.z; m4[3] = a.w;
+                p4[0] = b.x; p4[1] = b.y; p4[2] = b.z; p4[3] = b.w;
+            } else {
+                for (int r = 0; r < 4; ++r) {
+                    m4[r] = r < cnt ? J.mask[v + r] : 0.f;
+                    p4[r] = r < cnt ? J.presc[v + r] : 0.f;
+                }
+            }
+            for (int r = 0; r < 4; ++r) {
+                const float rr = s4[r] - p4[r];
+                g4[r] = 2.f * m4[r] * rr;
+                if (r < cnt) lsum += (double)m4[r] * (double)rr * (double)rr;
+            }
+            if (cnt == 4) *reinterpret_cast<float4*>(J.grad_dose + v) = make_float4(g4[0], g4[1], g4[2], g4[3]);
+            else for (int r = 0; r < cnt; ++r) J.grad_dose[v + r] = g4[r];
+        }
+    };
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nthr = (size_t)gridDim.x * blockDim.x;
+    if ((plane & 3) == 0) {
+        for (size_t v = 4 * tid; v < n; v += 4 * nthr) voxel4(v, 4);
+    } else {
+        for (size_t v = tid; v < n; v += nthr) voxel4(v, 1);
+    }
+    if (with_loss) {
+        __shared__ double red[256];
+        red[threadIdx.x] = lsum;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) J.loss_part[blockIdx.x] = red[0];
+    }
+}
+
 __global__ void fwd16_poison_kernel(const JobDev* __restrict__ jobs, int n_jobs, const int* err) {
     if (*err == 0) return;
     for (int j = 0; j < n_jobs; ++j) {
@@ -1050,7 +1008,19 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
     PBD_TRY(launch_dependent(fwd_tc16_kernel, dim3(grid), dim3(kThreads), smem, s, P));
     prof_mark(kProfFwd, 1, s);
     count_launch(2);
-    if (poison) {
+    // every job of a launch shares its output mode (the callers set it per launch)
+    if (!jobs_host[0].direct || with_loss) {
+        size_t maxn = 1;
+        for (int j = 0; j < n_jobs; ++j)
+            maxn = std::max(maxn, (size_t)jobs_host[j].nx * jobs_host[j].ny * jobs_host[j].nz);
+        // kLossBlocks blocks with the loss (the adjoint sums that many partials per job)
+        const int blocks = with_loss ? kLossBlocks
+                                     : (int)std::min<size_t>((maxn / 4 + 255) / 256, 4096);
+        fwd16_finalize_kernel<<<dim3(std::max(blocks, 1), n_jobs), 256, 0, s>>>(jobs_dev, with_loss,
+                                                                               err);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    } else if (poison) {
         fwd16_poison_kernel<<<num_sms(), 256, 0, s>>>(jobs_dev, n_jobs, err);
         PBD_LAUNCH_CHECK();
         count_launch(1);
