@@ -108,22 +108,28 @@ __device__ __forceinline__ Layout make_layout(int N1) {
     return L;
 }
 
+// Two adjacent K elements as packed bf16 {a in the low half, b in the high half}: hi, and for
+// split modes lo = bf16 of the remainders (the hi values back in FP32 are exact bit shifts).  One
+// packed conversion per word.
+template <int NARR>
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    if (NARR == 2) {
+        const __nv_bfloat162 l = __floats2bfloat162_rn(a - __uint_as_float(hi << 16),
+                                                       b - __uint_as_float(hi & 0xFFFF0000u));
+        lo = *reinterpret_cast<const uint32_t*>(&l);
+    } else {
+        lo = 0u;
+    }
+}
+
 // Split 8 floats into packed bf16 hi / lo words (lo = bf16 of the remainder).
 template <int NARR>
 __device__ __forceinline__ void split8(const float* v, uint4& hi, uint4& lo) {
     uint32_t h[4], l[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const uint32_t ha = bf16_bits(v[2 * q]), hb = bf16_bits(v[2 * q + 1]);
-        h[q] = ha | (hb << 16);
-        if (NARR == 2) {
-            const float ra = v[2 * q] - __uint_as_float(ha << 16);
-            const float rb = v[2 * q + 1] - __uint_as_float(hb << 16);
-            l[q] = bf16_bits(ra) | (bf16_bits(rb) << 16);
-        } else {
-            l[q] = 0u;
-        }
-    }
+    for (int q = 0; q < 4; ++q) split2<NARR>(v[2 * q], v[2 * q + 1], h[q], l[q]);
     hi = make_uint4(h[0], h[1], h[2], h[3]);
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
@@ -403,16 +409,8 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
                     vl[t] = valid ? (deriv ? el * fmaf(ddl, inv_s3, -inv_s) : el) : 0.f;
                     vh[t] = valid ? (deriv ? eh * fmaf(ddh, inv_s3, -inv_s) : eh) : 0.f;
                 }
-                const uint32_t la = bf16_bits(vl[0]), lb = bf16_bits(vl[1]);
-                const uint32_t ha = bf16_bits(vh[0]), hb = bf16_bits(vh[1]);
-                hi[0][kp] = la | (lb << 16);
-                hi[1][kp] = ha | (hb << 16);
-                if (NARR == 2) {
-                    lo[0][kp] = bf16_bits(vl[0] - __uint_as_float(la << 16)) |
-                                (bf16_bits(vl[1] - __uint_as_float(lb << 16)) << 16);
-                    lo[1][kp] = bf16_bits(vh[0] - __uint_as_float(ha << 16)) |
-                                (bf16_bits(vh[1] - __uint_as_float(hb << 16)) << 16);
-                }
+                split2<NARR>(vl[0], vl[1], hi[0][kp], lo[0][kp]);
+                split2<NARR>(vh[0], vh[1], hi[1][kp], lo[1][kp]);
             }
             const uint32_t col = kColA + (uint32_t)b * 128u + (uint32_t)(32 * half);
             tc::tmem_st16(tb + lane_base + col, hi[0]);
@@ -512,11 +510,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             for (int q = 0; q < 32; ++q) {
                 const float va = __uint_as_float(r[q >> 3][(2 * q) & 15]);
                 const float vb = __uint_as_float(r[q >> 3][(2 * q + 1) & 15]);
-                const uint32_t ha = bf16_bits(va), hb = bf16_bits(vb);
-                hi[q >> 4][q & 15] = ha | (hb << 16);
-                if (NARR == 2)
-                    lo[q >> 4][q & 15] = bf16_bits(va - __uint_as_float(ha << 16)) |
-                                         (bf16_bits(vb - __uint_as_float(hb << 16)) << 16);
+                split2<NARR>(va, vb, hi[q >> 4][q & 15], lo[q >> 4][q & 15]);
             }
             const uint32_t col = kColA + (uint32_t)b * 128u + (uint32_t)(32 * half);
             tc::tmem_st16(tb + lane_base + col, hi[0]);

@@ -344,7 +344,8 @@ int host_validate_field(const pbd_field* f) {
 
 int loss_partials(const pbd_field* f, int precision) {
     const int tiles = ((f->nx + kTile - 1) / kTile) * ((f->ny + kTile - 1) / kTile);
-    if (precision == PBD_PREC_FP32 || precision == PBD_PREC_FP16X3) return kLossBlocks;
+    if (precision == PBD_PREC_FP32) return kLossBlocks;
+    if (precision == PBD_PREC_FP16X3) return kLossBlocks16;
     return f->nz * tiles * kTcFwdWarps;
 }
 

@@ -151,15 +151,28 @@ __global__ void __launch_bounds__(256) pack_w16_kernel(const JobDev* __restrict_
     const JobDev& J = jobs[blockIdx.y];
     const int l = blockIdx.x;
     if (l >= J.nl) return;
-    const int nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;
+    const int nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;   // <= 64 x 64
     const float* w = J.w + (size_t)l * per;
     __shared__ float red[8];
+    __shared__ float ws[64 * 64];
+    // the layer's weights into shared memory, every load of a thread issued together
     float m = 0.f;
     bool nonfinite = false;
-    for (int e = threadIdx.x; e < per; e += blockDim.x) {
-        const float a = fabsf(__ldg(w + e));
-        if (!(a <= 3.0e38f)) nonfinite = true;   // NaN or inf: leave the layer unscaled
-        m = fmaxf(m, a);
+    {
+        float v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int e = threadIdx.x + q * 256;
+            v[q] = e < per ? __ldg(w + e) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int e = threadIdx.x + q * 256;
+            if (e < per) ws[e] = v[q];
+            const float a = fabsf(v[q]);
+            if (!(a <= 3.0e38f)) nonfinite = true;   // NaN or inf: leave the layer unscaled
+            m = fmaxf(m, a);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -181,7 +194,7 @@ __global__ void __launch_bounds__(256) pack_w16_kernel(const JobDev* __restrict_
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const int i = 8 * g + k;
-            v[k] = (i < nsx && j < nsy) ? ldexpf(__ldg(w + (size_t)j * nsx + i), e) : 0.f;
+            v[k] = (i < nsx && j < nsy) ? ldexpf(ws[j * nsx + i], e) : 0.f;
         }
         uint4 hi, lo;
         split8(v, hi, lo);
@@ -1013,8 +1026,8 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
         size_t maxn = 1;
         for (int j = 0; j < n_jobs; ++j)
             maxn = std::max(maxn, (size_t)jobs_host[j].nx * jobs_host[j].ny * jobs_host[j].nz);
-        // kLossBlocks blocks with the loss (the adjoint sums that many partials per job)
-        const int blocks = with_loss ? kLossBlocks
+        // kLossBlocks16 blocks with the loss (the adjoint sums that many partials per job)
+        const int blocks = with_loss ? kLossBlocks16
                                      : (int)std::min<size_t>((maxn / 4 + 255) / 256, 4096);
         fwd16_finalize_kernel<<<dim3(std::max(blocks, 1), n_jobs), 256, 0, s>>>(jobs_dev, with_loss,
                                                                                err);
