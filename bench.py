@@ -969,7 +969,7 @@ def main():
     if dom == "adjoint":
         kname = "adj_simt_kernel" if prec == "fp32" else "adj_tc_kernel"
     else:
-        kname = "fwd_simt_kernel" if prec == "fp32" else "fwd_tc_kernel"
+        kname = {"fp32": "fwd_simt_kernel", "fp16x3": "fwd_tc16_kernel"}.get(prec, "fwd_tc_kernel")
     # the split forms' own ceiling: TF32 runs at half the BF16 rate, three products per MAC
     # (BF16x3: the BF16 rate, three products); credited FLOPs count one product
     split_ceiling = {"fp16x3": peak / 3.0, "tf32x3": peak / 6.0, "bf16x3": peak / 3.0,

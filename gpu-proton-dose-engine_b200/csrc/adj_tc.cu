@@ -30,10 +30,10 @@
 //          spot are adjacent lanes of one warp: each lane evaluates the exponentials of half
 //          the row's columns and the pair swaps them (one shuffle per value), so every
 //          exponential of Gy serves Gy' too
-//      DR  pair n-1's Q from TMEM: Q / (2 pi s^2) into two (layer, slice) slots --
-//          P = Q[j, i] and S = Q[j, i'] + Q[j', i] (the j' lane's value moved to the j lane
-//          by shuffle) -- stored transposed ([i][j]) so that the j lanes of a warp write 64
-//          contiguous bytes
+//      DR  pair n-1's Q from TMEM: P = Q[j, i] / (2 pi s^2) into the (layer, slice) slot,
+//          stored transposed ([i][j]) so that the j lanes of a warp write 64 contiguous
+//          bytes; the dot products <P, W> and <S, W>, S = (Q[j, i'] + Q[j', i]) / (2 pi s^2)
+//          (the j' lane's value moved to the j lane by shuffle), summed over the warp
 //      B   [Gx | Gx'] -> smem (read by stage 2 only, whose previous use DR waited for);
 //          each Gaussian value and its derivative come from one exp
 //      E1  Y of pair n from TMEM, split, back into TMEM A[b]; arrive on ops2
@@ -41,9 +41,9 @@
 //    MMA warp 2: stage 2 after ops2 (A = split Y from TMEM), commit to mma2.
 //  Stage 2 of pair n-1 runs under G of pair n; stage 1 of pair n under DR and B.
 //
-// dL/dW_l = sum over active slices of IDD * slot P in slice order, and the dot products
-// <slot, W> for dL/dIDD and dL/dsigma, are formed by one follow-up kernel in a fixed order
-// (deterministic).  Every wait is bounded (2 s of %globaltimer, or a test limit); a warp
+// dL/dW_l = sum over active slices of IDD * slot P in slice order, and the sums of the warps'
+// dot-product partials (dL/dIDD, dL/dsigma), are formed by one follow-up kernel in a fixed
+// order (deterministic).  Every wait is bounded (2 s of %globaltimer, or a test limit); a warp
 // whose wait runs out sets the error word and leaves, the others' waits then run out in
 // turn, and the finalize pass turns the gradients into NaN.
 // Grids of at most 128 x 128 voxels per slice; lattices up to 64 x 64 spots.
@@ -303,6 +303,79 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
 }
 
 // ------------------------------------------------------------------------------------------
+// DR: a pair's Q (TMEM columns from tq: Q[., i] at i, Q[., i'] at N1 + i) -> the pair's P slot
+// and this warp's share of the pair's two dot products.  P = Q[j, i] / (2 pi s^2) is stored
+// transposed ([i][j]) so that the j lanes of a warp write 64 contiguous bytes.  The warps of a
+// lane quadrant split the i columns in chunks of 16 (tcgen05.ld is warp-collective); the j'
+// lane hands Q[j', i] to its j lane by shuffle, so each j lane also holds
+// S[j, i] = (Q[j, i'] + Q[j', i]) / (2 pi s^2) and forms <P, W> and <S, W> over its entries.
+// A butterfly over the warp gives the warp's partial sums, stored per (pair, warp); the
+// follow-up kernel adds the eight warps' partials in warp order.  Padding rows (j >= nsy) hold
+// products of unset TMEM rows and are never read into a sum.
+// ------------------------------------------------------------------------------------------
+// This thread's W entries for pr's DR: W_l[j, i] for its two 16-column chunks (zero where it
+// owns no entry).  Loaded a phase ahead of the DR, so that the load latency is hidden.
+__device__ __forceinline__ void load_w_rows(const Params& P, const Step& pr, int half, int jrow,
+                                            bool deriv, float (&wv)[2][16]) {
+    const JobDev& Jp = P.jobs[pr.job];
+    const int pnsx = Jp.nsx, pnsy = Jp.nsy;
+    const bool row_ok = !deriv && jrow < pnsy;
+    const float* wrow = Jp.w + (size_t)pr.l * pnsy * pnsx + (size_t)(row_ok ? jrow : 0) * pnsx;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int c0 = 16 * half + 32 * t;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int i = c0 + q;
+            wv[t][q] = (row_ok && i < pnsx) ? __ldg(wrow + i) : 0.f;
+        }
+    }
+}
+
+__device__ __forceinline__ void drain_q(const Params& P, const Step& pr, uint32_t tq, int half,
+                                        int jrow, bool deriv, int warp, int lane,
+                                        const float (&wv)[2][16]) {
+    const JobDev& Jp = P.jobs[pr.job];
+    const int pnsx = Jp.nsx, pnsy = Jp.nsy, nz = Jp.nz, N1 = P.N1;
+    const size_t per = (size_t)pnsy * pnsx;
+    const size_t pair = (size_t)pr.l * nz + pr.z;
+    float* slot_p = Jp.partial + pair * per;
+    const bool row_ok = !deriv && jrow < pnsy;
+    float dp = 0.f, ds = 0.f;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int c0 = 16 * half + 32 * t;   // N1 <= 64: at most two chunks per thread
+        if (c0 >= N1) break;
+        uint32_t ri[16], rd[16];
+        tc::tmem_ld16(tq + (uint32_t)c0, ri);
+        tc::tmem_ld16(tq + (uint32_t)(N1 + c0), rd);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int i = c0 + q;
+            const float vi = pr.nrm * __uint_as_float(ri[q]);   // Q[j, i] or Q[j', i]
+            const float vd = pr.nrm * __uint_as_float(rd[q]);   // Q[j, i']
+            const float b = __shfl_xor_sync(0xffffffffu, vi, 1);  // j lane: Q[j', i]
+            if (row_ok && i < pnsx) {
+                slot_p[(size_t)i * pnsy + jrow] = vi;
+                dp = fmaf(vi, wv[t][q], dp);
+                ds = fmaf(vd + b, wv[t][q], ds);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dp += __shfl_xor_sync(0xffffffffu, dp, o);
+        ds += __shfl_xor_sync(0xffffffffu, ds, o);
+    }
+    if (lane == 0) {
+        float* dots = Jp.partial + (size_t)Jp.nl * nz * per;   // (2, nl, nz, kMathWarps)
+        dots[pair * kMathWarps + warp] = dp;
+        dots[((size_t)Jp.nl * nz + pair) * kMathWarps + warp] = ds;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // Math warps.
 // ------------------------------------------------------------------------------------------
 template <int MODE>
@@ -342,6 +415,9 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         ++k;
         if (!__all_sync(0xffffffffu, ok)) break;
         if (cur.flags & kEnd) break;
+        // W of the pair this iteration drains, in flight while G runs
+        float wpre[2][16];
+        if (have_prev) load_w_rows(P, prev, half, jrow, deriv, wpre);
         const JobDev& J = P.jobs[cur.job];
         const int nx = J.nx, ny = J.ny, nsx = J.nsx, nsy = J.nsy;
         const int b = n & 1;
@@ -426,41 +502,13 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(ops1);
 
-        // ---- DR: Q of the previous pair -> the two slots ----
+        // ---- DR: Q of the previous pair -> its P slot and dot products ----
         if (have_prev) {
             ok = ok && wait_bar(mma2, ph2, P.wait_ns);
             if (ok) ph2 ^= 1;
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::fence_after_sync();
-            const JobDev& Jp = P.jobs[prev.job];
-            const int pnsx = Jp.nsx, pnsy = Jp.nsy;
-            const size_t per = (size_t)pnsy * pnsx;
-            // Two slots per (layer, slice): P = Q[j, i] and S = Q[j, i'] + Q[j', i] (each term
-            // scaled first).  The warps of a lane quadrant split the i columns in chunks of 16;
-            // a warp loads its chunk of the i and the i' columns (tcgen05.ld is warp-collective),
-            // the j' lane hands Q[j', i] to its j lane by shuffle, and the j lanes store.
-            {
-                float* slot_p = Jp.partial + ((size_t)prev.l * Jp.nz + prev.z) * per;
-                float* slot_s = slot_p + (size_t)Jp.nl * Jp.nz * per;
-                const bool row_ok = !deriv && jrow < pnsy;
-                for (int c0 = 16 * half; c0 < N1; c0 += 32) {
-                    uint32_t ri[16], rd[16];
-                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)c0, ri);
-                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(N1 + c0), rd);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) {
-                        const int i = c0 + q;
-                        const float vi = prev.nrm * __uint_as_float(ri[q]);   // Q[j, i] or Q[j', i]
-                        const float vd = prev.nrm * __uint_as_float(rd[q]);   // Q[j, i']
-                        const float b = __shfl_xor_sync(0xffffffffu, vi, 1);  // j lane: Q[j', i]
-                        if (row_ok && i < pnsx) {
-                            slot_p[(size_t)i * pnsy + jrow] = vi;
-                            slot_s[(size_t)i * pnsy + jrow] = vd + b;
-                        }
-                    }
-                }
-            }
+            drain_q(P, prev, tb + lane_base + kColQ, half, jrow, deriv, warp, lane, wpre);
         }
 
         // ---- B2 = [Gx | Gx'] -> smem (rows i and N1 + i, K = x).  Only stage 2 reads it,
@@ -534,35 +582,9 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         ok = wait_bar(mma2, ph2, P.wait_ns);
         if (__all_sync(0xffffffffu, ok)) {
             tc::fence_after_sync();
-            const JobDev& Jp = P.jobs[prev.job];
-            const int pnsx = Jp.nsx, pnsy = Jp.nsy;
-            const size_t per = (size_t)pnsy * pnsx;
-            // Two slots per (layer, slice): P = Q[j, i] and S = Q[j, i'] + Q[j', i] (each term
-            // scaled first).  The warps of a lane quadrant split the i columns in chunks of 16;
-            // a warp loads its chunk of the i and the i' columns (tcgen05.ld is warp-collective),
-            // the j' lane hands Q[j', i] to its j lane by shuffle, and the j lanes store.
-            {
-                float* slot_p = Jp.partial + ((size_t)prev.l * Jp.nz + prev.z) * per;
-                float* slot_s = slot_p + (size_t)Jp.nl * Jp.nz * per;
-                const bool row_ok = !deriv && jrow < pnsy;
-                for (int c0 = 16 * half; c0 < N1; c0 += 32) {
-                    uint32_t ri[16], rd[16];
-                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)c0, ri);
-                    tc::tmem_ld16(tb + lane_base + kColQ + (uint32_t)(N1 + c0), rd);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) {
-                        const int i = c0 + q;
-                        const float vi = prev.nrm * __uint_as_float(ri[q]);   // Q[j, i] or Q[j', i]
-                        const float vd = prev.nrm * __uint_as_float(rd[q]);   // Q[j, i']
-                        const float b = __shfl_xor_sync(0xffffffffu, vi, 1);  // j lane: Q[j', i]
-                        if (row_ok && i < pnsx) {
-                            slot_p[(size_t)i * pnsy + jrow] = vi;
-                            slot_s[(size_t)i * pnsy + jrow] = vd + b;
-                        }
-                    }
-                }
-            }
+            float wl[2][16];
+            load_w_rows(P, prev, half, jrow, deriv, wl);
+            drain_q(P, prev, tb + lane_base + kColQ, half, jrow, deriv, warp, lane, wl);
         }
     }
     if (!ok && lane == 0) atomicExch(P.err, 1);
@@ -626,152 +648,100 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     if (warp == 0) tc::tmem_dealloc(tmem_base_s, kCols);
 }
 
-// After the main kernel: dL/dW, the per-pair dot products and dL/dR in one pass over the
-// slots.  Block (segment of kRedZ slices, layer l, job): its threads hold W_l (transposed to
-// the slots' [i][j] order) in registers and walk the segment's active slices in order,
-// accumulating IDD * P slot into a partial dL/dW and forming <P slot, W> (dL/dIDD) and
-// IDD <S slot, W> (dL/dsigma) per slice (warp shuffles, then the warps in order).  The
-// block that completes a layer's last segment (per-layer arrival counter) sums the segment
-// partials in segment order into dL/dW and forms dL/dR_l in FP64; the one completing layer
-// 0 also sums the loss partials.  Every sum is in a fixed order: deterministic.
-constexpr int kRedZ = 8;           // slices per block
+// After the main kernel: dL/dW, the per-pair dot products and dL/dR from the slots, with no
+// block waiting on another.  Block (entry chunk, layer l, job): each thread owns one slot
+// entry e = i * nsy + j of layer l and accumulates IDD * P slot over the layer's active slices
+// in slice order (kRedStep slices' loads in flight together), then writes dL/dW[l, j, i].
+// Chunk 0 of every layer also adds, per active slice, the eight warp partials of <P, W>
+// (dL/dIDD) and <S, W> (dL/dsigma, times IDD) in warp order and forms dL/dR_l in FP64 (a
+// fixed tree over the block); chunk 0 of layer 0 sums the loss partials the same way.  Every
+// sum is in a fixed order: deterministic.
 constexpr int kRedThreads = 256;
-constexpr int kRedPer = 16;        // entries per thread: nsy * nsx <= 64 * 64 = 16 * 256
+constexpr int kRedStep = 32;       // slices whose loads are in flight together
+static_assert(kRedThreads % kRedStep == 0, "batches tile the shared IDD column");
+
+__device__ __forceinline__ double block_sum_fixed(double v, double* red) {
+    const int tid = threadIdx.x;
+    red[tid] = v;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (tid < w) red[tid] += red[tid + w];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
 
 __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
-    const JobDev* __restrict__ jobs, int with_range, int finalize_loss, const int* __restrict__ err,
-    int* layer_counts, int layer_stride) {
+    const JobDev* __restrict__ jobs, int with_range, int finalize_loss, const int* __restrict__ err) {
     // a programmatic dependent of the adjoint kernel: wait for its slots (no-op otherwise)
     asm volatile("griddepcontrol.wait;" ::: "memory");
     const JobDev& J = jobs[blockIdx.z];
-    int* layer_count = layer_counts + (size_t)blockIdx.z * layer_stride;   // this job's counters
-    const int seg = blockIdx.x, l = blockIdx.y;
+    const int ec = blockIdx.x, l = blockIdx.y;
     if (l >= J.nl) return;
     const int nz = J.nz, nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;
-    const int nseg = (nz + kRedZ - 1) / kRedZ;
-    if (seg >= nseg) return;
-    const size_t plane = (size_t)J.nl * nz * per;
-    float* part = J.partial + 2 * plane;           // (nl, nseg, per) segment partials
+    if (ec * kRedThreads >= per) return;
+    const int tid = threadIdx.x;
+    const int e = ec * kRedThreads + tid;
+    const bool own = e < per;
+    const size_t ndots = (size_t)J.nl * nz * kMathWarps;
+    const float* slots = J.partial + (size_t)l * nz * per;           // (nz, per) of layer l
+    const float* dots = J.partial + (size_t)J.nl * nz * per;          // (2, nl, nz, kMathWarps)
     const double* idd = J.idd + (size_t)l * nz;
-    const float* wl = J.w + (size_t)l * per;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    __shared__ float sdc[kRedZ][kRedThreads / 32], sds[kRedZ][kRedThreads / 32];
-    __shared__ int s_last;
-
-    float wv[kRedPer], acc[kRedPer];
-#pragma unroll
-    for (int k = 0; k < kRedPer; ++k) {
-        const int e = tid + k * kRedThreads;   // slot entry e = i * nsy + j
-        wv[k] = e < per ? wl[(size_t)(e % nsy) * nsx + e / nsy] : 0.f;
-        acc[k] = 0.f;
-    }
-    const int z0 = seg * kRedZ, z1 = min(nz, z0 + kRedZ);
-    // two slices per iteration, so that both slices' loads are in flight together
-    for (int z = z0; z < z1; z += 2) {
-        float pd[2] = {0.f, 0.f}, ps[2] = {0.f, 0.f};
-        float pv[2][kRedPer], qv[2][kRedPer], cf[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const double c = z + h < z1 ? idd[z + h] : 0.0;
-            const bool act = c != 0.0;
-            cf[h] = (float)c;
-            const float* pz = J.partial + ((size_t)l * nz + (act ? z + h : z)) * per;
-#pragma unroll
-            for (int k = 0; k < kRedPer; ++k) {
-                const int e = tid + k * kRedThreads;
-                const bool in = act && e < per;
-                pv[h][k] = in ? pz[e] : 0.f;
-                qv[h][k] = in ? pz[plane + e] : 0.f;
-            }
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-#pragma unroll
-            for (int k = 0; k < kRedPer; ++k) {
-                acc[k] = fmaf(cf[h], pv[h][k], acc[k]);
-                pd[h] = fmaf(pv[h][k], wv[k], pd[h]);
-                ps[h] = fmaf(qv[h][k], wv[k], ps[h]);
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                pd[h] += __shfl_xor_sync(0xffffffffu, pd[h], o);
-                ps[h] += __shfl_xor_sync(0xffffffffu, ps[h], o);
-            }
-        }
-        if (lane == 0) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-                if (z + h < z1) { sdc[z + h - z0][warp] = pd[h]; sds[z + h - z0][warp] = ps[h]; }
-        }
-    }
-    __syncthreads();
-    if (tid < z1 - z0) {
-        const int z = z0 + tid;
-        const double c = idd[z];
-        if (c != 0.0) {
-            float a = 0.f, b = 0.f;
-            for (int w = 0; w < kRedThreads / 32; ++w) { a += sdc[tid][w]; b += sds[tid][w]; }
-            J.dc[(size_t)l * nz + z] = a;
-            J.dsg[(size_t)l * nz + z] = (float)c * b;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < kRedPer; ++k) {
-        const int e = tid + k * kRedThreads;
-        if (e < per) part[((size_t)l * nseg + seg) * per + e] = acc[k];
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = atomicAdd(&layer_count[l], 1) == nseg - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
     const bool bad = *err != 0 || (J.fwd_err != nullptr && *J.fwd_err != 0);
     const float nan = __int_as_float(0x7fc00000);
-    {
-        // segment partials summed in segment order; every entry's load of a segment is
-        // issued together (segments unrolled by 4) so that many loads are in flight
-        float g[kRedPer];
+
+    // the layer's IDD column, kRedThreads slices at a time, in shared memory: each batch of
+    // slot loads then depends on nothing in flight.  A slice whose IDD rounds to 0 in FP32
+    // adds 0 (and its slot is not read); every slice read has IDD != 0, so the adjoint wrote it.
+    __shared__ float s_c[kRedThreads];
+    float acc = 0.f;
+    for (int zt = 0; zt < nz; zt += kRedThreads) {
+        const int zn = min(kRedThreads, nz - zt);
+        __syncthreads();   // the previous tile's reads of s_c are done
+        s_c[tid] = tid < zn ? (float)idd[zt + tid] : 0.f;
+        __syncthreads();
+        const float* sz = slots + (size_t)zt * per + e;
+        for (int z0 = 0; z0 < zn; z0 += kRedStep) {
+            float pv[kRedStep], cf[kRedStep];
 #pragma unroll
-        for (int k = 0; k < kRedPer; ++k) g[k] = 0.f;
-        const float* pl = part + (size_t)l * nseg * per;
-#pragma unroll 4
-        for (int sgi = 0; sgi < nseg; ++sgi) {
-#pragma unroll
-            for (int k = 0; k < kRedPer; ++k) {
-                const int e = tid + k * kRedThreads;
-                if (e < per) g[k] += __ldcg(pl + (size_t)sgi * per + e);
+            for (int h = 0; h < kRedStep; ++h) {
+                cf[h] = s_c[z0 + h];          // z0 + h < kRedThreads (kRedStep divides it)
+                pv[h] = (own && cf[h] != 0.f) ? sz[(size_t)(z0 + h) * per] : 0.f;
             }
-        }
 #pragma unroll
-        for (int k = 0; k < kRedPer; ++k) {
-            const int e = tid + k * kRedThreads;
-            if (e < per) J.grad_w[(size_t)l * per + (size_t)(e % nsy) * nsx + e / nsy] = bad ? nan : g[k];
+            for (int h = 0; h < kRedStep; ++h) acc = fmaf(cf[h], pv[h], acc);
         }
+    }
+    if (own) J.grad_w[(size_t)l * per + (size_t)(e % nsy) * nsx + e / nsy] = bad ? nan : acc;
+    if (ec != 0) return;
+
+    __shared__ double red[kRedThreads];
+    double a = 0.0;
+    for (int z = tid; z < nz; z += kRedThreads) {
+        const double c = idd[z];
+        if (c == 0.0) continue;
+        const size_t o = (size_t)l * nz + z;
+        const float* pa = dots + o * kMathWarps;
+        const float* pb = pa + ndots;
+        float sa = 0.f, sb = 0.f;
+#pragma unroll
+        for (int w = 0; w < kMathWarps; ++w) { sa += pa[w]; sb += pb[w]; }
+        const float dsg = (float)c * sb;
+        J.dc[o] = sa;
+        J.dsg[o] = dsg;
+        if (with_range) a += (double)sa * J.didd_dr[o] + (double)dsg * J.dsig_dr[o];
     }
     if (with_range) {
-        __shared__ double redd[kRedThreads];
-        double a = 0.0;
-        for (int z = tid; z < nz; z += kRedThreads) {
-            const size_t o = (size_t)l * nz + z;
-            if (idd[z] != 0.0)
-                a += (double)__ldcg(J.dc + o) * J.didd_dr[o] + (double)__ldcg(J.dsg + o) * J.dsig_dr[o];
-        }
-        redd[tid] = a;
-        __syncthreads();
-        for (int w = kRedThreads / 2; w > 0; w >>= 1) {
-            if (tid < w) redd[tid] += redd[tid + w];
-            __syncthreads();
-        }
-        if (tid == 0) J.grad_range[l] = bad ? nan : (float)redd[0];
+        const double r = block_sum_fixed(a, red);
+        if (tid == 0) J.grad_range[l] = bad ? nan : (float)r;
     }
-    if (finalize_loss && l == 0 && tid == 0) {
-        double sum = 0.0;
-        for (int b = 0; b < J.n_loss_part; ++b) sum += J.loss_part[b];
-        *J.loss = bad ? (double)nan : sum;
+    if (finalize_loss && l == 0) {
+        double t = 0.0;
+        for (int b = tid; b < J.n_loss_part; b += kRedThreads) t += J.loss_part[b];
+        const double sum = block_sum_fixed(t, red);
+        if (tid == 0) *J.loss = bad ? (double)nan : sum;
     }
 }
 
@@ -813,13 +783,15 @@ int tc_adjoint_dims(int precision, const pbd_field* f, int* N1) {
 }
 
 size_t tc_adjoint_counter_ints(int n_jobs, int max_layers) {
-    return 2u + (size_t)n_jobs * (size_t)max_layers;
+    (void)n_jobs;
+    (void)max_layers;
+    return 2u;
 }
 
 size_t tc_adjoint_slot_elems(const pbd_field* f) {
     const size_t per = (size_t)f->n_sy * f->n_sx;
-    const size_t nseg = ((size_t)f->nz + kRedZ - 1) / kRedZ;
-    return 2u * (size_t)f->n_layers * f->nz * per + (size_t)f->n_layers * nseg * per;
+    const size_t pairs = (size_t)f->n_layers * f->nz;
+    return pairs * per + 2u * pairs * kMathWarps;
 }
 
 int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs,
@@ -865,10 +837,10 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     if (precision == PBD_PREC_BF16) rc = launch_mode<PBD_PREC_BF16>(P, s);
     else rc = launch_mode<PBD_PREC_BF16X3>(P, s);
     PBD_TRY(rc);
-    (void)max_per;
-    PBD_TRY(launch_dependent(adj_tc_reduce_kernel, dim3((nzm + kRedZ - 1) / kRedZ, max_l, n_jobs),
+    PBD_TRY(launch_dependent(adj_tc_reduce_kernel,
+                             dim3((max_per + kRedThreads - 1) / kRedThreads, max_l, n_jobs),
                              dim3(kRedThreads), 0, s, (const JobDev*)jobs_dev, with_range,
-                             finalize_loss, (const int*)err, counter + 2, max_l));
+                             finalize_loss, (const int*)err));
     count_launch(2);
     return PBD_OK;
 }

@@ -182,14 +182,13 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
 
 // adjoint (tcgen05) -- adj_tc.cu.  Units (slice, chunk of `chunk` active layers) are
-// pulled z-major; `partial` holds two (layer, slice) slot planes of nsy * nsx floats and
-// the reduction's segment partials (tc_adjoint_slot_elems); counter[0] = unit counter,
-// counter[1] unused, then per job max_layers per-layer arrival counters; `err` = the error
-// word (cleared by the caller).
+// pulled z-major; `partial` holds one (layer, slice) slot plane of nsy * nsx floats and the
+// warps' dot-product partials of every pair (tc_adjoint_slot_elems); counter[0] = unit
+// counter, counter[1] unused; `err` = the error word (cleared by the caller).
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
 size_t tc_adjoint_slot_elems(const pbd_field* f);
-// Ints of the adjoint's counter block: unit counter, error word, then per job one arrival
-// counter per layer (max_layers of them).
+// Ints of the adjoint's counter block (the unit counter and one unused word, for any number of
+// jobs and layers).
 size_t tc_adjoint_counter_ints(int n_jobs, int max_layers);
 // counters_zeroed: the caller cleared the counter block earlier on the stream (so that no
 // memset sits between the forward and this launch, which runs as its programmatic dependent).
