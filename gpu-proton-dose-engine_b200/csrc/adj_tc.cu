@@ -91,6 +91,8 @@ struct Params {
     int stage;           // 1: each unit's dL/dD slice arrives by bulk copy into a staging buffer
                          //    (every job's slice is contiguous, 16-byte aligned, nx ny % 4 == 0)
     uint32_t o_stage;    // its shared-memory offset
+    int sym;             // 1: every job is symmetric in x and y (grid, lattice, origins), so the
+                         //    stage-2 operand [Gx | Gx'] equals the [Gy | Gy'] rows G evaluates
 };
 
 struct Layout {
@@ -304,28 +306,30 @@ __device__ __forceinline__ void mma_warp(const Params& P, const Layout& L, uint3
 
 // ------------------------------------------------------------------------------------------
 // DR: a pair's Q (TMEM columns from tq: Q[., i] at i, Q[., i'] at N1 + i) -> the pair's P slot
-// and this warp's share of the pair's two dot products.  P = Q[j, i] / (2 pi s^2) is stored
-// transposed ([i][j]) so that the j lanes of a warp write 64 contiguous bytes.  The warps of a
-// lane quadrant split the i columns in chunks of 16 (tcgen05.ld is warp-collective); the j'
-// lane hands Q[j', i] to its j lane by shuffle, so each j lane also holds
-// S[j, i] = (Q[j, i'] + Q[j', i]) / (2 pi s^2) and forms <P, W> and <S, W> over its entries.
-// A butterfly over the warp gives the warp's partial sums, stored per (pair, warp); the
-// follow-up kernel adds the eight warps' partials in warp order.  Padding rows (j >= nsy) hold
-// products of unset TMEM rows and are never read into a sum.
+// and this warp's share of the pair's two dot products.
+//  * Slot layout: P[j][i] = Q[j, i] / (2 pi s^2), rows of n1 = nsx rounded up to 16 floats
+//    (columns i >= nsx hold 0), so that a j lane writes its 8 columns as two 16-byte stores.
+//  * A thread's columns: 8-column chunks c0 = 8 half + 16 t, so that both halves of a lane
+//    quadrant drain the same number of chunks.
+//  * <P, W> is summed by the j lanes; <S, W>, S = (Q[j, i'] + Q[j', i]) / (2 pi s^2), by the
+//    j lane (Q[j, i'] W[j, i]) and the j' lane (Q[j', i] W[j, i]) together, and a butterfly
+//    over the warp adds all of them; the follow-up kernel adds the eight warps' partials in
+//    warp order.  Padding rows (j >= nsy) and columns (i >= nsx) hold products of unset
+//    operand rows and are never read into a sum.
 // ------------------------------------------------------------------------------------------
-// This thread's W entries for pr's DR: W_l[j, i] for its two 16-column chunks (zero where it
-// owns no entry).  Loaded a phase ahead of the DR, so that the load latency is hidden.
+// This thread's W entries for pr's DR (W_l[j, c0 + q], zero where it owns no entry).  Loaded a
+// phase ahead of the DR, so that the load latency is hidden.
 __device__ __forceinline__ void load_w_rows(const Params& P, const Step& pr, int half, int jrow,
-                                            bool deriv, float (&wv)[2][16]) {
+                                            float (&wv)[4][8]) {
     const JobDev& Jp = P.jobs[pr.job];
     const int pnsx = Jp.nsx, pnsy = Jp.nsy;
-    const bool row_ok = !deriv && jrow < pnsy;
+    const bool row_ok = jrow < pnsy;
     const float* wrow = Jp.w + (size_t)pr.l * pnsy * pnsx + (size_t)(row_ok ? jrow : 0) * pnsx;
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-        const int c0 = 16 * half + 32 * t;
+    for (int t = 0; t < 4; ++t) {
+        const int c0 = 8 * half + 16 * t;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
+        for (int q = 0; q < 8; ++q) {
             const int i = c0 + q;
             wv[t][q] = (row_ok && i < pnsx) ? __ldg(wrow + i) : 0.f;
         }
@@ -334,33 +338,39 @@ __device__ __forceinline__ void load_w_rows(const Params& P, const Step& pr, int
 
 __device__ __forceinline__ void drain_q(const Params& P, const Step& pr, uint32_t tq, int half,
                                         int jrow, bool deriv, int warp, int lane,
-                                        const float (&wv)[2][16]) {
+                                        const float (&wv)[4][8]) {
     const JobDev& Jp = P.jobs[pr.job];
     const int pnsx = Jp.nsx, pnsy = Jp.nsy, nz = Jp.nz, N1 = P.N1;
-    const size_t per = (size_t)pnsy * pnsx;
+    const int n1 = (pnsx + 15) / 16 * 16;
+    const size_t per = (size_t)pnsy * n1;
     const size_t pair = (size_t)pr.l * nz + pr.z;
-    float* slot_p = Jp.partial + pair * per;
-    const bool row_ok = !deriv && jrow < pnsy;
+    const bool row_ok = jrow < pnsy;
+    float* slot_row = Jp.partial + pair * per + (size_t)(row_ok ? jrow : 0) * n1;
     float dp = 0.f, ds = 0.f;
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-        const int c0 = 16 * half + 32 * t;   // N1 <= 64: at most two chunks per thread
-        if (c0 >= N1) break;
-        uint32_t ri[16], rd[16];
-        tc::tmem_ld16(tq + (uint32_t)c0, ri);
-        tc::tmem_ld16(tq + (uint32_t)(N1 + c0), rd);
+    for (int t = 0; t < 4; ++t) {
+        const int c0 = 8 * half + 16 * t;
+        if (c0 >= n1) break;
+        uint32_t ri[8], rd[8];
+        tc::tmem_ld8(tq + (uint32_t)c0, ri);
+        tc::tmem_ld8(tq + (uint32_t)(N1 + c0), rd);
         tc::tmem_wait_ld();
+        float pv[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int i = c0 + q;
-            const float vi = pr.nrm * __uint_as_float(ri[q]);   // Q[j, i] or Q[j', i]
-            const float vd = pr.nrm * __uint_as_float(rd[q]);   // Q[j, i']
-            const float b = __shfl_xor_sync(0xffffffffu, vi, 1);  // j lane: Q[j', i]
-            if (row_ok && i < pnsx) {
-                slot_p[(size_t)i * pnsy + jrow] = vi;
-                dp = fmaf(vi, wv[t][q], dp);
-                ds = fmaf(vd + b, wv[t][q], ds);
+        for (int q = 0; q < 8; ++q) {
+            const bool in = row_ok && c0 + q < pnsx;
+            const float vi = __uint_as_float(ri[q]);   // Q[j, i] (j lane) or Q[j', i] (j' lane)
+            const float vd = __uint_as_float(rd[q]);   // Q[j, i'] (j lane)
+            if (in) {
+                if (!deriv) dp = fmaf(vi, wv[t][q], dp);
+                ds = fmaf(deriv ? vi : vd, wv[t][q], ds);
             }
+            pv[q] = in ? pr.nrm * vi : 0.f;
+        }
+        if (!deriv && row_ok) {
+            float4* o = reinterpret_cast<float4*>(slot_row + c0);
+            o[0] = make_float4(pv[0], pv[1], pv[2], pv[3]);
+            o[1] = make_float4(pv[4], pv[5], pv[6], pv[7]);
         }
     }
 #pragma unroll
@@ -370,8 +380,27 @@ __device__ __forceinline__ void drain_q(const Params& P, const Step& pr, uint32_
     }
     if (lane == 0) {
         float* dots = Jp.partial + (size_t)Jp.nl * nz * per;   // (2, nl, nz, kMathWarps)
-        dots[pair * kMathWarps + warp] = dp;
-        dots[((size_t)Jp.nl * nz + pair) * kMathWarps + warp] = ds;
+        dots[pair * kMathWarps + warp] = pr.nrm * dp;
+        dots[((size_t)Jp.nl * nz + pair) * kMathWarps + warp] = pr.nrm * ds;
+    }
+}
+
+// Symmetric fields: this lane's G row (row j of Gy, or of Gy' on the j' lane; K columns
+// [64 half, +64) as packed bf16 pairs) stored as B2 row j (or N1 + j), K chunks 8 half + cc.
+template <int NARR>
+__device__ __forceinline__ void store_b2_sym(uint8_t* smem, const Layout& L, int N1, int half,
+                                             int jrow, bool deriv, const uint32_t (&hi)[2][16],
+                                             const uint32_t (&lo)[2][16]) {
+    const uint32_t planeR2 = (uint32_t)(2 * N1) * 16u;
+    const uint32_t row = (uint32_t)(deriv ? N1 + jrow : jrow);
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) {
+        const uint32_t off = L.b2 + (uint32_t)(8 * half + cc) * planeR2 + row * 16u;
+        const int a = cc >> 2, w = 4 * (cc & 3);
+        *reinterpret_cast<uint4*>(smem + off) = make_uint4(hi[a][w], hi[a][w + 1], hi[a][w + 2], hi[a][w + 3]);
+        if (NARR == 2)
+            *reinterpret_cast<uint4*>(smem + off + L.b2_lo) =
+                make_uint4(lo[a][w], lo[a][w + 1], lo[a][w + 2], lo[a][w + 3]);
     }
 }
 
@@ -416,8 +445,8 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         if (!__all_sync(0xffffffffu, ok)) break;
         if (cur.flags & kEnd) break;
         // W of the pair this iteration drains, in flight while G runs
-        float wpre[2][16];
-        if (have_prev) load_w_rows(P, prev, half, jrow, deriv, wpre);
+        float wpre[4][8];
+        if (have_prev) load_w_rows(P, prev, half, jrow, wpre);
         const JobDev& J = P.jobs[cur.job];
         const int nx = J.nx, ny = J.ny, nsx = J.nsx, nsy = J.nsy;
         const int b = n & 1;
@@ -465,11 +494,11 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         // a warp whose 32 TMEM rows are all padding (m >= 2 nsy) skips G and E1: those rows of
         // every product only ever feed rows of Q that are never read
         const bool pad_warp = 32 * sp >= 2 * nsy;
+        uint32_t hi[2][16], lo[2][16];   // this lane's G row, kept for B2 on symmetric fields
         if (!pad_warp) {
             const float dyf = (float)J.dy;
             const bool valid = jrow < nsy;
             const float cself = deriv ? 32.f : 0.f;   // first column of this lane's exponentials
-            uint32_t hi[2][16], lo[2][16];
 #pragma unroll
             for (int kp = 0; kp < 16; ++kp) {
                 float vl[2], vh[2];                     // columns 2 kp + t and 32 + 2 kp + t
@@ -508,12 +537,16 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
             if (ok) ph2 ^= 1;
             if (!__all_sync(0xffffffffu, ok)) break;
             tc::fence_after_sync();
-            drain_q(P, prev, tb + lane_base + kColQ, half, jrow, deriv, warp, lane, wpre);
         }
+        // symmetric fields: B2 = the G rows just evaluated.  Stage 2 of the previous pair, the
+        // only reader of B2, is complete (waited for above, or there is none).  Pad warps hold
+        // only rows j >= N1, which B2 does not have.
+        if (P.sym && !pad_warp && jrow < N1) store_b2_sym<NARR>(smem, L, N1, half, jrow, deriv, hi, lo);
+        if (have_prev) drain_q(P, prev, tb + lane_base + kColQ, half, jrow, deriv, warp, lane, wpre);
 
         // ---- B2 = [Gx | Gx'] -> smem (rows i and N1 + i, K = x).  Only stage 2 reads it,
         // and the previous pair's stage 2 is complete (DR waited), so one buffer serves. ----
-        {
+        if (!P.sym) {
             const uint32_t ob2 = L.b2;
             const double cx = 0.5 * (double)(nsx - 1);
             const float dxf = (float)J.dx;
@@ -582,8 +615,8 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
         ok = wait_bar(mma2, ph2, P.wait_ns);
         if (__all_sync(0xffffffffu, ok)) {
             tc::fence_after_sync();
-            float wl[2][16];
-            load_w_rows(P, prev, half, jrow, deriv, wl);
+            float wl[4][8];
+            load_w_rows(P, prev, half, jrow, wl);
             drain_q(P, prev, tb + lane_base + kColQ, half, jrow, deriv, warp, lane, wl);
         }
     }
@@ -650,8 +683,9 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
 
 // After the main kernel: dL/dW, the per-pair dot products and dL/dR from the slots, with no
 // block waiting on another.  Block (entry chunk, layer l, job): each thread owns one slot
-// entry e = i * nsy + j of layer l and accumulates IDD * P slot over the layer's active slices
-// in slice order (kRedStep slices' loads in flight together), then writes dL/dW[l, j, i].
+// entry e = j * n1 + i of layer l (n1 = nsx rounded up to 16) and accumulates IDD * P slot
+// over the layer's active slices in slice order (kRedStep slices' loads in flight together),
+// then writes dL/dW[l, j, i] for i < nsx.
 // Chunk 0 of every layer also adds, per active slice, the eight warp partials of <P, W>
 // (dL/dIDD) and <S, W> (dL/dsigma, times IDD) in warp order and forms dL/dR_l in FP64 (a
 // fixed tree over the block); chunk 0 of layer 0 sums the loss partials the same way.  Every
@@ -680,11 +714,13 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     const JobDev& J = jobs[blockIdx.z];
     const int ec = blockIdx.x, l = blockIdx.y;
     if (l >= J.nl) return;
-    const int nz = J.nz, nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;
+    const int nz = J.nz, nsx = J.nsx, nsy = J.nsy;
+    const int n1 = (nsx + 15) / 16 * 16, per = nsy * n1;
     if (ec * kRedThreads >= per) return;
     const int tid = threadIdx.x;
     const int e = ec * kRedThreads + tid;
-    const bool own = e < per;
+    const int ej = e / n1, ei = e - ej * n1;
+    const bool own = e < per && ei < nsx;
     const size_t ndots = (size_t)J.nl * nz * kMathWarps;
     const float* slots = J.partial + (size_t)l * nz * per;           // (nz, per) of layer l
     const float* dots = J.partial + (size_t)J.nl * nz * per;          // (2, nl, nz, kMathWarps)
@@ -714,7 +750,7 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
             for (int h = 0; h < kRedStep; ++h) acc = fmaf(cf[h], pv[h], acc);
         }
     }
-    if (own) J.grad_w[(size_t)l * per + (size_t)(e % nsy) * nsx + e / nsy] = bad ? nan : acc;
+    if (own) J.grad_w[((size_t)l * nsy + ej) * nsx + ei] = bad ? nan : acc;
     if (ec != 0) return;
 
     __shared__ double red[kRedThreads];
@@ -789,7 +825,8 @@ size_t tc_adjoint_counter_ints(int n_jobs, int max_layers) {
 }
 
 size_t tc_adjoint_slot_elems(const pbd_field* f) {
-    const size_t per = (size_t)f->n_sy * f->n_sx;
+    // slot rows of nsx rounded up to 16 floats: every job's slots start on a 64-byte boundary
+    const size_t per = (size_t)f->n_sy * (size_t)((f->n_sx + 15) / 16 * 16);
     const size_t pairs = (size_t)f->n_layers * f->nz;
     return pairs * per + 2u * pairs * kMathWarps;
 }
@@ -824,9 +861,16 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
         cm = std::max(cm, (jobs_host[j].nl + chunk - 1) / chunk);
         nzm = std::max(nzm, jobs_host[j].nz);
         max_l = std::max(max_l, jobs_host[j].nl);
-        max_per = std::max(max_per, jobs_host[j].nsy * jobs_host[j].nsx);
+        max_per = std::max(max_per, jobs_host[j].nsy * ((jobs_host[j].nsx + 15) / 16 * 16));
     }
     P.cmax = cm;
+    P.sym = 1;
+    for (int j = 0; j < n_jobs; ++j) {
+        const JobDev& J = jobs_host[j];
+        if (!(J.nx == J.ny && J.ox == J.oy && J.dx == J.dy && J.nsx == J.nsy && J.sx0 == J.sy0 &&
+              J.dsx == J.dsy))
+            P.sym = 0;
+    }
     const long long units = (long long)nzm * cm * n_jobs;
     if (units > (1LL << 30)) return PBD_ERR_UNSUPPORTED;
     P.n_units = (int)units;
