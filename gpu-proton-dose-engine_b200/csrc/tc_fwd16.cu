@@ -148,6 +148,9 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
 __global__ void __launch_bounds__(256) pack_w16_kernel(const JobDev* __restrict__ jobs, int K1,
                                                        int N1, int lmax, uint32_t img,
                                                        uint8_t* wpack, float* wmax, int* wexp) {
+    // the dose kernel (a programmatic dependent) may start its prologue now; it reads the packed
+    // maps only after griddepcontrol.wait, i.e. after this grid has completed
+    asm volatile("griddepcontrol.launch_dependents;");
     const JobDev& J = jobs[blockIdx.y];
     const int l = blockIdx.x;
     if (l >= J.nl) return;
@@ -307,7 +310,9 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
                 continue;
             }
             if (c >= nch) continue;
-            const int r0 = c * P.chunk, r1 = min(tot, r0 + P.chunk);
+            // nch pieces of equal size (within one layer) rather than chunk-sized ones and a
+            // remainder: the largest unit, which bounds the balance, is as small as nch allows
+            const int r0 = (int)((long long)c * tot / nch), r1 = (int)((long long)(c + 1) * tot / nch);
             // the unit's scale exponent: the smallest over its layers of
             // 14 - ceil(log2(bound on |s U|)), so that every s U of the unit fits FP16
             int ks = 127;
