@@ -347,30 +347,35 @@ __device__ __forceinline__ void drain_q(const Params& P, const Step& pr, uint32_
     const bool row_ok = jrow < pnsy;
     float* slot_row = Jp.partial + pair * per + (size_t)(row_ok ? jrow : 0) * n1;
     float dp = 0.f, ds = 0.f;
+    // a warp whose 32 rows are all padding (its first row 16 sp >= nsy) owns no entry: it skips
+    // the TMEM loads and stores zero partials
+    const bool pad = __shfl_sync(0xffffffffu, jrow, 0) >= pnsy;
+    if (!pad) {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int c0 = 8 * half + 16 * t;
-        if (c0 >= n1) break;
-        uint32_t ri[8], rd[8];
-        tc::tmem_ld8(tq + (uint32_t)c0, ri);
-        tc::tmem_ld8(tq + (uint32_t)(N1 + c0), rd);
-        tc::tmem_wait_ld();
-        float pv[8];
+        for (int t = 0; t < 4; ++t) {
+            const int c0 = 8 * half + 16 * t;
+            if (c0 >= n1) break;
+            uint32_t ri[8], rd[8];
+            tc::tmem_ld8(tq + (uint32_t)c0, ri);
+            tc::tmem_ld8(tq + (uint32_t)(N1 + c0), rd);
+            tc::tmem_wait_ld();
+            float pv[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const bool in = row_ok && c0 + q < pnsx;
-            const float vi = __uint_as_float(ri[q]);   // Q[j, i] (j lane) or Q[j', i] (j' lane)
-            const float vd = __uint_as_float(rd[q]);   // Q[j, i'] (j lane)
-            if (in) {
-                if (!deriv) dp = fmaf(vi, wv[t][q], dp);
-                ds = fmaf(deriv ? vi : vd, wv[t][q], ds);
+            for (int q = 0; q < 8; ++q) {
+                const bool in = row_ok && c0 + q < pnsx;
+                const float vi = __uint_as_float(ri[q]);   // Q[j, i] (j lane) or Q[j', i] (j' lane)
+                const float vd = __uint_as_float(rd[q]);   // Q[j, i'] (j lane)
+                if (in) {
+                    if (!deriv) dp = fmaf(vi, wv[t][q], dp);
+                    ds = fmaf(deriv ? vi : vd, wv[t][q], ds);
+                }
+                pv[q] = in ? pr.nrm * vi : 0.f;
             }
-            pv[q] = in ? pr.nrm * vi : 0.f;
-        }
-        if (!deriv && row_ok) {
-            float4* o = reinterpret_cast<float4*>(slot_row + c0);
-            o[0] = make_float4(pv[0], pv[1], pv[2], pv[3]);
-            o[1] = make_float4(pv[4], pv[5], pv[6], pv[7]);
+            if (!deriv && row_ok) {
+                float4* o = reinterpret_cast<float4*>(slot_row + c0);
+                o[0] = make_float4(pv[0], pv[1], pv[2], pv[3]);
+                o[1] = make_float4(pv[4], pv[5], pv[6], pv[7]);
+            }
         }
     }
 #pragma unroll
@@ -659,6 +664,9 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     // forward's last CTAs; nothing below runs before the forward has completed (no-op when
     // there is no such predecessor).
     asm volatile("griddepcontrol.wait;" ::: "memory");
+    // the reduce (a programmatic dependent) may be scheduled onto the SMs this grid frees; one
+    // CTA per SM here, so it takes no SM that a CTA of this grid still needs
+    asm volatile("griddepcontrol.launch_dependents;");
 
     if (warp >= kMathWarps) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));

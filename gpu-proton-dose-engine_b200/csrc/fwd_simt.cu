@@ -293,10 +293,12 @@ int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdIte
                    int with_loss, int precision, int poison, void* pack, size_t pack_bytes,
                    cudaStream_t s) {
     if (precision != PBD_PREC_FP32) {
-        PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, n_counter_ints * sizeof(int), s)));
+        // the split-FP16 path clears its unit counter in its pack kernel (no memset node between
+        // the job install and the dose kernels)
         if (precision == PBD_PREC_FP16X3 && jobs_host[0].layer_stride == 0)
             return launch_forward_tc16(jobs_dev, jobs_host, n_jobs, counter, err, chunk,
                                        with_loss, poison, pack, pack_bytes, s);
+        PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, n_counter_ints * sizeof(int), s)));
         return launch_forward_tc(precision, jobs_dev, jobs_host, n_jobs, counter, err, chunk,
                                  with_loss, poison, s);
     }

@@ -147,10 +147,14 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) pack_w16_kernel(const JobDev* __restrict__ jobs, int K1,
                                                        int N1, int lmax, uint32_t img,
-                                                       uint8_t* wpack, float* wmax, int* wexp) {
+                                                       uint8_t* wpack, float* wmax, int* wexp,
+                                                       int* unit_counter) {
     // the dose kernel (a programmatic dependent) may start its prologue now; it reads the packed
-    // maps only after griddepcontrol.wait, i.e. after this grid has completed
+    // maps and the unit counter only after griddepcontrol.wait, i.e. after this grid has completed
     asm volatile("griddepcontrol.launch_dependents;");
+    // launched as a programmatic dependent of the job install: its job views are visible after this
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *unit_counter = 0;
     const JobDev& J = jobs[blockIdx.y];
     const int l = blockIdx.x;
     if (l >= J.nl) return;
@@ -828,6 +832,10 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc16_kernel(Params P) {
     // the spot maps are packed by the kernel before this one (a programmatic dependent launch:
     // everything above overlaps its end)
     asm volatile("griddepcontrol.wait;" ::: "memory");
+    // the finalize pass (a programmatic dependent) may be scheduled onto the SMs this grid frees;
+    // it reads the partial slices only after its griddepcontrol.wait.  One CTA per SM here, so an
+    // early dependent takes no SM that a CTA of this grid still needs.
+    asm volatile("griddepcontrol.launch_dependents;");
 
     if (warp >= kMathWarps) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
@@ -853,6 +861,8 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc16_kernel(Params P) {
 __global__ void __launch_bounds__(256) fwd16_finalize_kernel(const JobDev* __restrict__ jobs,
                                                              int with_loss,
                                                              const int* __restrict__ err) {
+    // a programmatic dependent of the dose kernel: its partial slices are visible after this
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const JobDev& J = jobs[blockIdx.y];
     const size_t plane = (size_t)J.nx * J.ny, n = plane * J.nz;
     const bool bad = *err != 0;
@@ -1018,9 +1028,9 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
     // >= 116 KiB: one CTA (and its 512 TMEM columns) per SM
     const size_t smem = std::max<size_t>(pl.total, 116u * 1024u);
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
-    pack_w16_kernel<<<dim3(lmax, n_jobs), 256, 0, s>>>(jobs_dev, P.K1, P.N1, lmax, P.img,
-                                                       const_cast<uint8_t*>(P.wpack), wmax, wexp);
-    PBD_LAUNCH_CHECK();
+    PBD_TRY(launch_dependent(pack_w16_kernel, dim3(lmax, n_jobs), dim3(256), 0, s,
+                             (const JobDev*)jobs_dev, P.K1, P.N1, lmax, P.img,
+                             const_cast<uint8_t*>(P.wpack), wmax, wexp, counter));
     const int grid = std::max(1, std::min(P.n_units, num_sms()));
     prof_mark(kProfFwd, 0, s);
     PBD_TRY(launch_dependent(fwd_tc16_kernel, dim3(grid), dim3(kThreads), smem, s, P));
@@ -1034,9 +1044,8 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
         // kLossBlocks16 blocks with the loss (the adjoint sums that many partials per job)
         const int blocks = with_loss ? kLossBlocks16
                                      : (int)std::min<size_t>((maxn / 4 + 255) / 256, 4096);
-        fwd16_finalize_kernel<<<dim3(std::max(blocks, 1), n_jobs), 256, 0, s>>>(jobs_dev, with_loss,
-                                                                               err);
-        PBD_LAUNCH_CHECK();
+        PBD_TRY(launch_dependent(fwd16_finalize_kernel, dim3(std::max(blocks, 1), n_jobs), dim3(256),
+                                 0, s, (const JobDev*)jobs_dev, with_loss, (const int*)err));
         count_launch(1);
     } else if (poison) {
         fwd16_poison_kernel<<<num_sms(), 256, 0, s>>>(jobs_dev, n_jobs, err);
