@@ -6,6 +6,7 @@
 // per-call device state (job descriptors, schedules, partial sums) lives in the
 // caller's workspace and is written by kernels from launch parameters, so every call
 // can be captured into a CUDA graph.
+#include <algorithm>
 #include <math.h>
 #include <string.h>
 
@@ -1034,26 +1035,49 @@ int pbd_forward_wed_curves(const pbd_field* f, const pbd_lut_spec* spec, const v
 }
 
 // ---- heterogeneous media: dL/dW -----------------------------------------------------
+// Tensor-core precisions: one adjoint launch over L single-layer jobs (job l: layer l's weights,
+// widths and scaled dL/dD map, depth dose 1 on its active slices) -- the batched adjoint's
+// machinery, each job with its own slots.  FP32: one single-layer SIMT adjoint per layer.
 struct WedAdjCarve {
-    int* status;         // status header: the per-layer adjoints' error word
+    int* status;         // status header: the adjoint's error word
     double* act;         // (L, nz) activity table
     float* maps;         // (L, wed_lateral_stride) dL/dD times each layer's depth dose
-    void* adj;           // one single-layer adjoint's workspace, reused layer after layer
+    void* adj;           // FP32: one single-layer adjoint's workspace, reused layer after layer
     size_t adj_bytes;
+    JobDev *fwd, *jobs;  // tensor cores: the install kernel's (unused) forward views, the jobs
+    float *apart, *dcs, *dsgs;
+    int* acnt;           // the adjoint's unit counter block
+    size_t slot_elems;   // slots of one single-layer job
 };
 
 static int carve_wed_adj(const pbd_field* f, int precision, void* base, WedAdjCarve& w,
                          size_t* used) {
     pbd_field f1 = *f;
     f1.n_layers = 1;
-    size_t ab = 0;
-    PBD_TRY(pbd_adjoint_workspace(&f1, precision, &ab));
     Carve c(base);
     w.status = c.take<int>(kStatusInts);
     w.act = c.take<double>((size_t)f->n_layers * f->nz);
     w.maps = c.take<float>((size_t)f->n_layers * wed_lateral_stride(f));
-    w.adj = c.take<char>(ab);
-    w.adj_bytes = ab;
+    w.adj = nullptr; w.adj_bytes = 0;
+    w.fwd = w.jobs = nullptr; w.apart = w.dcs = w.dsgs = nullptr; w.acnt = nullptr;
+    w.slot_elems = 0;
+    if (precision == PBD_PREC_FP32) {
+        size_t ab = 0;
+        PBD_TRY(pbd_adjoint_workspace(&f1, precision, &ab));
+        w.adj = c.take<char>(ab);
+        w.adj_bytes = ab;
+    } else {
+        int n1 = 0;
+        PBD_TRY(tc_adjoint_dims(precision, &f1, &n1));
+        const size_t L = (size_t)f->n_layers;
+        w.slot_elems = tc_adjoint_slot_elems(&f1);
+        w.fwd = c.take<JobDev>(L);
+        w.jobs = c.take<JobDev>(L);
+        w.apart = c.take<float>(L * w.slot_elems);
+        w.dcs = c.take<float>(L * f->nz);
+        w.dsgs = c.take<float>(L * f->nz);
+        w.acnt = c.take<int>(tc_adjoint_counter_ints((int)L, 1));
+    }
     *used = c.used + 256;
     return PBD_OK;
 }
@@ -1089,17 +1113,62 @@ int pbd_adjoint_wed(const pbd_field* f, const pbd_lut_spec* spec, const void* cu
                              s));
     PBD_TRY(lut_wed_grad_maps(spec, f->n_layers, curves, curves_bytes, grad_dose, wed, nvox,
                               lstride, wc.maps, s));
-    PBD_TRY(cuda_rc(cudaMemsetAsync(wc.status, 0, kStatusInts * sizeof(int), s)));
     // layer l: the adjoint of its lateral map with depth dose 1 on its active slices
     pbd_field f1 = *f;
     f1.n_layers = 1;
     const size_t per = (size_t)f->n_sy * f->n_sx;
-    for (int l = 0; l < f->n_layers; ++l)
-        PBD_TRY(adjoint_one(&f1, w + (size_t)l * per, wc.act + (size_t)l * f->nz,
-                            sigma + (size_t)l * f->nz, nullptr, nullptr,
-                            wc.maps + (size_t)l * lstride, grad_w + (size_t)l * per, nullptr,
-                            precision, wc.adj, wc.adj_bytes, wc.status + kStatAdj, s));
-    return PBD_OK;
+    if (precision == PBD_PREC_FP32) {
+        PBD_TRY(cuda_rc(cudaMemsetAsync(wc.status, 0, kStatusInts * sizeof(int), s)));
+        for (int l = 0; l < f->n_layers; ++l)
+            PBD_TRY(adjoint_one(&f1, w + (size_t)l * per, wc.act + (size_t)l * f->nz,
+                                sigma + (size_t)l * f->nz, nullptr, nullptr,
+                                wc.maps + (size_t)l * lstride, grad_w + (size_t)l * per, nullptr,
+                                precision, wc.adj, wc.adj_bytes, wc.status + kStatAdj, s));
+        return PBD_OK;
+    }
+    // tensor cores: the L single-layer jobs installed kGradInstall at a time (the first group
+    // also clears the status header), then one adjoint launch and one reduce launch over them
+    std::vector<JobDev> views((size_t)f->n_layers);
+    GradBufs b{};
+    b.fwd = wc.fwd; b.adj = wc.jobs; b.fpart = nullptr; b.farr = nullptr; b.lpart = nullptr;
+    b.apart = wc.apart; b.dcs = wc.dcs; b.dsgs = wc.dsgs; b.fwd_err = nullptr;
+    b.status = wc.status;
+    JobDev base{};
+    fill_job(&f1, &base);
+    for (int g0 = 0; g0 < f->n_layers; g0 += kGradInstall) {
+        GradTable t;
+        memset(&t, 0, sizeof(t));
+        t.base = g0;
+        t.n = std::min(kGradInstall, f->n_layers - g0);
+        for (int k = 0; k < t.n; ++k) {
+            const int l = g0 + k;
+            GradLite& a = t.j[k];
+            a.nx = base.nx; a.ny = base.ny; a.nz = base.nz;
+            a.nsx = base.nsx; a.nsy = base.nsy; a.nl = 1;
+            a.max_chunks_f = 1; a.max_chunks_a = 1; a.direct = 0; a.n_loss_part = 0;
+            a.ox = base.ox; a.oy = base.oy; a.dx = base.dx; a.dy = base.dy;
+            a.sx0 = base.sx0; a.sy0 = base.sy0; a.dsx = base.dsx; a.dsy = base.dsy;
+            a.w = w + (size_t)l * per;
+            a.idd = wc.act + (size_t)l * f->nz;
+            a.sigma = sigma + (size_t)l * f->nz;
+            a.grad_dose = wc.maps + (size_t)l * lstride;
+            a.grad_w = grad_w + (size_t)l * per;
+            a.slot_off = (size_t)l * wc.slot_elems;
+            a.dcs_off = (size_t)l * f->nz;
+            JobDev& v = views[(size_t)l];
+            v = base;
+            v.nl = 1; v.max_chunks = 1;
+            v.w = a.w; v.idd = a.idd; v.sigma = a.sigma; v.grad_dose = a.grad_dose;
+            v.grad_w = a.grad_w;
+            v.partial = wc.apart + a.slot_off;
+            v.dc = wc.dcs + a.dcs_off; v.dsg = wc.dsgs + a.dcs_off;
+        }
+        install_grad_kernel<<<(std::max(t.n, kStatusInts) + 63) / 64, 64, 0, s>>>(t, b);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    }
+    return launch_adjoint_tc(precision, wc.jobs, views.data(), f->n_layers, wc.acnt,
+                             wc.status + kStatAdj, 1, 0, 0, 0, s);
 }
 
 int pbd_loss_grad_batch_workspace(const pbd_grad_job* jobs, int n_jobs, int precision,

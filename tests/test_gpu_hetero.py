@@ -192,7 +192,7 @@ def test_gradient_vs_oracle(pb):
                          sig, wed_np, grad.astype(np.float64))
     wed = pb.hetero.wed_raytrace(rho, g)
     pos = np.abs(grad) + 0.1
-    for prec in ("fp32", "tf32x3"):
+    for prec in ("fp32", "tf32x3", "fp16x3"):
         plan = pb.hetero.WedPlan(prob, precision=prec)
         got = plan.adjoint(torch.as_tensor(grad, device="cuda"), wed).cpu().numpy()
         err = rel(got, want)
