@@ -588,6 +588,8 @@ def hetero_bench(args):
                      ("wed_curves", curves),
                      ("heterogeneous_forward", lambda: plan.forward(wed, out=out)),
                      ("heterogeneous_adjoint", lambda: plan.adjoint(gdose, wed)),
+                     ("heterogeneous_adjoint_with_range",
+                      lambda: plan.adjoint(gdose, wed, with_range=True)),
                      ("homogeneous_forward", lambda: homog.forward(out=out_h))):
         trace()
         fn()

@@ -189,6 +189,12 @@ _SIGS = {
     "pbd_adjoint_wed": (c_int, [POINTER(Field), POINTER(LutSpec), c_void_p, c_size_t, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                                 c_size_t, c_void_p]),
+    "pbd_adjoint_wed_range_workspace": (c_int, [POINTER(Field), POINTER(LutSpec), c_int,
+                                                POINTER(c_size_t)]),
+    "pbd_adjoint_wed_range": (c_int, [POINTER(Field), POINTER(LutSpec), c_void_p, c_size_t,
+                                      c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p,
+                                      c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                                      c_size_t, c_void_p]),
     "pbd_adam_step": (c_int, [POINTER(AdamParams), c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "pbd_scenario_combine": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -762,6 +762,9 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     if (ec != 0) return;
 
     __shared__ double red[kRedThreads];
+    // per job: no dL/dR output, or a missing derivative table, contributes nothing (the
+    // heterogeneous range gradient's two job sets use one table each)
+    const bool rng = with_range && J.grad_range != nullptr;
     double a = 0.0;
     for (int z = tid; z < nz; z += kRedThreads) {
         const double c = idd[z];
@@ -775,9 +778,11 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
         const float dsg = (float)c * sb;
         J.dc[o] = sa;
         J.dsg[o] = dsg;
-        if (with_range) a += (double)sa * J.didd_dr[o] + (double)dsg * J.dsig_dr[o];
+        if (rng)
+            a += (J.didd_dr ? (double)sa * J.didd_dr[o] : 0.0) +
+                 (J.dsig_dr ? (double)dsg * J.dsig_dr[o] : 0.0);
     }
-    if (with_range) {
+    if (rng) {
         const double r = block_sum_fixed(a, red);
         if (tid == 0) J.grad_range[l] = bad ? nan : (float)r;
     }

@@ -1034,15 +1034,25 @@ int pbd_forward_wed_curves(const pbd_field* f, const pbd_lut_spec* spec, const v
                             stream);
 }
 
-// ---- heterogeneous media: dL/dW -----------------------------------------------------
-// Tensor-core precisions: one adjoint launch over L single-layer jobs (job l: layer l's weights,
-// widths and scaled dL/dD map, depth dose 1 on its active slices) -- the batched adjoint's
-// machinery, each job with its own slots.  FP32: one single-layer SIMT adjoint per layer.
+// ---- heterogeneous media: dL/dW and dL/dR -------------------------------------------
+// D = sum_l IDD_l(WED) Lat_l, Lat_l = Gy_l W_l Gx_l^T with water's widths at the geometric depth.
+//  * dL/dW_l = A_l^T (g IDD_l(WED)): the adjoint of layer l's map g IDD_l(WED) with depth dose 1
+//    on its active slices.
+//  * dL/dR_l = sum_v g dIDD_l/dR(WED) Lat_l + sum_z dL/dsigma_lz dsigma_lz/dR.  The first term is
+//    <A_l^T (g dIDD_l/dR(WED)), W_l> = sum_z <P_lz, W_l> of a second job set whose maps use the
+//    curves' central difference at range shifts +-h; the second is the first set's per-pair
+//    dL/dsigma dotted with dsigma/dR.
+// Tensor-core precisions: one adjoint launch over every job (set s, layer l), the batched
+// adjoint's machinery with single-layer jobs.  FP32: one SIMT adjoint per (set, layer).
 struct WedAdjCarve {
+    int sets;            // 1: dL/dW; 2: dL/dW and dL/dR
     int* status;         // status header: the adjoint's error word
-    double* act;         // (L, nz) activity table
-    float* maps;         // (L, wed_lateral_stride) dL/dD times each layer's depth dose
-    void* adj;           // FP32: one single-layer adjoint's workspace, reused layer after layer
+    double* act;         // (sets, L, nz) activity tables
+    float* maps;         // (sets, L, wed_lateral_stride) the jobs' dL/dD maps
+    double* zeros;       // FP32 with dL/dR: (L, nz) zero table
+    float* gw2;          // set 1's dL/dW (unused), (L, nsy, nsx)
+    float* r1;           // set 1's part of dL/dR, (L)
+    void* adj;           // FP32: one single-layer adjoint's workspace, reused job after job
     size_t adj_bytes;
     JobDev *fwd, *jobs;  // tensor cores: the install kernel's (unused) forward views, the jobs
     float *apart, *dcs, *dsgs;
@@ -1050,14 +1060,23 @@ struct WedAdjCarve {
     size_t slot_elems;   // slots of one single-layer job
 };
 
-static int carve_wed_adj(const pbd_field* f, int precision, void* base, WedAdjCarve& w,
+static int carve_wed_adj(const pbd_field* f, int precision, int sets, void* base, WedAdjCarve& w,
                          size_t* used) {
     pbd_field f1 = *f;
     f1.n_layers = 1;
+    const size_t L = (size_t)f->n_layers, per = (size_t)f->n_sy * f->n_sx;
+    const size_t nj = (size_t)sets * L;
     Carve c(base);
+    w.sets = sets;
     w.status = c.take<int>(kStatusInts);
-    w.act = c.take<double>((size_t)f->n_layers * f->nz);
-    w.maps = c.take<float>((size_t)f->n_layers * wed_lateral_stride(f));
+    w.act = c.take<double>(nj * f->nz);
+    w.maps = c.take<float>(nj * wed_lateral_stride(f));
+    w.zeros = nullptr; w.gw2 = nullptr; w.r1 = nullptr;
+    if (sets == 2) {
+        w.gw2 = c.take<float>(L * per);
+        w.r1 = c.take<float>(L);
+        if (precision == PBD_PREC_FP32) w.zeros = c.take<double>(L * f->nz);
+    }
     w.adj = nullptr; w.adj_bytes = 0;
     w.fwd = w.jobs = nullptr; w.apart = w.dcs = w.dsgs = nullptr; w.acnt = nullptr;
     w.slot_elems = 0;
@@ -1069,16 +1088,106 @@ static int carve_wed_adj(const pbd_field* f, int precision, void* base, WedAdjCa
     } else {
         int n1 = 0;
         PBD_TRY(tc_adjoint_dims(precision, &f1, &n1));
-        const size_t L = (size_t)f->n_layers;
         w.slot_elems = tc_adjoint_slot_elems(&f1);
-        w.fwd = c.take<JobDev>(L);
-        w.jobs = c.take<JobDev>(L);
-        w.apart = c.take<float>(L * w.slot_elems);
-        w.dcs = c.take<float>(L * f->nz);
-        w.dsgs = c.take<float>(L * f->nz);
-        w.acnt = c.take<int>(tc_adjoint_counter_ints((int)L, 1));
+        w.fwd = c.take<JobDev>(nj);
+        w.jobs = c.take<JobDev>(nj);
+        w.apart = c.take<float>(nj * w.slot_elems);
+        w.dcs = c.take<float>(nj * f->nz);
+        w.dsgs = c.take<float>(nj * f->nz);
+        w.acnt = c.take<int>(tc_adjoint_counter_ints((int)nj, 1));
     }
     *used = c.used + 256;
+    return PBD_OK;
+}
+
+__global__ void wed_range_combine_kernel(float* grad_range, const float* r1, int n) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < n) grad_range[l] += r1[l];
+}
+
+// The adjoints of the carve's job sets (maps and activity tables already written).
+static int wed_adjoint_jobs(const pbd_field* f, const WedAdjCarve& wc, const float* w,
+                            const double* sigma, const double* dsigma_dr, float* grad_w,
+                            float* grad_range, int precision, cudaStream_t s) {
+    pbd_field f1 = *f;
+    f1.n_layers = 1;
+    const int L = f->n_layers;
+    const size_t per = (size_t)f->n_sy * f->n_sx, lstride = wed_lateral_stride(f);
+    const size_t nzL = (size_t)L * f->nz;
+    const bool rng = wc.sets == 2;
+    if (precision == PBD_PREC_FP32) {
+        PBD_TRY(cuda_rc(cudaMemsetAsync(wc.status, 0, kStatusInts * sizeof(int), s)));
+        if (rng) PBD_TRY(cuda_rc(cudaMemsetAsync(wc.zeros, 0, nzL * sizeof(double), s)));
+        for (int st = 0; st < wc.sets; ++st)
+            for (int l = 0; l < L; ++l) {
+                const size_t lz = (size_t)l * f->nz;
+                const double* act = wc.act + (size_t)st * nzL + lz;
+                const double* didd = !rng ? nullptr : (st == 0 ? wc.zeros + lz : act);
+                const double* dsig = !rng ? nullptr : (st == 0 ? dsigma_dr + lz : wc.zeros + lz);
+                float* gw = (st == 0 ? grad_w : wc.gw2) + (size_t)l * per;
+                float* gr = !rng ? nullptr : (st == 0 ? grad_range : wc.r1) + l;
+                PBD_TRY(adjoint_one(&f1, w + (size_t)l * per, act, sigma + lz, didd, dsig,
+                                    wc.maps + ((size_t)st * L + l) * lstride, gw, gr, precision,
+                                    wc.adj, wc.adj_bytes, wc.status + kStatAdj, s));
+            }
+    } else {
+        // the jobs installed kGradInstall at a time (the first group also clears the status
+        // header), then one adjoint launch and one reduce launch over them
+        const int nj = wc.sets * L;
+        std::vector<JobDev> views((size_t)nj);
+        GradBufs b{};
+        b.fwd = wc.fwd; b.adj = wc.jobs; b.fpart = nullptr; b.farr = nullptr; b.lpart = nullptr;
+        b.apart = wc.apart; b.dcs = wc.dcs; b.dsgs = wc.dsgs; b.fwd_err = nullptr;
+        b.status = wc.status;
+        JobDev base{};
+        fill_job(&f1, &base);
+        for (int g0 = 0; g0 < nj; g0 += kGradInstall) {
+            GradTable t;
+            memset(&t, 0, sizeof(t));
+            t.base = g0;
+            t.n = std::min(kGradInstall, nj - g0);
+            for (int k = 0; k < t.n; ++k) {
+                const int jb = g0 + k, st = jb / L, l = jb % L;
+                const size_t lz = (size_t)l * f->nz;
+                GradLite& a = t.j[k];
+                a.nx = base.nx; a.ny = base.ny; a.nz = base.nz;
+                a.nsx = base.nsx; a.nsy = base.nsy; a.nl = 1;
+                a.max_chunks_f = 1; a.max_chunks_a = 1; a.direct = 0; a.n_loss_part = 0;
+                a.ox = base.ox; a.oy = base.oy; a.dx = base.dx; a.dy = base.dy;
+                a.sx0 = base.sx0; a.sy0 = base.sy0; a.dsx = base.dsx; a.dsy = base.dsy;
+                a.w = w + (size_t)l * per;
+                a.idd = wc.act + (size_t)st * nzL + lz;
+                a.sigma = sigma + lz;
+                // set 0: the sigma term of dL/dR; set 1: sum_z <P, W> (the activity is 1 on
+                // every slice that the reduce reads)
+                a.didd = rng && st == 1 ? a.idd : nullptr;
+                a.dsig = rng && st == 0 ? dsigma_dr + lz : nullptr;
+                a.grad_dose = wc.maps + (size_t)jb * lstride;
+                a.grad_w = (st == 0 ? grad_w : wc.gw2) + (size_t)l * per;
+                a.grad_range = !rng ? nullptr : (st == 0 ? grad_range : wc.r1) + l;
+                a.slot_off = (size_t)jb * wc.slot_elems;
+                a.dcs_off = (size_t)jb * f->nz;
+                JobDev& v = views[(size_t)jb];
+                v = base;
+                v.nl = 1; v.max_chunks = 1;
+                v.w = a.w; v.idd = a.idd; v.sigma = a.sigma; v.grad_dose = a.grad_dose;
+                v.didd_dr = a.didd; v.dsig_dr = a.dsig;
+                v.grad_w = a.grad_w; v.grad_range = a.grad_range;
+                v.partial = wc.apart + a.slot_off;
+                v.dc = wc.dcs + a.dcs_off; v.dsg = wc.dsgs + a.dcs_off;
+            }
+            install_grad_kernel<<<(std::max(t.n, kStatusInts) + 63) / 64, 64, 0, s>>>(t, b);
+            PBD_LAUNCH_CHECK();
+            count_launch(1);
+        }
+        PBD_TRY(launch_adjoint_tc(precision, wc.jobs, views.data(), nj, wc.acnt,
+                                  wc.status + kStatAdj, 1, rng ? 1 : 0, 0, 0, s));
+    }
+    if (rng) {
+        wed_range_combine_kernel<<<(L + 127) / 128, 128, 0, s>>>(grad_range, wc.r1, L);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    }
     return PBD_OK;
 }
 
@@ -1089,7 +1198,7 @@ int pbd_adjoint_wed_workspace(const pbd_field* f, const pbd_lut_spec* spec, int 
     PBD_TRY(adjoint_supported(f));
     if (!spec || !bytes) return PBD_ERR_NULL_ARG;
     WedAdjCarve w;
-    return carve_wed_adj(f, precision, nullptr, w, bytes);
+    return carve_wed_adj(f, precision, 1, nullptr, w, bytes);
 }
 
 int pbd_adjoint_wed(const pbd_field* f, const pbd_lut_spec* spec, const void* curves,
@@ -1103,72 +1212,60 @@ int pbd_adjoint_wed(const pbd_field* f, const pbd_lut_spec* spec, const void* cu
     PBD_TRY(adjoint_supported(f));
     WedAdjCarve wc;
     size_t need = 0;
-    PBD_TRY(carve_wed_adj(f, precision, nullptr, wc, &need));
+    PBD_TRY(carve_wed_adj(f, precision, 1, nullptr, wc, &need));
     if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
-    PBD_TRY(carve_wed_adj(f, precision, workspace, wc, &need));
+    PBD_TRY(carve_wed_adj(f, precision, 1, workspace, wc, &need));
     cudaStream_t s = (cudaStream_t)stream;
     const size_t nslice = (size_t)f->ny * f->nx, nvox = (size_t)f->nz * nslice;
-    const size_t lstride = wed_lateral_stride(f);
     PBD_TRY(lut_wed_activity(spec, f->n_layers, curves, curves_bytes, wed, f->nz, nslice, wc.act,
                              s));
     PBD_TRY(lut_wed_grad_maps(spec, f->n_layers, curves, curves_bytes, grad_dose, wed, nvox,
-                              lstride, wc.maps, s));
-    // layer l: the adjoint of its lateral map with depth dose 1 on its active slices
-    pbd_field f1 = *f;
-    f1.n_layers = 1;
-    const size_t per = (size_t)f->n_sy * f->n_sx;
-    if (precision == PBD_PREC_FP32) {
-        PBD_TRY(cuda_rc(cudaMemsetAsync(wc.status, 0, kStatusInts * sizeof(int), s)));
-        for (int l = 0; l < f->n_layers; ++l)
-            PBD_TRY(adjoint_one(&f1, w + (size_t)l * per, wc.act + (size_t)l * f->nz,
-                                sigma + (size_t)l * f->nz, nullptr, nullptr,
-                                wc.maps + (size_t)l * lstride, grad_w + (size_t)l * per, nullptr,
-                                precision, wc.adj, wc.adj_bytes, wc.status + kStatAdj, s));
-        return PBD_OK;
-    }
-    // tensor cores: the L single-layer jobs installed kGradInstall at a time (the first group
-    // also clears the status header), then one adjoint launch and one reduce launch over them
-    std::vector<JobDev> views((size_t)f->n_layers);
-    GradBufs b{};
-    b.fwd = wc.fwd; b.adj = wc.jobs; b.fpart = nullptr; b.farr = nullptr; b.lpart = nullptr;
-    b.apart = wc.apart; b.dcs = wc.dcs; b.dsgs = wc.dsgs; b.fwd_err = nullptr;
-    b.status = wc.status;
-    JobDev base{};
-    fill_job(&f1, &base);
-    for (int g0 = 0; g0 < f->n_layers; g0 += kGradInstall) {
-        GradTable t;
-        memset(&t, 0, sizeof(t));
-        t.base = g0;
-        t.n = std::min(kGradInstall, f->n_layers - g0);
-        for (int k = 0; k < t.n; ++k) {
-            const int l = g0 + k;
-            GradLite& a = t.j[k];
-            a.nx = base.nx; a.ny = base.ny; a.nz = base.nz;
-            a.nsx = base.nsx; a.nsy = base.nsy; a.nl = 1;
-            a.max_chunks_f = 1; a.max_chunks_a = 1; a.direct = 0; a.n_loss_part = 0;
-            a.ox = base.ox; a.oy = base.oy; a.dx = base.dx; a.dy = base.dy;
-            a.sx0 = base.sx0; a.sy0 = base.sy0; a.dsx = base.dsx; a.dsy = base.dsy;
-            a.w = w + (size_t)l * per;
-            a.idd = wc.act + (size_t)l * f->nz;
-            a.sigma = sigma + (size_t)l * f->nz;
-            a.grad_dose = wc.maps + (size_t)l * lstride;
-            a.grad_w = grad_w + (size_t)l * per;
-            a.slot_off = (size_t)l * wc.slot_elems;
-            a.dcs_off = (size_t)l * f->nz;
-            JobDev& v = views[(size_t)l];
-            v = base;
-            v.nl = 1; v.max_chunks = 1;
-            v.w = a.w; v.idd = a.idd; v.sigma = a.sigma; v.grad_dose = a.grad_dose;
-            v.grad_w = a.grad_w;
-            v.partial = wc.apart + a.slot_off;
-            v.dc = wc.dcs + a.dcs_off; v.dsg = wc.dsgs + a.dcs_off;
-        }
-        install_grad_kernel<<<(std::max(t.n, kStatusInts) + 63) / 64, 64, 0, s>>>(t, b);
-        PBD_LAUNCH_CHECK();
-        count_launch(1);
-    }
-    return launch_adjoint_tc(precision, wc.jobs, views.data(), f->n_layers, wc.acnt,
-                             wc.status + kStatAdj, 1, 0, 0, 0, s);
+                              wed_lateral_stride(f), wc.maps, s));
+    return wed_adjoint_jobs(f, wc, w, sigma, nullptr, grad_w, nullptr, precision, s);
+}
+
+int pbd_adjoint_wed_range_workspace(const pbd_field* f, const pbd_lut_spec* spec, int precision,
+                                    size_t* bytes) {
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    PBD_TRY(adjoint_supported(f));
+    if (!spec || !bytes) return PBD_ERR_NULL_ARG;
+    WedAdjCarve w;
+    return carve_wed_adj(f, precision, 2, nullptr, w, bytes);
+}
+
+int pbd_adjoint_wed_range(const pbd_field* f, const pbd_lut_spec* spec, const void* curves,
+                          size_t curves_bytes, const void* curves_p, const void* curves_m,
+                          double h, const float* w, const double* sigma, const double* dsigma_dr,
+                          const double* wed, const float* grad_dose, float* grad_w,
+                          float* grad_range, int precision, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+    if (!f || !spec || !curves || !curves_p || !curves_m || !w || !sigma || !dsigma_dr || !wed ||
+        !grad_dose || !grad_w || !grad_range)
+        return PBD_ERR_NULL_ARG;
+    if (!(h > 0.0) || !isfinite(h)) return PBD_ERR_BAD_VALUE;
+    PBD_TRY(host_validate_field(f));
+    PBD_TRY(check_field_precision(f, precision));
+    PBD_TRY(adjoint_supported(f));
+    WedAdjCarve wc;
+    size_t need = 0;
+    PBD_TRY(carve_wed_adj(f, precision, 2, nullptr, wc, &need));
+    if (!workspace || workspace_bytes < need) return PBD_ERR_WORKSPACE;
+    PBD_TRY(carve_wed_adj(f, precision, 2, workspace, wc, &need));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int L = f->n_layers;
+    const size_t nslice = (size_t)f->ny * f->nx, nvox = (size_t)f->nz * nslice;
+    const size_t lstride = wed_lateral_stride(f);
+    // set 0: g IDD_l(WED) on the nominal curves' active slices; set 1: g dIDD_l/dR(WED) on the
+    // slices that either shifted curve reaches
+    PBD_TRY(lut_wed_activity(spec, L, curves, curves_bytes, wed, f->nz, nslice, wc.act, s));
+    PBD_TRY(lut_wed_grad_maps(spec, L, curves, curves_bytes, grad_dose, wed, nvox, lstride,
+                              wc.maps, s));
+    PBD_TRY(lut_wed_activity(spec, L, curves_p, curves_bytes, wed, f->nz, nslice,
+                             wc.act + (size_t)L * f->nz, s, curves_m, curves_bytes));
+    PBD_TRY(lut_wed_grad_maps_dr(spec, L, curves_p, curves_bytes, curves_m, curves_bytes, h,
+                                 grad_dose, wed, nvox, lstride, wc.maps + (size_t)L * lstride, s));
+    return wed_adjoint_jobs(f, wc, w, sigma, dsigma_dr, grad_w, grad_range, precision, s);
 }
 
 int pbd_loss_grad_batch_workspace(const pbd_grad_job* jobs, int n_jobs, int precision,

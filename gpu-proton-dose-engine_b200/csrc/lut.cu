@@ -670,6 +670,39 @@ __global__ void __launch_bounds__(256) wed_grad_maps_kernel(LutDims dm, const La
     }
 }
 
+// Depth dose of a layer's curve at depth d (the curve's interval search and np.interp
+// semantics, as in wed_grad_maps_kernel): 0 outside [0, zmax].
+__device__ __forceinline__ double curve_at(const LayerScal& sc, const double2* pts, int n, double d) {
+    const double zm = sc.zmax;
+    if (d < 0.0 || d > zm) return 0.0;
+    const double st = (zm - 0.0) / (double)(n - 1), is = 1.0 / st;
+    int lo = 0;
+    double x0 = 0.0;
+    locate_lin(d, 0.0, zm, n, st, is, lo, x0);
+    const double2 pt = __ldg(pts + lo);
+    return x0 == d ? pt.x : pt.y * (d - x0) + pt.x;
+}
+
+// maps (L, lstride): dL/dD times the range derivative of each layer's depth dose at the WED,
+// (IDD+_l(WED) - IDD-_l(WED)) / (2 h), from the curves at range shifts +h and -h (FP64 difference,
+// one FP32 rounding of the product).
+__global__ void __launch_bounds__(256) wed_grad_maps_dr_kernel(
+    LutDims dm, const LayerScal* scp, const double2* ptp, const LayerScal* scm,
+    const double2* ptm, const float* grad, const double* wed, size_t nvox, int n_layers,
+    size_t lstride, double inv2h, float* maps) {
+    const int n = dm.n_idd;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (size_t)gridDim.x * blockDim.x) {
+        const double d = wed[v];
+        const double g = (double)grad[v];
+        for (int l = 0; l < n_layers; ++l) {
+            const double dp = curve_at(scp[l], ptp + (size_t)l * n, n, d);
+            const double dmn = curve_at(scm[l], ptm + (size_t)l * n, n, d);
+            maps[(size_t)l * lstride + v] = (float)((dp - dmn) * inv2h * g);
+        }
+    }
+}
+
 // Curve points of the smoothed depth curves: {fp[k], slope_k} with slope_k = (fp[k+1] - fp[k])
 // / (x[k+1] - x[k]) on the grid linspace(0, zmax, n) -- the operands and the single rounding
 // of np.interp's slope (and of interp_lin) -- and 0 at the last point.  Value and slope share a
@@ -697,6 +730,7 @@ __global__ void wed_slope_kernel(LutDims dm, const LayerScal* scal, const double
 constexpr int kActThreads = 1024;
 
 __global__ void __launch_bounds__(kActThreads) wed_activity_kernel(const LayerScal* scal,
+                                                                   const LayerScal* scal2,
                                                                    const double* wed,
                                                                    size_t nslice, int nz,
                                                                    int n_layers, double* act) {
@@ -727,8 +761,11 @@ __global__ void __launch_bounds__(kActThreads) wed_activity_kernel(const LayerSc
     }
     __syncthreads();
     const double smin = red[0];
-    for (int l = threadIdx.x; l < n_layers; l += kActThreads)
-        act[(size_t)l * nz + z] = smin <= scal[l].zmax ? 1.0 : 0.0;
+    // with a second curve set: active where either set's curve reaches
+    for (int l = threadIdx.x; l < n_layers; l += kActThreads) {
+        const double zm = scal2 ? fmax(scal[l].zmax, scal2[l].zmax) : scal[l].zmax;
+        act[(size_t)l * nz + z] = smin <= zm ? 1.0 : 0.0;
+    }
 }
 
 // Water-equivalent depth at the voxel centres z_k = oz + k dz along +z (the beam axis):
@@ -969,14 +1006,23 @@ int lut_wed_curves(const pbd_lut_spec* s, int n_layers, const double* energies,
 }
 
 int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, size_t curves_bytes,
-                     const double* wed, int nz, size_t nslice, double* act, cudaStream_t st) {
+                     const double* wed, int nz, size_t nslice, double* act, cudaStream_t st,
+                     const void* curves2, size_t curves2_bytes) {
     PBD_TRY(validate_spec(s, n_layers));
     if (!wed || !act) return PBD_ERR_NULL_ARG;
     LutDims dm;
     LutWs w;
     double2* pts = nullptr;
     PBD_TRY(wed_dims(s, n_layers, curves, curves_bytes, dm, w, pts));
-    wed_activity_kernel<<<nz, kActThreads, 0, st>>>(w.scal, wed, nslice, nz, n_layers, act);
+    const LayerScal* scal2 = nullptr;
+    if (curves2) {
+        LutDims dm2;
+        LutWs w2;
+        double2* pts2 = nullptr;
+        PBD_TRY(wed_dims(s, n_layers, curves2, curves2_bytes, dm2, w2, pts2));
+        scal2 = w2.scal;
+    }
+    wed_activity_kernel<<<nz, kActThreads, 0, st>>>(w.scal, scal2, wed, nslice, nz, n_layers, act);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return PBD_OK;
@@ -1029,6 +1075,29 @@ int lut_wed_grad_maps(const pbd_lut_spec* s, int n_layers, const void* curves,
     const int blocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 8);
     wed_grad_maps_kernel<<<std::max(blocks, 1), 256, 0, st>>>(dm, w.scal, pts, grad, wed, nvox,
                                                               n_layers, lstride, maps);
+    PBD_LAUNCH_CHECK();
+    count_launch(1);
+    return PBD_OK;
+}
+
+int lut_wed_grad_maps_dr(const pbd_lut_spec* s, int n_layers, const void* curves_p,
+                         size_t curves_p_bytes, const void* curves_m, size_t curves_m_bytes,
+                         double h, const float* grad, const double* wed, size_t nvox,
+                         size_t lstride, float* maps, cudaStream_t st) {
+    PBD_TRY(validate_spec(s, n_layers));
+    if (!grad || !wed || !maps || !curves_p || !curves_m) return PBD_ERR_NULL_ARG;
+    if (lstride < nvox) return PBD_ERR_BAD_VALUE;
+    if (!(h > 0.0) || !isfinite(h)) return PBD_ERR_BAD_VALUE;
+    LutDims dp, dmm;
+    LutWs wp, wm;
+    double2* pp = nullptr;
+    double2* pm = nullptr;
+    PBD_TRY(wed_dims(s, n_layers, curves_p, curves_p_bytes, dp, wp, pp));
+    PBD_TRY(wed_dims(s, n_layers, curves_m, curves_m_bytes, dmm, wm, pm));
+    const int blocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)num_sms() * 8);
+    wed_grad_maps_dr_kernel<<<std::max(blocks, 1), 256, 0, st>>>(dp, wp.scal, pp, wm.scal, pm, grad,
+                                                                 wed, nvox, n_layers, lstride,
+                                                                 0.5 / h, maps);
     PBD_LAUNCH_CHECK();
     count_launch(1);
     return PBD_OK;

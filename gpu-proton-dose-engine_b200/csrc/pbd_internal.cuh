@@ -242,8 +242,11 @@ int lut_csda(const double* e, double* r, int n, int inverse, cudaStream_t st);
 int lut_curve_workspace(const pbd_lut_spec* s, int n_layers, size_t* bytes);
 int lut_wed_curves(const pbd_lut_spec* s, int n_layers, const double* energies,
                    const double* shift, void* curves, size_t curves_bytes, cudaStream_t st);
+// act (L, nz): 1 where some voxel of the slice lies within the layer's curve (of either set,
+// when a second curve set is given)
 int lut_wed_activity(const pbd_lut_spec* s, int n_layers, const void* curves, size_t curves_bytes,
-                     const double* wed, int nz, size_t nslice, double* act, cudaStream_t st);
+                     const double* wed, int nz, size_t nslice, double* act, cudaStream_t st,
+                     const void* curves2 = nullptr, size_t curves2_bytes = 0);
 int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, size_t lstride,
                     const double* wed, size_t nvox, float* dose, int* err, const int* err2,
                     const void* curves, size_t curves_bytes, cudaStream_t st);
@@ -252,6 +255,12 @@ int lut_wed_combine(const pbd_lut_spec* s, int n_layers, const float* lateral, s
 int lut_wed_grad_maps(const pbd_lut_spec* s, int n_layers, const void* curves,
                       size_t curves_bytes, const float* grad, const double* wed, size_t nvox,
                       size_t lstride, float* maps, cudaStream_t st);
+// maps (L, lstride): dL/dD times (IDD+_l(WED) - IDD-_l(WED)) / (2 h), the curves built at range
+// shifts +h and -h (the heterogeneous range gradient's per-layer input).
+int lut_wed_grad_maps_dr(const pbd_lut_spec* s, int n_layers, const void* curves_p,
+                         size_t curves_p_bytes, const void* curves_m, size_t curves_m_bytes,
+                         double h, const float* grad, const double* wed, size_t nvox,
+                         size_t lstride, float* maps, cudaStream_t st);
 int lut_wed_raytrace(int nz, int ny, int nx, double oz, double dz, const float* rho, double* wed,
                      cudaStream_t st);
 

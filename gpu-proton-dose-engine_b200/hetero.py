@@ -14,7 +14,9 @@ implemented.  Here, on the device:
   depth (a broad-beam ray-casting approximation; the lateral scattering in the material is
   not modelled) (``pbd_build_wed_curves`` once, then ``pbd_forward_wed_curves``).  In water it
   reproduces the homogeneous dose.  ``WedPlan(problem).adjoint(grad_dose, wed)`` gives dL/dW
-  (``pbd_adjoint_wed``), for plan optimisation in the medium.
+  (``pbd_adjoint_wed``), and with ``with_range=True`` also dL/d(range shift) per layer
+  (``pbd_adjoint_wed_range``: the depth curves' and the widths' central differences at +-h),
+  for plan optimisation in the medium.
 """
 from __future__ import annotations
 
@@ -54,7 +56,8 @@ class WedPlan:
     and the workspaces of ``pbd_forward_wed_curves`` and (on first use) ``pbd_adjoint_wed``."""
 
     def __init__(self, problem, *, precision: str = "tf32x3", device=None,
-                 idd_model: ph.IDDModel = ph.DEFAULT_IDD, sigma_x0: float = 0.30):
+                 idd_model: ph.IDDModel = ph.DEFAULT_IDD, sigma_x0: float = 0.30,
+                 fd_step: float = 0.005):
         torch = _lib.require_cuda()
         self.torch = torch
         self.device = torch.device(device or "cuda")
@@ -74,14 +77,40 @@ class WedPlan:
                             ctypes.byref(self.spec), self.precision)
         self.ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
         self.adj_ws = None
+        self.range_ws = None
+        self.idd_model, self.sigma_x0, self.fd_step = idd_model, sigma_x0, float(fd_step)
+        self.curves_pm = None   # the curves at range shifts +h and -h, built on first use
+        self.dsigma_dr = None
         # the depth curves depend on the energies only: built once, reused by every call
         cbytes = _lib.query("pbd_wed_curves_workspace", ctypes.byref(self.spec), len(L.energies))
         self.curves = torch.empty(cbytes, dtype=torch.uint8, device=self.device)
-        _lib.call("pbd_build_wed_curves", ctypes.byref(self.spec), len(L.energies),
-                  _lib.ptr(self.energies), None, _lib.ptr(self.curves), cbytes,
-                  _lib.stream_handle(self.device))
+        self._build_curves(self.curves, None)
         self.shape = (g.nz, g.ny, g.nx)
         self.nvox = g.nz * g.ny * g.nx
+
+    def _build_curves(self, out, shift):
+        _lib.call("pbd_build_wed_curves", ctypes.byref(self.spec), int(self.energies.numel()),
+                  _lib.ptr(self.energies), _lib.ptr(shift), _lib.ptr(out), out.numel(),
+                  _lib.stream_handle(self.device))
+
+    def _range_tables(self):
+        """The curves at range shifts +-h and the widths' range derivative (once per plan)."""
+        if self.curves_pm is None:
+            torch = self.torch
+            g = self.problem.grid
+            h = self.fd_step
+            n = int(self.energies.numel())
+            pm = []
+            for sign in (1.0, -1.0):
+                c = torch.empty_like(self.curves)
+                self._build_curves(c, torch.full((n,), sign * h, dtype=torch.float64,
+                                                 device=self.device))
+                pm.append(c)
+            self.curves_pm = tuple(pm)
+            self.dsigma_dr = ph.build_tables(g.nz, g.oz, g.dz, self.problem.lattice.energies,
+                                             idd_model=self.idd_model, sigma_x0=self.sigma_x0,
+                                             fd_step=h, device=self.device).dsigma_dr
+        return self.curves_pm, self.dsigma_dr
 
     def _wed(self, wed):
         """The WED map as a contiguous float64 device tensor (host data is uploaded)."""
@@ -114,14 +143,31 @@ class WedPlan:
                   self.ws.numel(), _lib.stream_handle(self.device))
         return out
 
-    def adjoint(self, grad_dose, wed, w=None):
+    def adjoint(self, grad_dose, wed, w=None, with_range: bool = False):
         """dL/dW (float32 device tensor (L, nsy, nsx)) of the heterogeneous dose for the
-        dL/dD ``grad_dose`` ((nz, ny, nx)) and the WED map ``wed`` (``pbd_adjoint_wed``)."""
+        dL/dD ``grad_dose`` ((nz, ny, nx)) and the WED map ``wed`` (``pbd_adjoint_wed``).
+        ``with_range=True`` returns (dL/dW, dL/dR), dL/dR (L,) float32 the gradient in each
+        layer's range shift (``pbd_adjoint_wed_range``)."""
         torch = self.torch
         wd = self._wed(wed)
         wt = self._weights(w)
         g = torch.as_tensor(grad_dose).to(self.device, torch.float32).contiguous()
         _lib.check_arg(g, "grad_dose", self.nvox, torch.float32, self.device)
+        if with_range:
+            (cp, cm), dsig = self._range_tables()
+            if self.range_ws is None:
+                nbytes = _lib.query("pbd_adjoint_wed_range_workspace", ctypes.byref(self.field),
+                                    ctypes.byref(self.spec), self.precision)
+                self.range_ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+            gw = torch.empty_like(self.w)
+            gr = torch.empty(self.w.shape[0], dtype=torch.float32, device=self.device)
+            _lib.call("pbd_adjoint_wed_range", ctypes.byref(self.field), ctypes.byref(self.spec),
+                      _lib.ptr(self.curves), self.curves.numel(), _lib.ptr(cp), _lib.ptr(cm),
+                      self.fd_step, _lib.ptr(wt), _lib.ptr(self.sigma), _lib.ptr(dsig),
+                      _lib.ptr(wd), _lib.ptr(g), _lib.ptr(gw), _lib.ptr(gr), self.precision,
+                      _lib.ptr(self.range_ws), self.range_ws.numel(),
+                      _lib.stream_handle(self.device))
+            return gw, gr
         if self.adj_ws is None:
             nbytes = _lib.query("pbd_adjoint_wed_workspace", ctypes.byref(self.field),
                                 ctypes.byref(self.spec), self.precision)

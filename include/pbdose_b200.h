@@ -133,7 +133,7 @@ PBD_API int pbd_launch_count(long long *n);
  * a wait that runs out makes the call's results NaN and sets a status word at the start of
  * its workspace.  This reads those words on `stream`, waits for the stream, and stores
  * PBD_OK or PBD_ERR_TIMEOUT in *status.  Valid after pbd_forward, pbd_adjoint, pbd_loss_grad,
- * pbd_forward_batch, pbd_loss_grad_batch, pbd_forward_wed(_curves) and pbd_adjoint_wed; not
+ * pbd_forward_batch, pbd_loss_grad_batch, pbd_forward_wed(_curves) and pbd_adjoint_wed(_range); not
  * for use inside stream capture. */
 PBD_API int pbd_workspace_status(const void *workspace, size_t workspace_bytes, int *status,
                                  void *stream);
@@ -281,13 +281,33 @@ PBD_API int pbd_forward_wed_curves(const pbd_field *f, const pbd_lut_spec *spec,
  * grad_w (L, nsy, nsx) float32, sum over voxels of grad_dose * IDD_l(WED) * dLateral_l/dW_l --
  * the adjoint of pbd_forward_wed_curves (same field, spec, curve blob, w, sigma, wed).  No
  * counterpart in the reference.  Per layer: dL/dD times the layer's depth dose at the WED,
- * then the layer's adjoint (the same kernels as pbd_adjoint). */
+ * then the layer's adjoint (the kernels of pbd_adjoint; on the tensor cores one launch over
+ * every layer). */
 PBD_API int pbd_adjoint_wed_workspace(const pbd_field *f, const pbd_lut_spec *spec, int precision,
                                       size_t *bytes);
 PBD_API int pbd_adjoint_wed(const pbd_field *f, const pbd_lut_spec *spec, const void *curves,
                             size_t curves_bytes, const float *w, const double *sigma,
                             const double *wed, const float *grad_dose, float *grad_w,
                             int precision, void *workspace, size_t workspace_bytes, void *stream);
+
+/* dL/dW and dL/d(range shift) of the heterogeneous dose for a given dL/dD: grad_w as
+ * pbd_adjoint_wed, grad_range (L) float32.  No counterpart in the reference (its only
+ * heterogeneous code is the WED stub, physics.py:421-423).  A range shift moves each layer's
+ * depth curve and its water widths: dL/dR_l = sum_v g IDD'_l(WED) Lat_l + sum_z dL/dsigma_lz
+ * dsigma_lz/dR, with IDD'_l the central difference (curves_p - curves_m) / (2 h) of the layer's
+ * curves built by pbd_build_wed_curves at range shifts +h and -h (same spec, energies and
+ * blob size as `curves`), and dsigma_dr (L, nz) float64 the widths' range derivative
+ * (pbd_build_luts with fd_step = h).  Both terms come from one adjoint launch on the tensor
+ * cores (FP32: one SIMT adjoint per layer and term). */
+PBD_API int pbd_adjoint_wed_range_workspace(const pbd_field *f, const pbd_lut_spec *spec,
+                                            int precision, size_t *bytes);
+PBD_API int pbd_adjoint_wed_range(const pbd_field *f, const pbd_lut_spec *spec,
+                                  const void *curves, size_t curves_bytes, const void *curves_p,
+                                  const void *curves_m, double h, const float *w,
+                                  const double *sigma, const double *dsigma_dr, const double *wed,
+                                  const float *grad_dose, float *grad_w, float *grad_range,
+                                  int precision, void *workspace, size_t workspace_bytes,
+                                  void *stream);
 
 /* ---- plan-optimisation steps (no counterpart in the reference) ---------------------
  * Device-resident state, so that an optimisation iteration (tables, loss gradient,

@@ -203,3 +203,64 @@ def test_gradient_vs_oracle(pb):
         lhs = float(np.sum(gp * wl["weights"]))
         rhs = float(np.sum(pos * d))
         assert abs(lhs - rhs) <= 1e-5 * abs(rhs), (prec, lhs, rhs)
+
+
+def _slab(g):
+    zc = g.oz + np.arange(g.nz) * g.dz
+    rho = np.ones((g.nz, g.ny, g.nx), dtype=np.float32)
+    rho[(zc >= 2.0) & (zc < 3.0)] = 1.6
+    rho[(zc >= 4.0) & (zc < 5.4), :, : g.nx // 2] = 0.25
+    return zc, rho
+
+
+def test_range_gradient_vs_oracle(pb):
+    """dL/dW and dL/d(range shift) of the heterogeneous dose in one call
+    (pbd_adjoint_wed_range) for a random dL/dD in the slab phantom, against the oracle: dL/dW
+    by float64 autograd, dL/dR by the chain rule through the central differences at +-h of the
+    depth curves (at the WED) and of the widths (float64, autograd for the widths' part).
+    Tolerance 1e-4 of max for both (the adjoint's split-BF16 products; FP32 well inside)."""
+    import torch
+    wl, en, prob = _cfg0(pb)
+    g = prob.grid
+    zc, rho = _slab(g)
+    wed_np = hr.wed_ref(rho, g.oz, g.dz)
+    rng = np.random.default_rng(5)
+    grad = rng.standard_normal((g.nz, g.ny, g.nx)).astype(np.float32)
+    h = 0.005
+    want_r = hr.grad_range_ref(g.x, g.y, prob.lattice.spot_x, prob.lattice.spot_y, wl["weights"],
+                               en, zc, wed_np, grad.astype(np.float64), h)
+    sig = pr.layer_luts(zc, en)[1]
+    want_w = hr.grad_w_ref(g.x, g.y, prob.lattice.spot_x, prob.lattice.spot_y, wl["weights"], en,
+                           sig, wed_np, grad.astype(np.float64))
+    wed = pb.hetero.wed_raytrace(rho, g)
+    for prec in ("fp32", "tf32x3", "fp16x3"):
+        plan = pb.hetero.WedPlan(prob, precision=prec, fd_step=h)
+        gw, gr = plan.adjoint(torch.as_tensor(grad, device="cuda"), wed, with_range=True)
+        ew, er_ = rel(gw.cpu().numpy(), want_w), rel(gr.cpu().numpy(), want_r)
+        print(f"{prec}: heterogeneous dL/dW {ew:.2e}, dL/dR {er_:.2e} of max")
+        assert ew < 1e-4, prec
+        assert er_ < 1e-4, prec
+        # the dL/dW of the range call equals the plain adjoint's
+        gw1 = plan.adjoint(torch.as_tensor(grad, device="cuda"), wed)
+        assert torch.equal(gw, gw1), prec
+
+
+def test_range_gradient_in_water_equals_homogeneous(pb):
+    """In water (rho = 1, WED = depth) the heterogeneous dL/dR equals the homogeneous
+    adjoint's dL/dR through the depth tables' range derivatives (the same central differences
+    at the grid depths): 1e-4 of max, and dL/dW likewise."""
+    import torch
+    wl, en, prob = _cfg0(pb)
+    g = prob.grid
+    rho = np.ones((g.nz, g.ny, g.nx), dtype=np.float32)
+    wed = pb.hetero.wed_raytrace(rho, g)
+    grad = torch.as_tensor(np.random.default_rng(6).standard_normal((g.nz, g.ny, g.nx)),
+                           dtype=torch.float32, device="cuda")
+    for prec in ("fp32", "tf32x3"):
+        hp = pb.hetero.WedPlan(prob, precision=prec, fd_step=0.005)
+        gw, gr = hp.adjoint(grad, wed, with_range=True)
+        dp = pb.engines.DosePlan(prob, tables="device", precision=prec, fd_step=0.005)
+        gw0, gr0 = dp.adjoint(grad, with_range=True)
+        torch.cuda.synchronize()
+        assert rel(gw.cpu().numpy(), gw0.cpu().numpy()) < 1e-4, prec
+        assert rel(gr.cpu().numpy(), gr0.cpu().numpy()) < 1e-4, prec

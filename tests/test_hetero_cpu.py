@@ -79,6 +79,20 @@ def test_wed_entry_points_validate_before_device_work():
     nog = list(aargs)
     nog[7] = None                                   # no dL/dD
     assert lib.pbd_adjoint_wed(*nog, fake, ab.value, None) == -1
+    # dL/dW and dL/d(range shift) of the heterogeneous dose
+    rb = ctypes.c_size_t(0)
+    assert lib.pbd_adjoint_wed_range_workspace(ctypes.byref(f), ctypes.byref(spec), 1,
+                                               ctypes.byref(rb)) == 0 and rb.value > ab.value
+    assert lib.pbd_adjoint_wed_range_workspace(ctypes.byref(f), None, 1, ctypes.byref(rb)) == -1
+    rargs = [ctypes.byref(f), ctypes.byref(spec), fake, cb.value, fake, fake, 0.005, fake, fake,
+             fake, fake, fake, fake, fake, 1]
+    assert lib.pbd_adjoint_wed_range(*rargs, None, 0, None) == -7
+    bad_h = list(rargs)
+    bad_h[6] = 0.0                                  # no central-difference step
+    assert lib.pbd_adjoint_wed_range(*bad_h, fake, rb.value, None) == -10
+    nor = list(rargs)
+    nor[13] = None                                  # no dL/dR output
+    assert lib.pbd_adjoint_wed_range(*nor, fake, rb.value, None) == -1
 
 
 def test_oracle_dose_in_water_equals_reference_dose():
@@ -154,3 +168,42 @@ def test_oracle_nan_and_out_of_range_semantics():
     for fill in (1e3, -1.0):
         assert np.count_nonzero(hr.dose_ref(xv, yv, xs, ys, w, en, sig,
                                             np.full_like(wed, fill))) == 0
+
+
+def test_oracle_range_gradient_matches_its_central_difference():
+    """The oracle's heterogeneous dL/d(range shift) (the chain rule through the +-h central
+    differences of the depth curves and widths, what the device computes) against the central
+    difference of the oracle's own loss L(dR) = sum(g D(dR)) on the 32 x 32 x 64 field in a
+    slab phantom, layers 0, 3 and 7.  The two differ at second order in the secants, which the
+    tables' non-smoothness in range (CSDA binning, the Fermi-Eyges grid) makes ~1e-3 of max."""
+    from oracle import physics_ref as pr
+    pb = load_pkg()
+    wl = pb.workloads.build_workload(0)
+    gd = wl["grid"]
+    grid = pb.model.DoseGrid(gd["nx"], gd["ny"], gd["nz"], gd["dx"], gd["dy"], gd["dz"], gd["ox"],
+                             gd["oy"], gd["oz"])
+    lat = pb.model.SpotLattice(wl["n_sx"], wl["n_sy"], wl["n_layers"], wl["spot_pitch"],
+                               wl["spot_pitch"], x0=wl["x0"], y0=wl["y0"], weights=wl["weights"])
+    en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
+    zc = grid.oz + np.arange(grid.nz) * grid.dz
+    rho = np.ones((grid.nz, grid.ny, grid.nx))
+    rho[(zc >= 2.0) & (zc < 3.0)] = 1.6
+    rho[(zc >= 4.0) & (zc < 5.4), :, : grid.nx // 2] = 0.25
+    wed = hr.wed_ref(rho, grid.oz, grid.dz)
+    g = np.random.default_rng(5).standard_normal(wed.shape)
+    h = 0.005
+    got = hr.grad_range_ref(grid.x, grid.y, lat.spot_x, lat.spot_y, wl["weights"], en, zc, wed,
+                            g, h)
+
+    def loss(shift):
+        _, sig = pr.layer_luts(zc, en, range_shift=shift)
+        e2 = pr.energy_from_range(pr.csda_range(en) + shift)
+        d = hr.dose_ref(grid.x, grid.y, lat.spot_x, lat.spot_y, wl["weights"], e2, sig, wed)
+        return float(np.sum(g * d))
+
+    scale = np.max(np.abs(got))
+    for l in (0, 3, 7):
+        s = np.zeros(len(en))
+        s[l] = h
+        fd = (loss(s) - loss(-s)) / (2.0 * h)
+        assert abs(fd - got[l]) <= 1e-2 * scale, (l, fd, got[l])
