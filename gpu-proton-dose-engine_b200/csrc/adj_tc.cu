@@ -690,17 +690,22 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
 }
 
 // After the main kernel: dL/dW, the per-pair dot products and dL/dR from the slots, with no
-// block waiting on another.  Block (entry chunk, layer l, job): each thread owns one slot
-// entry e = j * n1 + i of layer l (n1 = nsx rounded up to 16) and accumulates IDD * P slot
-// over the layer's active slices in slice order (kRedStep slices' loads in flight together),
-// then writes dL/dW[l, j, i] for i < nsx.
-// Chunk 0 of every layer also adds, per active slice, the eight warp partials of <P, W>
-// (dL/dIDD) and <S, W> (dL/dsigma, times IDD) in warp order and forms dL/dR_l in FP64 (a
-// fixed tree over the block); chunk 0 of layer 0 sums the loss partials the same way.  Every
-// sum is in a fixed order: deterministic.
+// block waiting on another.  Block (entry chunk, layer l, job): kRedEnt slot entries
+// e = j * n1 + i of layer l (n1 = nsx rounded up to 16) times kRedSeg depth segments.  The
+// layer's IDD column is staged in shared memory with its last active slice ze; segment s of an
+// entry sums IDD * P slot over its quarter of [0, ze) in slice order, its slot values arriving
+// by asynchronous 4-byte copies (cp.async: kRedB slices per batch, every copy of a batch in
+// flight together; inactive slices copy nothing and read 0); the segments' sums are then added
+// in segment order and written as dL/dW[l, j, i] (i < nsx).  One more block per layer (the
+// last in x) adds, per active slice, the eight warp partials of <P, W> (dL/dIDD) and <S, W>
+// (dL/dsigma, times IDD) in warp order and forms dL/dR_l in FP64 (a fixed tree over the
+// block); that block of layer 0 sums the loss partials the same way.  Every sum is in a fixed
+// order: deterministic.
 constexpr int kRedThreads = 256;
-constexpr int kRedStep = 32;       // slices whose loads are in flight together
-static_assert(kRedThreads % kRedStep == 0, "batches tile the shared IDD column");
+constexpr int kRedEnt = 64;                        // entries per block
+constexpr int kRedSeg = kRedThreads / kRedEnt;     // depth segments per entry
+constexpr int kRedTile = 1024;                     // slices staged per pass
+constexpr int kRedB = 16;                          // slices per copy batch
 
 __device__ __forceinline__ double block_sum_fixed(double v, double* red) {
     const int tid = threadIdx.x;
@@ -724,9 +729,10 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     if (l >= J.nl) return;
     const int nz = J.nz, nsx = J.nsx, nsy = J.nsy;
     const int n1 = (nsx + 15) / 16 * 16, per = nsy * n1;
-    if (ec * kRedThreads >= per) return;
-    const int tid = threadIdx.x;
-    const int e = ec * kRedThreads + tid;
+    const int nchunk = (per + kRedEnt - 1) / kRedEnt;   // entry blocks; block nchunk: the dots
+    if (ec > nchunk) return;
+    const int tid = threadIdx.x, el = tid % kRedEnt, sg = tid / kRedEnt;
+    const int e = ec * kRedEnt + el;
     const int ej = e / n1, ei = e - ej * n1;
     const bool own = e < per && ei < nsx;
     const size_t ndots = (size_t)J.nl * nz * kMathWarps;
@@ -735,62 +741,86 @@ __global__ void __launch_bounds__(kRedThreads) adj_tc_reduce_kernel(
     const double* idd = J.idd + (size_t)l * nz;
     const bool bad = *err != 0 || (J.fwd_err != nullptr && *J.fwd_err != 0);
     const float nan = __int_as_float(0x7fc00000);
+    __shared__ double red[kRedThreads];
+    if (ec == nchunk) {
+        // per job: no dL/dR output, or a missing derivative table, contributes nothing (the
+        // heterogeneous range gradient's two job sets use one table each)
+        const bool rng = with_range && J.grad_range != nullptr;
+        double a = 0.0;
+        for (int z = tid; z < nz; z += kRedThreads) {
+            const double c = idd[z];
+            if (c == 0.0) continue;
+            const size_t o = (size_t)l * nz + z;
+            const float* pa = dots + o * kMathWarps;
+            const float* pb = pa + ndots;
+            float sa = 0.f, sb = 0.f;
+#pragma unroll
+            for (int w = 0; w < kMathWarps; ++w) { sa += pa[w]; sb += pb[w]; }
+            const float dsg = (float)c * sb;
+            J.dc[o] = sa;
+            J.dsg[o] = dsg;
+            if (rng)
+                a += (J.didd_dr ? (double)sa * J.didd_dr[o] : 0.0) +
+                     (J.dsig_dr ? (double)dsg * J.dsig_dr[o] : 0.0);
+        }
+        if (rng) {
+            const double r = block_sum_fixed(a, red);
+            if (tid == 0) J.grad_range[l] = bad ? nan : (float)r;
+        }
+        if (finalize_loss && l == 0) {
+            double t = 0.0;
+            for (int b = tid; b < J.n_loss_part; b += kRedThreads) t += J.loss_part[b];
+            const double sum = block_sum_fixed(t, red);
+            if (tid == 0) *J.loss = bad ? (double)nan : sum;
+        }
+        return;
+    }
 
-    // the layer's IDD column, kRedThreads slices at a time, in shared memory: each batch of
-    // slot loads then depends on nothing in flight.  A slice whose IDD rounds to 0 in FP32
-    // adds 0 (and its slot is not read); every slice read has IDD != 0, so the adjoint wrote it.
-    __shared__ float s_c[kRedThreads];
+    __shared__ float s_c[kRedTile];
+    __shared__ int s_end;
+    __shared__ float sbuf[kRedB][kRedThreads];
+    __shared__ float s_part[kRedSeg][kRedEnt];
     float acc = 0.f;
-    for (int zt = 0; zt < nz; zt += kRedThreads) {
-        const int zn = min(kRedThreads, nz - zt);
-        __syncthreads();   // the previous tile's reads of s_c are done
-        s_c[tid] = tid < zn ? (float)idd[zt + tid] : 0.f;
+    const float* se = slots + (own ? e : 0);
+    for (int zt = 0; zt < nz; zt += kRedTile) {
+        const int zn = min(kRedTile, nz - zt);
+        __syncthreads();   // the previous pass's reads of s_c and s_end are done
+        if (tid == 0) s_end = 0;
+        for (int z = tid; z < zn; z += kRedThreads) s_c[z] = (float)idd[zt + z];
         __syncthreads();
-        const float* sz = slots + (size_t)zt * per + e;
-        for (int z0 = 0; z0 < zn; z0 += kRedStep) {
-            float pv[kRedStep], cf[kRedStep];
+        for (int z = tid; z < zn; z += kRedThreads)
+            if (s_c[z] != 0.f) atomicMax(&s_end, z + 1);
+        __syncthreads();
+        const int ze = s_end;   // slices [0, ze) of the pass hold every active one
+        const int q = (ze + kRedSeg - 1) / kRedSeg;
+        const int zb = sg * q, zf = min(ze, zb + q);
+        for (int z0 = zb; z0 < zf; z0 += kRedB) {
 #pragma unroll
-            for (int h = 0; h < kRedStep; ++h) {
-                cf[h] = s_c[z0 + h];          // z0 + h < kRedThreads (kRedStep divides it)
-                pv[h] = (own && cf[h] != 0.f) ? sz[(size_t)(z0 + h) * per] : 0.f;
+            for (int h = 0; h < kRedB; ++h) {
+                const int z = z0 + h;
+                const bool rd = own && z < zf && s_c[z < zf ? z : zb] != 0.f;
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(
+                                 tc::smem_u32(&sbuf[h][tid])),
+                             "l"(se + (size_t)(zt + (rd ? z : 0)) * per), "r"(rd ? 4 : 0)
+                             : "memory");
             }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
-            for (int h = 0; h < kRedStep; ++h) acc = fmaf(cf[h], pv[h], acc);
+            for (int h = 0; h < kRedB; ++h) {
+                const int z = z0 + h;
+                const float cf = z < zf ? s_c[z] : 0.f;
+                acc = fmaf(cf, sbuf[h][tid], acc);
+            }
         }
     }
-    if (own) J.grad_w[((size_t)l * nsy + ej) * nsx + ei] = bad ? nan : acc;
-    if (ec != 0) return;
-
-    __shared__ double red[kRedThreads];
-    // per job: no dL/dR output, or a missing derivative table, contributes nothing (the
-    // heterogeneous range gradient's two job sets use one table each)
-    const bool rng = with_range && J.grad_range != nullptr;
-    double a = 0.0;
-    for (int z = tid; z < nz; z += kRedThreads) {
-        const double c = idd[z];
-        if (c == 0.0) continue;
-        const size_t o = (size_t)l * nz + z;
-        const float* pa = dots + o * kMathWarps;
-        const float* pb = pa + ndots;
-        float sa = 0.f, sb = 0.f;
+    s_part[sg][el] = acc;
+    __syncthreads();
+    if (sg == 0 && own) {
+        float g = s_part[0][el];
 #pragma unroll
-        for (int w = 0; w < kMathWarps; ++w) { sa += pa[w]; sb += pb[w]; }
-        const float dsg = (float)c * sb;
-        J.dc[o] = sa;
-        J.dsg[o] = dsg;
-        if (rng)
-            a += (J.didd_dr ? (double)sa * J.didd_dr[o] : 0.0) +
-                 (J.dsig_dr ? (double)dsg * J.dsig_dr[o] : 0.0);
-    }
-    if (rng) {
-        const double r = block_sum_fixed(a, red);
-        if (tid == 0) J.grad_range[l] = bad ? nan : (float)r;
-    }
-    if (finalize_loss && l == 0) {
-        double t = 0.0;
-        for (int b = tid; b < J.n_loss_part; b += kRedThreads) t += J.loss_part[b];
-        const double sum = block_sum_fixed(t, red);
-        if (tid == 0) *J.loss = bad ? (double)nan : sum;
+        for (int k = 1; k < kRedSeg; ++k) g += s_part[k][el];
+        J.grad_w[((size_t)l * nsy + ej) * nsx + ei] = bad ? nan : g;
     }
 }
 
@@ -895,7 +925,7 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
     else rc = launch_mode<PBD_PREC_BF16X3>(P, s);
     PBD_TRY(rc);
     PBD_TRY(launch_dependent(adj_tc_reduce_kernel,
-                             dim3((max_per + kRedThreads - 1) / kRedThreads, max_l, n_jobs),
+                             dim3((max_per + kRedEnt - 1) / kRedEnt + 1, max_l, n_jobs),
                              dim3(kRedThreads), 0, s, (const JobDev*)jobs_dev, with_range,
                              finalize_loss, (const int*)err));
     count_launch(2);

@@ -24,12 +24,15 @@ thread_local int g_adj_chunk = 0;
 struct JobPair {
     JobDev j[2];
     int n;
+    int nzero;           // ints of `zero` to clear (<= 32), e.g. the adjoint's counter block
+    int* zero;
 };
 
-// Installs the call's job views and clears its status header (may be null).
+// Installs the call's job views and clears its status header (may be null) and p.zero.
 __global__ void install_jobs_kernel(JobPair p, JobDev* dst, int* status) {
     if ((int)threadIdx.x < p.n) dst[threadIdx.x] = p.j[threadIdx.x];
     if (status && (int)threadIdx.x < kStatusInts) status[threadIdx.x] = 0;
+    if (p.zero && (int)threadIdx.x < p.nzero) p.zero[threadIdx.x] = 0;
 }
 
 struct JobLite {
@@ -698,11 +701,14 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
     fill_adj_view(f, ws, A);
     A.fwd_err = ws.status + kStatFwd;
     p.j[1] = A;
-    // the adjoint's counters are cleared before the forward, so that forward -> adjoint ->
-    // reduce run back to back (programmatic dependent launches)
-    if (ws.adj_tc)
-        PBD_TRY(cuda_rc(cudaMemsetAsync(ws.acnt, 0,
-                                        tc_adjoint_counter_ints(1, f->n_layers) * sizeof(int), s)));
+    // the adjoint's counters are cleared by the install, before the forward, so that forward
+    // -> adjoint -> reduce run back to back (programmatic dependent launches)
+    if (ws.adj_tc) {
+        const size_t nc = tc_adjoint_counter_ints(1, f->n_layers);
+        if (nc > 32) return PBD_ERR_UNSUPPORTED;
+        p.zero = ws.acnt;
+        p.nzero = (int)nc;
+    }
     install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
     PBD_LAUNCH_CHECK();
     count_launch(1);
