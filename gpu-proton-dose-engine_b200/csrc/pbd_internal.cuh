@@ -59,7 +59,8 @@ constexpr int kSpotChunk = 64;      // spots per lattice chunk in the FP32 forwa
 constexpr int kAdjMaxSpots = 64;    // adjoint lattice limit per axis
 constexpr int kMaxChunkCost = 64;   // largest layers-per-item / z-per-item
 constexpr int kLossBlocks = 296;    // fixed grid of the loss reduction (deterministic order)
-constexpr int kLossBlocks16 = 1184; // the same for the split-FP16 forward's finalize (8 per SM)
+constexpr int kLossBlocks16 = 592;  // the same for the split-FP16 forward's finalize (4 per SM:
+                                    // one wave at its 64 registers per thread)
 constexpr int kTcAdjChunk = 4;      // default active layers per tensor-core adjoint unit
                                     // (4 measured best on the 128^3 / 41 x 41 x 40 field)
 constexpr int kTcFwdWarps = 8;      // math warps of the tensor-core forward: each owns 32 rows x

@@ -858,6 +858,8 @@ __global__ void __launch_bounds__(kThreads, 1) fwd_tc16_kernel(Params P) {
 // partial slices in chunk order (or the dose itself, direct), NaN when a wait of the forward ran
 // out; with the loss, dL/dD = 2 m (D - P) and per-block FP64 partial sums of m (D - P)^2 in a
 // fixed order.  Four voxels per thread per step when every slice plane is a multiple of four.
+constexpr int kFinMaxZ = 1024;   // slices whose partial-slice counts the finalize stages
+
 __global__ void __launch_bounds__(256) fwd16_finalize_kernel(const JobDev* __restrict__ jobs,
                                                              int with_loss,
                                                              const int* __restrict__ err) {
@@ -913,7 +915,62 @@ __global__ void __launch_bounds__(256) fwd16_finalize_kernel(const JobDev* __res
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t nthr = (size_t)gridDim.x * blockDim.x;
     if ((plane & 3) == 0) {
-        for (size_t v = 4 * tid; v < n; v += 4 * nthr) voxel4(v, 4);
+        // Four voxels of one slice per group, two groups per step: the slices' partial-slice
+        // counts are staged in shared memory and the mask and prescription loads issued first,
+        // so that a step waits on one round of loads (the partial slices).  Sums in piece order,
+        // the loss in group order: deterministic.
+        __shared__ int s_nch[kFinMaxZ];
+        const bool stage = !J.direct && J.nz <= kFinMaxZ;
+        if (stage)
+            for (int z = threadIdx.x; z < J.nz; z += blockDim.x) s_nch[z] = J.nchunks[z];
+        __syncthreads();
+        auto nch_of = [&](size_t v) -> int {
+            if (J.direct) return 1;
+            const int z = (int)(v / plane);
+            return stage ? s_nch[z] : J.nchunks[z];
+        };
+        const float* src = J.direct ? J.dose : J.partial;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        auto finish = [&](size_t v, float4 s, float4 m, float4 pr) {
+            if (bad) s = make_float4(nan, nan, nan, nan);
+            if (!J.direct || bad) *reinterpret_cast<float4*>(J.dose + v) = s;
+            if (with_loss) {
+                const float r0 = s.x - pr.x, r1 = s.y - pr.y, r2 = s.z - pr.z, r3 = s.w - pr.w;
+                lsum += (double)m.x * (double)r0 * (double)r0;
+                lsum += (double)m.y * (double)r1 * (double)r1;
+                lsum += (double)m.z * (double)r2 * (double)r2;
+                lsum += (double)m.w * (double)r3 * (double)r3;
+                *reinterpret_cast<float4*>(J.grad_dose + v) =
+                    make_float4(2.f * m.x * r0, 2.f * m.y * r1, 2.f * m.z * r2, 2.f * m.w * r3);
+            }
+        };
+        for (size_t va = 4 * tid; va < n; va += 8 * nthr) {
+            const size_t vb = va + 4 * nthr;
+            const bool hb = vb < n;
+            float4 ma = zero4, pa = zero4, mb = zero4, pb = zero4;
+            if (with_loss) {
+                ma = __ldcs(reinterpret_cast<const float4*>(J.mask + va));
+                pa = __ldcs(reinterpret_cast<const float4*>(J.presc + va));
+                if (hb) {
+                    mb = __ldcs(reinterpret_cast<const float4*>(J.mask + vb));
+                    pb = __ldcs(reinterpret_cast<const float4*>(J.presc + vb));
+                }
+            }
+            const int na = nch_of(va), nb = hb ? nch_of(vb) : 0;
+            float4 sa = zero4, sb = zero4;
+            for (int k = 0; k < na || k < nb; ++k) {
+                if (k < na) {
+                    const float4 a = __ldcs(reinterpret_cast<const float4*>(src + (size_t)k * n + va));
+                    sa.x += a.x; sa.y += a.y; sa.z += a.z; sa.w += a.w;
+                }
+                if (k < nb) {
+                    const float4 b = __ldcs(reinterpret_cast<const float4*>(src + (size_t)k * n + vb));
+                    sb.x += b.x; sb.y += b.y; sb.z += b.z; sb.w += b.w;
+                }
+            }
+            finish(va, sa, ma, pa);
+            if (hb) finish(vb, sb, mb, pb);
+        }
     } else {
         for (size_t v = tid; v < n; v += nthr) voxel4(v, 1);
     }
@@ -1043,7 +1100,8 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
             maxn = std::max(maxn, (size_t)jobs_host[j].nx * jobs_host[j].ny * jobs_host[j].nz);
         // kLossBlocks16 blocks with the loss (the adjoint sums that many partials per job)
         const int blocks = with_loss ? kLossBlocks16
-                                     : (int)std::min<size_t>((maxn / 4 + 255) / 256, 4096);
+                                     : (int)std::min<size_t>((maxn / 8 + 255) / 256,
+                                                             (size_t)num_sms() * 4);
         PBD_TRY(launch_dependent(fwd16_finalize_kernel, dim3(std::max(blocks, 1), n_jobs), dim3(256),
                                  0, s, (const JobDev*)jobs_dev, with_loss, (const int*)err));
         count_launch(1);
