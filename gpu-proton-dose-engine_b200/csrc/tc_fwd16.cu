@@ -19,9 +19,9 @@
 // operand's scale.  kind::f16 takes K = 16 per MMA (twice TF32's 8) at twice the TF32 rate.
 //
 // CTA = 8 math warps, 1 scheduler / producer warp, 3 MMA warps; one CTA per SM (persistent).
-//  * Scheduler warp: units (slice z, piece c, tile) from an atomic counter in z-major order, a
-//    slice's n active layers cut into ceil(n / C) pieces of equal size; per unit the scale
-//    exponent; one step per active layer into an 8-deep ring.  As producer it also brings each step's spot map into a shared-memory ring
+//  * Scheduler warp: units (slice z, chunk c of <= C active layers, tile) from an atomic
+//    counter in z-major order (the shallow slices, which see the most layers, first); per unit
+//    the scale exponent; one step per active layer into an 8-deep ring.  As producer it also brings each step's spot map into a shared-memory ring
 //    with one bulk copy (cp.async.bulk, mbarrier transaction count): the maps are packed once
 //    per call by pack_w16_kernel into the exact operand image (hi rows then lo rows, K-major
 //    8 x 16-byte core matrices), so the math warps never load W.
@@ -314,9 +314,7 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, uint8_t* smem, S
                 continue;
             }
             if (c >= nch) continue;
-            // nch pieces of equal size (within one layer) rather than chunk-sized ones and a
-            // remainder: the largest unit, which bounds the balance, is as small as nch allows
-            const int r0 = (int)((long long)c * tot / nch), r1 = (int)((long long)(c + 1) * tot / nch);
+            const int r0 = c * P.chunk, r1 = min(tot, r0 + P.chunk);
             // the unit's scale exponent: the smallest over its layers of
             // 14 - ceil(log2(bound on |s U|)), so that every s U of the unit fits FP16
             int ks = 127;
