@@ -93,6 +93,14 @@ struct Params {
     uint32_t o_stage;    // its shared-memory offset
     int sym;             // 1: every job is symmetric in x and y (grid, lattice, origins), so the
                          //    stage-2 operand [Gx | Gx'] equals the [Gy | Gy'] rows G evaluates
+    int adapt;           // 1 (one job, no explicit schedule): every CTA counts the active pairs T
+                         //    and uses units of ceil(T / grid) + 1 layers (chunk, cmax, n_units
+                         //    then describe that unit size)
+};
+
+// The adjoint's unit decomposition in force (P's, or the one the CTA derived).
+struct Units {
+    int chunk, cmax, n_units;
 };
 
 struct Layout {
@@ -139,9 +147,9 @@ __device__ __forceinline__ void split8(const float* v, uint4& hi, uint4& lo) {
 // ------------------------------------------------------------------------------------------
 // Scheduler warp: units (z, chunk) -> one step per active layer.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint64_t* full,
-                                               uint64_t* empty, uint8_t* smem, uint64_t* sfull,
-                                               uint64_t* sfree) {
+__device__ __forceinline__ void scheduler_warp(const Params& P, const Units U, Step* ring,
+                                               uint64_t* full, uint64_t* empty, uint8_t* smem,
+                                               uint64_t* sfull, uint64_t* sfree) {
     const int lane = threadIdx.x & 31;
     const unsigned FULL = 0xffffffffu;
     int k = 0, nu = 0;       // ring pushes; units whose slice was copied into the staging buffer
@@ -164,11 +172,11 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
         int u = 0;
         if (lane == 0) u = atomicAdd(P.counter, 1);
         u = __shfl_sync(FULL, u, 0);
-        if (u >= P.n_units) break;
+        if (u >= U.n_units) break;
         int v = u;
         const int job = v % P.n_jobs; v /= P.n_jobs;
-        const int c = v % P.cmax;
-        const int z = v / P.cmax;
+        const int c = v % U.cmax;
+        const int z = v / U.cmax;
         const JobDev& J = P.jobs[job];
         const int nz = J.nz, nl = J.nl;
         if (z >= nz) continue;
@@ -179,9 +187,9 @@ __device__ __forceinline__ void scheduler_warp(const Params& P, Step* ring, uint
             const bool a = l < nl && idd[(size_t)l * nz + z] != 0.0;
             tot += __popc(__ballot_sync(FULL, a));
         }
-        const int r0 = c * P.chunk;
+        const int r0 = c * U.chunk;
         if (r0 >= tot) continue;   // no chunk c here (slices no layer reaches carry no gradient)
-        const int r1 = min(tot, r0 + P.chunk);
+        const int r1 = min(tot, r0 + U.chunk);
         if (P.stage) {
             // the unit's dL/dD slice into the staging buffer, once the math warps have converted
             // the previous unit's copy
@@ -667,11 +675,38 @@ __global__ void __launch_bounds__(kThreads, 1) adj_tc_kernel(Params P) {
     // the reduce (a programmatic dependent) may be scheduled onto the SMs this grid frees; one
     // CTA per SM here, so it takes no SM that a CTA of this grid still needs
     asm volatile("griddepcontrol.launch_dependents;");
+    // Units: the largest unit bounds the balance of the persistent grid (a slice with exactly
+    // C active layers is one unit, claimed late), so units just above the mean load per CTA,
+    // ceil(T / grid) + 1 layers, balance best (a scheduling model and measurements agree); the
+    // job views are visible from here on.
+    __shared__ Units s_units;
+    __shared__ int s_pairs;
+    Units U{P.chunk, P.cmax, P.n_units};
+    if (P.adapt) {
+        if (threadIdx.x == 0) s_pairs = 0;
+        __syncthreads();
+        const JobDev& J = P.jobs[0];
+        const int ne = J.nz * J.nl;
+        int cnt = 0;
+        for (int e = threadIdx.x; e < ne; e += kThreads) cnt += J.idd[e] != 0.0 ? 1 : 0;
+        cnt = __reduce_add_sync(0xffffffffu, cnt);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&s_pairs, cnt);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int g = (int)gridDim.x;
+            int c = (s_pairs + g - 1) / g + 1;
+            c = c < 1 ? 1 : (c > kMaxChunkCost ? kMaxChunkCost : c);
+            const int cm = (J.nl + c - 1) / c;
+            s_units = Units{c, cm, J.nz * cm};
+        }
+        __syncthreads();
+        U = s_units;
+    }
 
     if (warp >= kMathWarps) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtrlRegs));
         if (warp == kSchedWarp) {
-            scheduler_warp(P, ring, full, empty, smem, &sbars[0], &sbars[1]);
+            scheduler_warp(P, U, ring, full, empty, smem, &sbars[0], &sbars[1]);
         } else if (warp == kS1Warp || warp == kS2Warp) {
             const Layout L = make_layout<NARR>(P.N1);
             mma_warp<MODE>(P, L, tc::smem_u32(smem), tmem_base_s, warp == kS1Warp ? 1 : 2, ring,
@@ -907,6 +942,8 @@ int launch_adjoint_tc(int precision, JobDev* jobs_dev, const JobDev* jobs_host, 
         max_per = std::max(max_per, jobs_host[j].nsy * ((jobs_host[j].nsx + 15) / 16 * 16));
     }
     P.cmax = cm;
+    // one job and no explicit schedule: the CTAs derive the unit size from the active pairs
+    P.adapt = (n_jobs == 1 && schedule_adj_override() == 0) ? 1 : 0;
     P.sym = 1;
     for (int j = 0; j < n_jobs; ++j) {
         const JobDev& J = jobs_host[j];

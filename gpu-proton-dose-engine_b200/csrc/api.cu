@@ -302,6 +302,8 @@ int smem_optin(const void* fn, int bytes, int min_regs, int* set_bytes) {
 unsigned long long wait_limit_ns() { return g_wait_ns ? g_wait_ns : 2000000000ull; }
 int test_hold() { return g_hold; }
 
+int schedule_adj_override() { return g_adj_chunk; }
+
 int num_sms() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;

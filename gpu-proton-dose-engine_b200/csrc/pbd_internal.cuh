@@ -187,6 +187,8 @@ int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_job
 // warps' dot-product partials of every pair (tc_adjoint_slot_elems); counter[0] = unit
 // counter, counter[1] unused; `err` = the error word (cleared by the caller).
 int tc_adjoint_dims(int precision, const pbd_field* f, int* N1);
+// The calling thread's explicit adjoint item size (pbd_set_schedule), 0 when none is set.
+int schedule_adj_override();
 size_t tc_adjoint_slot_elems(const pbd_field* f);
 // Ints of the adjoint's counter block (the unit counter and one unused word, for any number of
 // jobs and layers).
