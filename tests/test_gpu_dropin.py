@@ -192,3 +192,26 @@ def test_timeout_status_and_recovery(pb, prec):
     assert torch.equal(gw_again, gw_good)
     if prec == "tf32x3":
         assert rel(again.cpu().numpy(), ref) < F32_TOL
+
+
+def test_adjoint_unit_size_leaves_the_gradient_bit_identical(pb):
+    """The single-job tensor-core adjoint derives its unit size on the device from the active
+    pairs (20 layers on the clinical field).  A pair's products do not depend on the unit that
+    carries it, and the reduce sums in a fixed order, so dL/dW, dL/dR and the loss equal, bit for
+    bit, those of explicit unit sizes (4 and 9 layers), with the forward unchanged."""
+    import torch
+    wl = pb.workloads.build_workload(2)
+    prob = pb.model.problem_from_workload(wl)
+    m = torch.as_tensor(wl["mask"], device="cuda")
+    p = torch.as_tensor(wl["presc"], device="cuda")
+    outs = {}
+    for sched in (None, (20, 4), (20, 9)):
+        plan = pb.engines.DosePlan(prob, tables="device", precision="fp16x3")
+        plan.schedule = sched
+        o = plan.loss_grad(m, p)
+        torch.cuda.synchronize()
+        outs[sched] = {k: v.clone() for k, v in o.items() if torch.is_tensor(v)}
+    base = outs[None]
+    for sched in ((20, 4), (20, 9)):
+        for k in ("grad_w", "grad_range", "loss"):
+            assert torch.equal(outs[sched][k], base[k]), (sched, k)
