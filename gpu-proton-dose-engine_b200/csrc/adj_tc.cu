@@ -475,7 +475,7 @@ __device__ __forceinline__ void math_warps(const Params& P, const Layout& L, uin
                 if (!__all_sync(0xffffffffu, ok)) break;
                 g = reinterpret_cast<const float*>(smem + P.o_stage);
             }
-#pragma unroll 2
+#pragma unroll 1
             for (int r = 0; r < 8; ++r) {
                 const int e = tid + r * kMath;
                 const int x = e & 127, c = e >> 7;

@@ -585,7 +585,7 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
             const double cx = 0.5 * (double)(J.nsx - 1), cy = 0.5 * (double)(J.nsy - 1);
             const double yv = J.oy + (double)(ty * kTile + grow) * J.dy;
             const double xv = J.ox + (double)(tx * kTile + grow) * J.dx;
-#pragma unroll
+#pragma unroll 1
             for (int r = 0; r < kMaxR; ++r) {
                 const int g = ghalf + 2 * r;
                 if (r < N1 / 16) {
@@ -616,7 +616,7 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
         uint8_t* a2h = smem + P.oA2 + (uint32_t)ia2 * 2u * aBytes2;
         uint8_t* a1h = smem + P.oA1 + (uint32_t)ia * 2u * aBytes1;
         auto operand = [&](int tab0, int nc, uint8_t* dst, uint32_t lo_off) {
-#pragma unroll
+#pragma unroll 1
             for (int r = 0; r < kMaxR; ++r) {
                 if (r < nc) {
                     const float4 p = tab[(tab0 + 2 * r) * kMath + tid];
