@@ -644,12 +644,14 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
     };
 
     // E1: U of step m from TMEM, times f1, split -> B2[m % nB2] (x rows, K = j).
-    auto e1 = [&](const Step& st, int m) -> bool {
+    // E1 in two parts: the TMEM loads of U are issued before the next step's G, which hides
+    // their latency, and waited for after it (G issues no TMEM load of its own).
+    const int ncol = N1 / 2, c0 = half * ncol;   // this warp's columns j: multiple of 8
+    uint32_t rb[4][8], rc[4][8];
+    auto e1_issue = [&](int m) -> bool {
         bool w = wait_bar(B.uf, (uint32_t)(m & 1), P.wait_ns);
         if (!__all_sync(0xffffffffu, w)) return false;
         tc::fence_after_sync();
-        const int ncol = N1 / 2, c0 = half * ncol;   // this warp's columns j: multiple of 8
-        uint32_t rb[4][8], rc[4][8];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             if (q * 8 < ncol) {
@@ -657,6 +659,10 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
                 tc::tmem_ld8(tb + kColU + lane_base + (uint32_t)(N1 + c0 + 8 * q), rc[q]);
             }
         }
+        return true;
+    };
+    auto e1 = [&](const Step& st, int m) -> bool {
+        bool w = true;
         tc::tmem_wait_ld();
         tc::fence_before_sync();
         __syncwarp();
@@ -755,9 +761,16 @@ __device__ __forceinline__ void math_warps(const Params& P, uint8_t* smem, uint3
                 have = true;
             }
         }
+        if (p1) {
+            ok = e1_issue(i1);
+            if (!ok) break;
+        }
         if (have) {
             ok = gen(cur, ng);
-            if (!ok) break;
+            if (!ok) {
+                tc::tmem_wait_ld();   // the E1 loads in flight land before the kernel leaves
+                break;
+            }
         }
         if (p1) {
             ok = e1(s1, i1);
