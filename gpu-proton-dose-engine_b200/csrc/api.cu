@@ -206,7 +206,7 @@ struct Ws {
     int* anch;
     void* pack;          // split-FP16 forward: packed spot maps
     size_t pack_bytes;
-    int* acnt;           // tensor-core adjoint: unit counter, error word, per-layer counters
+    int* acnt;           // tensor-core adjoint: its counter block (unit counter)
     float* apart;
     float* dc;
     float* dsg;
@@ -249,7 +249,8 @@ int carve_ws(const pbd_field* f, bool fwd, bool adj, bool loss, int precision, v
         size_t pe = 0;
         int n1 = 0;
         if (tc_adjoint_dims(precision, f, &n1) == PBD_OK) {
-            // tensor-core adjoint: (slice, layer-chunk) units, two slots per (layer, slice)
+            // tensor-core adjoint: (slice, layer-chunk) units, one slot and the warps' dot
+            // products per active (layer, slice)
             w.adj_tc = 1;
             w.a_chunk = g_adj_chunk > 0 ? w.a_chunk : kTcAdjChunk;
             pe = tc_adjoint_slot_elems(f);
