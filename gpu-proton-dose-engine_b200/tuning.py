@@ -19,8 +19,11 @@ import threading
 
 from . import _lib
 
-CANDIDATES_FWD = (8, 16, 24, 32)
-CANDIDATES_ADJ = (2, 4, 8, 16)
+# 0 = the library's default: 20 forward layers per unit (split FP16), and for one job the
+# adjoint's unit size derived on the device from the active pairs (ceil(T / grid) + 1); an
+# explicit adjoint size switches that derivation off, so 0 stays a candidate.
+CANDIDATES_FWD = (0, 12, 16, 24, 32)
+CANDIDATES_ADJ = (0, 4, 8, 10)
 _lock = threading.Lock()
 
 
