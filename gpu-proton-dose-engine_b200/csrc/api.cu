@@ -21,13 +21,6 @@ namespace {
 thread_local int g_fwd_chunk = 0;   // 0 = default
 thread_local int g_adj_chunk = 0;
 
-struct JobPair {
-    JobDev j[2];
-    int n;
-    int nzero;           // ints of `zero` to clear (<= 32), e.g. the adjoint's counter block
-    int* zero;
-};
-
 // Installs the call's job views and clears its status header (may be null) and p.zero.
 __global__ void install_jobs_kernel(JobPair p, JobDev* dst, int* status) {
     if ((int)threadIdx.x < p.n) dst[threadIdx.x] = p.j[threadIdx.x];
@@ -581,12 +574,16 @@ int pbd_forward(const pbd_field* f, const float* w, const double* idd, const dou
     J.max_chunks = (f->n_layers + ws.f_chunk - 1) / ws.f_chunk;
     J.item_base = 0; J.max_items = ws.f_items;
     J.partial = ws.fpart; J.nchunks = ws.fnch; J.arrive = ws.farr;
-    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
-    PBD_LAUNCH_CHECK();
-    count_launch(1);
+    // split FP16: the pack kernel installs the views (one launch fewer before the dose kernel)
+    const bool merged = precision == PBD_PREC_FP16X3;
+    if (!merged) {
+        install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    }
     return launch_forward(ws.jobs, &J, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
                           ws.status + kStatFwd, ws.f_chunk, 0, precision, 1, ws.pack,
-                          ws.pack_bytes, s);
+                          ws.pack_bytes, s, merged ? &p : nullptr, ws.jobs, ws.status);
 }
 
 // err: the adjoint's error word (the workspace's own status word unless a caller passes its
@@ -712,12 +709,16 @@ int pbd_loss_grad(const pbd_field* f, const float* w, const double* idd, const d
         p.zero = ws.acnt;
         p.nzero = (int)nc;
     }
-    install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
-    PBD_LAUNCH_CHECK();
-    count_launch(1);
+    // split FP16: the pack kernel installs the views (one launch fewer before the dose kernel)
+    const bool merged = precision == PBD_PREC_FP16X3;
+    if (!merged) {
+        install_jobs_kernel<<<1, 32, 0, s>>>(p, ws.jobs, ws.status);
+        PBD_LAUNCH_CHECK();
+        count_launch(1);
+    }
     PBD_TRY(launch_forward(ws.jobs, &F, 1, ws.fitems, ws.f_items, ws.counters, ws.n_fcount,
                            ws.status + kStatFwd, ws.f_chunk, 1, precision, 0, ws.pack,
-                           ws.pack_bytes, s));
+                           ws.pack_bytes, s, merged ? &p : nullptr, ws.jobs, ws.status));
     return run_adjoint(ws, precision, &A, with_range, 1, ws.adj_tc, ws.status + kStatAdj, s);
 }
 

@@ -295,13 +295,16 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
                    int total_items, int* counter, size_t n_counter_ints, int* err, int chunk,
                    int with_loss, int precision, int poison, void* pack, size_t pack_bytes,
-                   cudaStream_t s) {
+                   cudaStream_t s, const JobPair* inst, JobDev* inst_dst, int* inst_status) {
+    const bool tc16 = precision == PBD_PREC_FP16X3 && jobs_host[0].layer_stride == 0;
+    if (inst && !tc16) return PBD_ERR_UNSUPPORTED;   // only the split-FP16 pack installs views
     if (precision != PBD_PREC_FP32) {
         // the split-FP16 path clears its unit counter in its pack kernel (no memset node between
-        // the job install and the dose kernels)
-        if (precision == PBD_PREC_FP16X3 && jobs_host[0].layer_stride == 0)
+        // the job install and the dose kernels) and may install the job views there too
+        if (tc16)
             return launch_forward_tc16(jobs_dev, jobs_host, n_jobs, counter, err, chunk,
-                                       with_loss, poison, pack, pack_bytes, s);
+                                       with_loss, poison, pack, pack_bytes, s, inst, inst_dst,
+                                       inst_status);
         PBD_TRY(cuda_rc(cudaMemsetAsync(counter, 0, n_counter_ints * sizeof(int), s)));
         return launch_forward_tc(precision, jobs_dev, jobs_host, n_jobs, counter, err, chunk,
                                  with_loss, poison, s);

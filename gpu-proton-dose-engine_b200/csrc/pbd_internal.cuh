@@ -51,6 +51,15 @@ struct JobDev {
                                   // the dose itself)
 };
 
+// A call's job views, installed into the device array by the call's first kernel (which also
+// clears the status header and `zero`).
+struct JobPair {
+    JobDev j[2];
+    int n;
+    int nzero;           // ints of `zero` to clear (<= 32), e.g. the adjoint's counter block
+    int* zero;
+};
+
 struct FwdItem { int job, z, ty, tx, lb, le, chunk, cost; };
 struct AdjItem { int job, l, zb, ze, chunk, cost, pad0, pad1; };
 
@@ -177,7 +186,8 @@ int fwd_plan_sizes(const pbd_field* f, int chunk, size_t* partial_elems, int* it
 int launch_forward(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, FwdItem* items,
                    int total_items, int* counter, size_t n_counter_ints, int* err, int chunk,
                    int with_loss, int precision, int poison, void* pack, size_t pack_bytes,
-                   cudaStream_t s);
+                   cudaStream_t s, const JobPair* inst = nullptr,
+                   JobDev* inst_dst = nullptr, int* inst_status = nullptr);
 
 // (slice, tile, layer-chunk) work items sorted longest-first, one CTA per job.
 int launch_slice_schedule(JobDev* jobs_dev, FwdItem* items, int chunk, int n_jobs, cudaStream_t s);
@@ -220,7 +230,8 @@ int launch_forward_f64(const pbd_field* f, const double* w, const double* idd,
 size_t tc16_pack_bytes(int n_jobs, int max_layers, int nsx, int nsy);
 int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, int* counter,
                         int* err, int chunk, int with_loss, int poison, void* pack,
-                        size_t pack_bytes, cudaStream_t s);
+                        size_t pack_bytes, cudaStream_t s, const JobPair* inst = nullptr,
+                        JobDev* inst_dst = nullptr, int* inst_status = nullptr);
 
 // adjoint (FP32 SIMT) -- adj_simt.cu
 int adj_chunk_depths(const pbd_field* f);

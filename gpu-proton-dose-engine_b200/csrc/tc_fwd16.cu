@@ -49,6 +49,7 @@
 #include <algorithm>
 #include <cuda_fp16.h>
 #include <math.h>
+#include <string.h>
 
 #include "pbd_internal.cuh"
 #include "tc_common.cuh"
@@ -148,14 +149,26 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
 __global__ void __launch_bounds__(256) pack_w16_kernel(const JobDev* __restrict__ jobs, int K1,
                                                        int N1, int lmax, uint32_t img,
                                                        uint8_t* wpack, float* wmax, int* wexp,
-                                                       int* unit_counter) {
+                                                       int* unit_counter, JobPair inst,
+                                                       int has_inst, JobDev* inst_dst,
+                                                       int* inst_status) {
     // the dose kernel (a programmatic dependent) may start its prologue now; it reads the packed
-    // maps and the unit counter only after griddepcontrol.wait, i.e. after this grid has completed
+    // maps, the unit counter and the job views only after griddepcontrol.wait, i.e. after this
+    // grid has completed
     asm volatile("griddepcontrol.launch_dependents;");
-    // launched as a programmatic dependent of the job install: its job views are visible after this
+    // launched as a programmatic dependent of the kernel before it (the job install, or the
+    // previous call's last kernel when this grid installs the views itself)
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *unit_counter = 0;
-    const JobDev& J = jobs[blockIdx.y];
+    if (blockIdx.x == 0 && blockIdx.y == 0) {
+        if (threadIdx.x == 0) *unit_counter = 0;
+        if (has_inst) {
+            // the call's job views, status header and cleared counters (install_jobs_kernel's work)
+            if ((int)threadIdx.x < inst.n) inst_dst[threadIdx.x] = inst.j[threadIdx.x];
+            if (inst_status && (int)threadIdx.x < kStatusInts) inst_status[threadIdx.x] = 0;
+            if (inst.zero && (int)threadIdx.x < inst.nzero) inst.zero[threadIdx.x] = 0;
+        }
+    }
+    const JobDev& J = has_inst ? inst.j[blockIdx.y] : jobs[blockIdx.y];
     const int l = blockIdx.x;
     if (l >= J.nl) return;
     const int nsx = J.nsx, nsy = J.nsy, per = nsx * nsy;   // <= 64 x 64
@@ -1047,7 +1060,8 @@ size_t tc16_pack_bytes(int n_jobs, int max_layers, int nsx, int nsy) {
 
 int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, int* counter,
                         int* err, int chunk, int with_loss, int poison, void* pack,
-                        size_t pack_bytes, cudaStream_t s) {
+                        size_t pack_bytes, cudaStream_t s,
+                        const JobPair* inst, JobDev* inst_dst, int* inst_status) {
     Params P{};
     P.jobs = jobs_dev;
     P.n_jobs = n_jobs;
@@ -1096,9 +1110,16 @@ int launch_forward_tc16(JobDev* jobs_dev, const JobDev* jobs_host, int n_jobs, i
     // >= 116 KiB: one CTA (and its 512 TMEM columns) per SM
     const size_t smem = std::max<size_t>(pl.total, 116u * 1024u);
     if (smem > (size_t)max_dyn) return PBD_ERR_NO_SMEM;
+    JobPair ip;
+    memset(&ip, 0, sizeof(ip));
+    if (inst) {
+        if (n_jobs > inst->n || inst->n > 2) return PBD_ERR_UNSUPPORTED;
+        ip = *inst;
+    }
     PBD_TRY(launch_dependent(pack_w16_kernel, dim3(lmax, n_jobs), dim3(256), 0, s,
                              (const JobDev*)jobs_dev, P.K1, P.N1, lmax, P.img,
-                             const_cast<uint8_t*>(P.wpack), wmax, wexp, counter));
+                             const_cast<uint8_t*>(P.wpack), wmax, wexp, counter, ip,
+                             inst ? 1 : 0, inst_dst, inst_status));
     const int grid = std::max(1, std::min(P.n_units, num_sms()));
     prof_mark(kProfFwd, 0, s);
     PBD_TRY(launch_dependent(fwd_tc16_kernel, dim3(grid), dim3(kThreads), smem, s, P));
