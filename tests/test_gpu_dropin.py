@@ -14,7 +14,7 @@
 * Bounded device waits: with the schedulers held (test hook) every wait runs out, the call's
   outputs are NaN and the status query reports PBD_ERR_TIMEOUT; the next call is correct.
 
-Tolerances: float32 doses 1e-6 of max, float64 doses 1e-12.
+Tolerances: float32 doses 1e-6 of max (the accuracy bound for FP32 and split forms), float64 doses 1e-12.
 """
 import ctypes
 from types import SimpleNamespace

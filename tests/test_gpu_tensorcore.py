@@ -1,7 +1,7 @@
 """Tensor-core (tcgen05) forward against the float64 oracle, every precision mode.
 
 Tolerances (max |dD| / max D against float64):
-  tf32x3, fp16x3:    1e-6   -- the north-star bound for the split forms
+  tf32x3, fp16x3:    1e-6   -- the accuracy bound for the split forms
   bf16x3:            5e-5   -- reported; the split with bf16 parts keeps ~16 mantissa bits
   tf32:              5e-3   -- one TF32 product (10-bit mantissa)
   bf16:              5e-2   -- one BF16 product (7-bit mantissa)
@@ -216,7 +216,7 @@ def test_loss_grad_graph_replay_matches_eager(pb):
 # ----------------------------------------------------------------------- precision study
 # The 200x200x256 / 61x61x60 field (1 mm voxels, 223,260 beams) in every precision mode
 # against the float64 oracle fed the reference's own tables (luts_cfg4.npz).  Bounds: FP32
-# and TF32x3 at the north-star 1e-6 of max; the reduced modes pinned at ~5x their measured
+# and TF32x3 at the 1e-6-of-max accuracy bound; the reduced modes pinned at ~5x their measured
 # error (BF16x3 2.0e-6, TF32 2.7e-4, BF16 2.1e-3); the FP64 kernel at 1e-12.
 CFG4_TOL = {"fp32": 1e-6, "tf32x3": 1e-6, "fp16x3": 1e-6, "bf16x3": 1e-5, "tf32": 1e-3,
             "bf16": 1e-2}
