@@ -70,8 +70,9 @@ constexpr int kMaxChunkCost = 64;   // largest layers-per-item / z-per-item
 constexpr int kLossBlocks = 296;    // fixed grid of the loss reduction (deterministic order)
 constexpr int kLossBlocks16 = 592;  // the same for the split-FP16 forward's finalize (4 per SM:
                                     // one wave at its 64 registers per thread)
-constexpr int kTcAdjChunk = 4;      // default active layers per tensor-core adjoint unit
-                                    // (4 measured best on the 128^3 / 41 x 41 x 40 field)
+constexpr int kTcAdjChunk = 4;      // host unit size of the single-job tensor-core adjoint: it
+                                    // sizes the grid (min(units, SMs)); with no explicit schedule
+                                    // the CTAs then use ceil(active pairs / grid) + 1 layers
 constexpr int kTcFwdWarps = 8;      // math warps of the tensor-core forward: each owns 32 rows x
                                     // 64 columns of a tile, its own arrival counter and loss partial
 
