@@ -915,21 +915,17 @@ def main():
     launches = int(round(launches_per_eval * K))
 
     # ---- end to end through the public API, host buffers (pinned) ----
+    # grad_w, grad_range and loss in one packed buffer on each side: one download per step
     w_host = torch.tensor(wl["weights"], dtype=torch.float32).pin_memory()
-    gw_host = torch.empty_like(w_host).pin_memory()
-    gr_host = torch.empty(wl["n_layers"], dtype=torch.float32).pin_memory()
-    loss_host = torch.empty((), dtype=torch.float64).pin_memory()
+    host_res = plan.alloc_host_results()
+    out_p = plan.alloc_outputs(packed=True)
 
     def eager_e2e():
-        o = plan.loss_grad(m, p, w=w_host, outputs=out)
-        gw_host.copy_(o["grad_w"], non_blocking=True)
-        gr_host.copy_(o["grad_range"], non_blocking=True)
-        loss_host.copy_(o["loss"], non_blocking=True)
+        plan.loss_grad(m, p, w=w_host, outputs=out_p)
+        host_res["packed"].copy_(out_p["packed"], non_blocking=True)
 
     t2_eager = timed(eager_e2e)
-    g_e2e = pb.engines.LossGradGraph(plan, m, p, host_w=w_host,
-                                     host_out={"grad_w": gw_host, "grad_range": gr_host,
-                                               "loss": loss_host})
+    g_e2e = pb.engines.LossGradGraph(plan, m, p, host_w=w_host, host_out=host_res)
     for _ in range(max(args.warmup, 3)):
         g_e2e.replay()
     t2 = timed(g_e2e.replay)
@@ -957,7 +953,7 @@ def main():
     clk = clocks.stop()
     e2e = world * K / (t2 * 1e-3)
     h2d = w_host.numel() * 4
-    d2h = gw_host.numel() * 4 + gr_host.numel() * 4 + 8
+    d2h = host_res["packed"].numel()   # the packed span: grad_w, grad_range, loss and padding
 
     # ---- roofline of the dominant kernel ----
     pk, pk_src = peaks()
@@ -1001,7 +997,8 @@ def main():
                        "parallelism": f"{world} independent evaluations (one per rank)"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "how": "DosePlan loss gradient replayed from a "
-                    "CUDA graph that uploads the weights and downloads dL/dW, dL/dR and L"},
+                    "CUDA graph that uploads the weights and downloads dL/dW, dL/dR and L "
+                    "(one packed copy)"},
             "eager": {"value": world * K / (t_eager * 1e-3),
                       "e2e": world * K / (t2_eager * 1e-3),
                       "how": "one DosePlan.loss_grad call per step (host work per call)"},

@@ -36,6 +36,35 @@ def resolve_precision(precision, lattice) -> int:
     return _lib.precision_code(precision)
 DEFAULT_FD_STEP = 0.005   # cm: central-difference step of the range-derivative tables
 
+# The loss gradient's small results, in the order they sit in one packed buffer.
+PACKED_RESULTS = ("grad_w", "grad_range", "loss")
+
+
+def packed_result_layout(n_weights: int, n_layers: int):
+    """Byte offsets and sizes of grad_w (float32), grad_range (float32) and loss (float64)
+    in one packed buffer, each at a 256-byte boundary, and the bytes that span them: a single
+    copy of that span moves all three results between device and host."""
+    sizes = (4 * int(n_weights), 4 * int(n_layers), 8)
+    offs, o = [], 0
+    for n in sizes:
+        offs.append(o)
+        o += (n + 255) // 256 * 256
+    return tuple(offs), sizes, offs[-1] + sizes[-1]
+
+
+def packed_result_views(buf, w_shape, n_layers: int) -> dict:
+    """Typed views of grad_w, grad_range and loss in a uint8 buffer with the packed layout
+    (``buf`` is kept under the key "packed")."""
+    import torch
+    offs, sizes, span = packed_result_layout(int(np.prod(w_shape)), n_layers)
+    if buf.dtype != torch.uint8 or buf.dim() != 1 or buf.numel() < span:
+        raise ValueError(f"packed buffer must be a 1-D uint8 tensor of at least {span} bytes")
+    (o0, o1, o2), (n0, n1, n2) = offs, sizes
+    return {"grad_w": buf[o0:o0 + n0].view(torch.float32).view(tuple(w_shape)),
+            "grad_range": buf[o1:o1 + n1].view(torch.float32),
+            "loss": buf[o2:o2 + n2].view(torch.float64).view(()),
+            "packed": buf[:span]}
+
 
 def lateral_kernel(vox_axis, spot_axis, sigma, normalized: bool = True) -> np.ndarray:
     """Host utility with the reference's semantics (engines.py:49-61); not used by the engine,
@@ -302,14 +331,32 @@ class DosePlan:
             o = dict(o, grad_range=None)
         return o
 
-    def alloc_outputs(self):
+    def alloc_outputs(self, packed: bool = False):
+        """Device tensors for ``loss_grad``.  With ``packed``, grad_w, grad_range and loss are
+        views of one buffer (``packed_result_layout``; the buffer is under "packed"), so that
+        one copy downloads all three (see ``alloc_host_results``)."""
         torch = self.torch
         nl = self.w.shape[0]
-        return {"dose": torch.empty(self.shape, dtype=torch.float32, device=self.device),
-                "grad_dose": torch.empty(self.shape, dtype=torch.float32, device=self.device),
-                "loss": torch.zeros((), dtype=torch.float64, device=self.device),
-                "grad_w": torch.empty_like(self.w),
-                "grad_range": torch.zeros(nl, dtype=torch.float32, device=self.device)}
+        out = {"dose": torch.empty(self.shape, dtype=torch.float32, device=self.device),
+               "grad_dose": torch.empty(self.shape, dtype=torch.float32, device=self.device)}
+        if packed:
+            span = packed_result_layout(self.w.numel(), nl)[2]
+            buf = torch.zeros(span, dtype=torch.uint8, device=self.device)
+            out.update(packed_result_views(buf, tuple(self.w.shape), nl))
+        else:
+            out.update({"loss": torch.zeros((), dtype=torch.float64, device=self.device),
+                        "grad_w": torch.empty_like(self.w),
+                        "grad_range": torch.zeros(nl, dtype=torch.float32, device=self.device)})
+        return out
+
+    def alloc_host_results(self) -> dict:
+        """Pinned host tensors grad_w, grad_range and loss in the packed layout of
+        ``alloc_outputs(packed=True)`` (the whole buffer under "packed")."""
+        torch = self.torch
+        nl = self.w.shape[0]
+        span = packed_result_layout(self.w.numel(), nl)[2]
+        buf = torch.zeros(span, dtype=torch.uint8).pin_memory()
+        return packed_result_views(buf, tuple(self.w.shape), nl)
 
 
 class LossGradGraph:
@@ -321,15 +368,30 @@ class LossGradGraph:
     ``host_w`` (a pinned host tensor of the weights' shape) every replay first uploads it,
     and with ``host_out`` (a dict of pinned host tensors keyed like the outputs: any of
     "loss", "grad_w", "grad_range", "dose") every replay ends by downloading those results.
-    ``mask`` and ``presc`` stay referenced; change their contents in place, not the tensors."""
+    The device results sit in one packed buffer; when ``host_out`` comes from
+    ``DosePlan.alloc_host_results`` (its "packed" key), grad_w, grad_range and loss come back
+    in one copy.  ``mask`` and ``presc`` stay referenced; change their contents in place, not
+    the tensors."""
 
     def __init__(self, plan: "DosePlan", mask, presc, host_w=None, host_out=None):
         torch = plan.torch
         self.plan = plan
         self.mask, self.presc = mask, presc
         self.w = plan.w.clone()
-        self.out = plan.alloc_outputs()
+        self.out = plan.alloc_outputs(packed=True)
         self.host_w, self.host_out = host_w, dict(host_out or {})
+        copies = []
+        packed = "packed" in self.host_out
+        if packed:
+            hp = self.host_out["packed"]
+            if hp.numel() != self.out["packed"].numel() or hp.dtype != self.out["packed"].dtype:
+                raise ValueError("host_out['packed'] does not have the packed result layout")
+            copies.append((hp, self.out["packed"]))
+        for k, t in self.host_out.items():
+            if k == "packed" or (packed and k in PACKED_RESULTS):
+                continue   # inside the packed copy
+            copies.append((t, self.out[k]))
+        self._copies = copies
         # first call outside the capture: workspace allocation and schedule lookup
         plan.loss_grad(mask, presc, w=self.w, outputs=self.out)
         torch.cuda.synchronize(plan.device)
@@ -338,8 +400,8 @@ class LossGradGraph:
             if host_w is not None:
                 self.w.copy_(host_w, non_blocking=True)
             plan.loss_grad(mask, presc, w=self.w, outputs=self.out)
-            for k, t in self.host_out.items():
-                t.copy_(self.out[k], non_blocking=True)
+            for dst, src in self._copies:
+                dst.copy_(src, non_blocking=True)
 
     def replay(self):
         """Enqueue one evaluation on the current stream; returns the device outputs."""

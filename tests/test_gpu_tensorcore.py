@@ -189,7 +189,8 @@ def test_tc_adjoint_wide_lattice(pb):
 
 def test_loss_grad_graph_replay_matches_eager(pb):
     """LossGradGraph: the captured loss gradient, with the weight upload and the result
-    download inside the graph, equals an eager call, also after the host weights change."""
+    download inside the graph, equals an eager call, also after the host weights change; with
+    the packed host results (one download for grad_w, grad_range and loss) as well."""
     import torch
     wl = pb.workloads.build_workload(0)
     en = pr.layer_energies(wl["n_layers"], wl["r_min"], wl["r_max"])
@@ -203,14 +204,26 @@ def test_loss_grad_graph_replay_matches_eager(pb):
     loss_host = torch.empty((), dtype=torch.float64).pin_memory()
     g = pb.engines.LossGradGraph(plan, m, p, host_w=w_host,
                                  host_out={"grad_w": gw_host, "loss": loss_host})
+    # the packed host results: grad_w, grad_range and loss downloaded by one copy
+    plan16 = pb.engines.DosePlan(prob, tables="device", precision="fp16x3")
+    w16_host = torch.tensor(wl["weights"], dtype=torch.float32).pin_memory()
+    hres = plan16.alloc_host_results()
+    g16 = pb.engines.LossGradGraph(plan16, m, p, host_w=w16_host, host_out=hres)
+    assert len(g16._copies) == 1
     for scale in (1.0, 1.1):
         w_host.mul_(scale)
+        w16_host.mul_(scale)
         g.replay()
+        g16.replay()
         torch.cuda.synchronize()
         ref = plan.loss_grad(m, p, w=w_host.cuda())
+        ref16 = plan16.loss_grad(m, p, w=w16_host.cuda())
         torch.cuda.synchronize()
         assert rel(gw_host.numpy(), ref["grad_w"].cpu().numpy()) == 0.0
         assert float(loss_host) == float(ref["loss"].item())
+        assert torch.equal(hres["grad_w"], ref16["grad_w"].cpu())
+        assert torch.equal(hres["grad_range"], ref16["grad_range"].cpu())
+        assert float(hres["loss"]) == float(ref16["loss"].item())
 
 
 # ----------------------------------------------------------------------- precision study

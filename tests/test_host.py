@@ -268,6 +268,38 @@ def test_tuning_cache_and_schedule(pb, lib, tmp_path, monkeypatch):
     assert fwd_ws() == base
 
 
+def test_packed_result_layout(pb):
+    """grad_w, grad_range and loss in one buffer: each at a 256-byte boundary, no overlap,
+    typed views that write exactly their own bytes, and a too-small buffer refused."""
+    import torch
+    eng = pb.engines
+    offs, sizes, span = eng.packed_result_layout(41 * 41 * 40, 40)
+    assert all(o % 256 == 0 for o in offs)
+    assert sizes == (4 * 67240, 160, 8)
+    assert all(offs[i] + sizes[i] <= offs[i + 1] for i in range(2))
+    assert span == offs[2] + 8
+    buf = torch.zeros(span, dtype=torch.uint8)
+    v = eng.packed_result_views(buf, (40, 41, 41), 40)
+    assert v["grad_w"].shape == (40, 41, 41) and v["grad_w"].is_contiguous()
+    assert v["grad_range"].shape == (40,) and v["loss"].shape == ()
+    v["grad_w"].fill_(1.0)
+    v["grad_range"].fill_(2.0)
+    v["loss"].fill_(3.0)
+    raw = buf.numpy()
+    assert np.array_equal(raw[offs[0]:offs[0] + sizes[0]].view(np.float32),
+                          np.ones(67240, np.float32))
+    assert np.array_equal(raw[offs[1]:offs[1] + sizes[1]].view(np.float32),
+                          np.full(40, 2.0, np.float32))
+    assert raw[offs[2]:offs[2] + 8].view(np.float64)[0] == 3.0
+    gaps = np.ones(span, bool)
+    for o, n in zip(offs, sizes):
+        gaps[o:o + n] = False
+    assert not raw[gaps].any()
+    assert v["packed"].numel() == span
+    with pytest.raises(ValueError):
+        eng.packed_result_views(torch.zeros(span - 1, dtype=torch.uint8), (40, 41, 41), 40)
+
+
 def test_engine_host_utilities_match_oracle(pb):
     """The reference's host utilities kept in engines.py (lateral_kernel, relative_error,
     normalize_dose, operation_counts) against the oracle's restatements and the FLOP count the
